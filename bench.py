@@ -1,0 +1,329 @@
+"""Benchmark: fused energy + pose-gradient pair-terms/s on the 65536 x 65536 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload 2]
+
+One step = one energy + pose-gradient evaluation of the REF model (compi.cu:753-772
+restated) over all N x M source/target pairs at one pose: the per-pose prologue, the
+fused adjoint kernel and the FP64 reduction.  A pair-term is one (i, j) pair at one
+pose.  Inputs are seeded synthetic clouds of the named workload (no dataset).
+
+value       whole-job pair-terms/s with the clouds resident on the device (CUDA events
+            around each step on the launching stream; the L2 is flushed between steps
+            by writing 256 MiB, outside the timed events).
+e2e         the same metric through the C ABI with host buffers: dugma_init (FP64 host
+            clouds and covariances copied in), dugma_energy_grad (E and g copied out)
+            and dugma_fr_m per step, wall clock.
+roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instructions per
+            pair x pairs per launch / launch time from CUDA events inside the library)
+            against the FP32 fused-multiply-add rate measured in this run.
+plain_fd    the plain form: energy + central finite differences (13 energy evaluations).
+cpu_baseline  the FP64 C/OpenMP oracle on a bounded sample of source rows, all host cores.
+
+Multi-GPU: each rank evaluates its own multistart pose of the same problem (independent
+units, no collective on the data path): weak scaling, value = sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic per-pair operation counts of the REF kernels, 3D (see the kernel sources)
+FP32_INSTR_ADJOINT = 44     # d 6, u = kC'd 9, exponent 3, d d^T 6, exponent 6, accumulations 14
+FP32_INSTR_ENERGY = 26      # d 6, two Horner quadratic forms 9 + 9, accumulation 2
+SFU_PER_PAIR = 2            # two ex2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fd", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n and world != 1:
+        raise SystemExit(f"--gpus {n} but WORLD_SIZE={world}")
+    return rank, world, local
+
+
+def workload(wl):
+    from dugma_b200 import synth
+    return synth.WORKLOADS[wl]()
+
+
+def eval_pose(P, rank):
+    """The pose of rank r: ground truth perturbed by a seeded multistart offset (rank 0: 10 deg, 2 cm)."""
+    from dugma_b200.pose import expmap
+    rng = np.random.default_rng(100 + rank)
+    ax = rng.standard_normal(3)
+    ax /= np.linalg.norm(ax)
+    R = P.R_G @ expmap(ax * np.radians(10.0))
+    t = P.t_G + 0.02 * ax
+    return R, t
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, path, index):
+        self.path, self.index = path, index
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_rate(P, R, t, sig, budget_s=8.0):
+    """Oracle (FP64, OpenMP, all host threads) pair-terms/s on a bounded sample of source rows."""
+    from oracle import oracle as orc
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    rows = 64
+    done = 0
+    t0 = time.perf_counter()
+    i0 = 0
+    while time.perf_counter() - t0 < budget_s and i0 < st.N:
+        i1 = min(st.N, i0 + rows)
+        st.energy(R, t, sig, i0=i0, i1=i1)
+        done += (i1 - i0) * st.M
+        i0 = i1
+        rows = min(rows * 2, 4096)
+    el = time.perf_counter() - t0
+    return done / el, done, el, orc.num_threads()
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU implementation of the path (the FP64 oracle port; the reference has no
+    CPU code of its own), all host threads, rank 0 only, a bounded sample of rows per step."""
+    if rank != 0:
+        return
+    from dugma_b200 import synth
+    P = workload(args.workload)
+    R, t = eval_pose(P, 0)
+    from oracle import oracle as orc
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    _, d2 = st.nn(R, t, 1)
+    sig = float(np.mean(d2) / 3.0)
+    rows = 256
+    for _ in range(args.warmup):
+        st.energy(R, t, sig, i0=0, i1=rows)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        i0 = (k * rows) % (st.N - rows)
+        st.energy(R, t, sig, i0=i0, i1=i0 + rows)
+    el = time.perf_counter() - t0
+    val = args.steps * rows * st.M / el
+    line = {"impl": "reference", "metric": "energy+grad pair-terms/s", "value": val, "unit": "pair-terms/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{P.name} N=M={P.N}, energy + pose gradient, REF model"},
+            "cpu_baseline": {"value": val, "unit": "pair-terms/s", "cores": orc.num_threads(), "kind": "port",
+                             "sample": f"{rows} source rows x {st.M} targets per step"},
+            "e2e": {"value": val, "unit": "pair-terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from dugma_b200 import _lib, api
+    L = _lib.load(build_if_missing=False)
+
+    P = workload(args.workload)
+    R, t = eval_pose(P, rank)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    sig = api.update_sig(h, R, t)
+    tune = api.autotune(h, 0)
+    pairs = P.N * P.M
+
+    stream = torch.cuda.current_stream()
+    pose = torch.zeros(16, dtype=torch.float64, device="cuda")
+    pose[:9] = torch.tensor(np.asarray(R).T.reshape(-1))
+    pose[9:12] = torch.tensor(t)
+    pose[12] = sig
+    out = torch.zeros(8, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        rc = L.dugma_energy_grad_async(h.arr, pose.data_ptr(), 0, out.data_ptr(), None, stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(L.dugma_last_error().decode())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    import ctypes
+    L.dugma_timing(h.arr, 1, None, None)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                else f"/tmp/clocks_rank{rank}.csv", local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    kms = ctypes.c_double(0)
+    kl = ctypes.c_int(0)
+    L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
+    L.dugma_timing(h.arr, 0, None, None)
+    if world > 1:
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * pairs * args.steps / (ms * 1e-3)
+    res = out.cpu().numpy()
+
+    # roofline of the adjoint kernel
+    peak = ctypes.c_double(0)
+    L.dugma_calibrate(0, ctypes.byref(peak), None)
+    sfu = ctypes.c_double(0)
+    L.dugma_calibrate(1, ctypes.byref(sfu), None)
+    kernel_ms = kms.value / max(kl.value, 1)
+    achieved = FP32_INSTR_ADJOINT * pairs / (kernel_ms * 1e-3)
+    sfu_frac = SFU_PER_PAIR * pairs / (kernel_ms * 1e-3) / sfu.value if sfu.value else None
+
+    extra = {}
+    if not args.no_fd and rank == 0:
+        # plain form: energy + central FD over 6 pose coordinates (13 energy evaluations)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        api.energy_fd_grad(h, R, t, sig)
+        reps = max(2, args.steps // 4)
+        t0.record()
+        for _ in range(reps):
+            api.energy_fd_grad(h, R, t, sig)
+        t1.record()
+        torch.cuda.synchronize()
+        fd_ms = t0.elapsed_time(t1) / reps
+        adj_ms = ms / args.steps
+        extra["plain_fd"] = {"ms_per_gradient": fd_ms, "evals_per_s": 1e3 / fd_ms,
+                             "adjoint_evals_per_s": 1e3 / adj_ms, "adjoint_speedup": fd_ms / adj_ms,
+                             "energy_evals_per_gradient": 13}
+
+    e2e = None
+    if not args.no_e2e:
+        X_C, Y_C = P.X_C, P.Y_C
+        h2d = 8 * (P.X.size + X_C.size + P.Y.size + Y_C.size)
+        # warm-up of the end-to-end path
+        _, h2 = api.init(P.X, X_C, P.Y, Y_C)
+        api.energy_grad(h2, R, t, sig)
+        api.fr_m(h2)
+        ksteps = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(ksteps):
+            _, h2 = api.init(P.X, X_C, P.Y, Y_C)
+            api.energy_grad(h2, R, t, sig)
+            api.fr_m(h2)
+        el = time.perf_counter() - t0
+        e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps}
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        rate, done, el, cores = cpu_rate(P, R, t, sig)
+        cpu = {"value": rate, "unit": "pair-terms/s", "cores": cores, "kind": "port",
+               "sample": f"{done // P.M} source rows x {P.M} targets ({el:.1f} s, FP64 oracle, OpenMP)"}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": "energy+grad pair-terms/s", "value": value, "unit": "pair-terms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{P.name}: N=M={P.N}, REF model energy + pose gradient (fused adjoint), "
+                                   "one multistart pose per GPU", "l2": "flushed between steps (256 MiB write)",
+                       "sigma": sig, "kernel_shape": tune.split(" ")[0] if tune else None},
+            "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
+                         "unit": "Tinstr/s (FP32 pipe, lane ops)", "frac": achieved / peak.value,
+                         "traffic": None, "peak_source": "FP32 FMA-chain kernel measured in this run",
+                         "sfu_frac": sfu_frac, "kernel_ms": kernel_ms,
+                         "instr_per_pair": FP32_INSTR_ADJOINT},
+            "gpu_launches": 3 * args.steps,
+            "result": {"E": float(res[0]), "g": [float(v) for v in res[1:7]]},
+            "autotune": tune,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if clocks:
+            line["clocks"] = clocks
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    api.fr_m(h)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,404 @@
+// coef.cu -- surrogate coefficients (the compi plugin) by moment accumulation.
+//
+// The reference accumulates 637 (3D) / 45 (2D) per-pair coefficient terms with FP64
+// shared-memory atomics (compi.cu:632-3407, 96-460).  Every one of those terms is a
+// product of a source-side factor and a target-side factor (see gen/gen_coef.py), so
+//   A_k = sum_ij P_ij c_k(x_i, B_i, y'_j, C'_j)
+// is a fixed linear combination of the moments
+//   M2[m,a,b] = sum_i B_i[m] f_i[a] H2_i[b],   H2_i = sum_j P_ij g(y'_j)   (pass A, source-stationary)
+//   M1[m,a,b] = sum_j C'_j[m] g_j[a] H1_j[b],  H1_j = sum_i P_ij f(x_i)    (pass B, target-stationary)
+// with f, g the degree <= 2 monomials of a point (10 in 3D, 6 in 2D).  Per pair this is
+// the P computation plus 10 multiply-adds in each pass instead of 637 atomics.
+#include <cmath>
+
+#include "coef_map.h"
+#include "context.hpp"
+#include "pairs.cuh"
+
+namespace dugma {
+
+template <int D> struct Feat { static constexpr int N = 1 + D + Sym<D>::N; };
+
+template <int D>
+__host__ __device__ inline void monomials(const double* p, double* f)
+{
+    f[0] = 1.0;
+    for (int a = 0; a < D; ++a) f[1 + a] = p[a];
+    for (int k = 0; k < Sym<D>::N; ++k) f[1 + D + k] = p[Sym<D>::a(k)] * p[Sym<D>::b(k)];
+}
+
+// ---------------------------------------------------------------------------
+// Records: y side (v0 = y'hi, lv; v1 = y'lo; v2/v3 = k C'_j Horner-packed; g = monomials of y')
+//          x side (v0 = x, lw; v1 = 0;     v2/v3 = k B_i Horner-packed;  g = monomials of x)
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void coef_prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
+                                     const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
+                                     Rec128* __restrict__ yr, const float* __restrict__ x,
+                                     const float* __restrict__ xinv, const float* __restrict__ lwx, int N, int N_pad,
+                                     Rec128* __restrict__ xr)
+{
+    constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
+    double R[9], t[3];
+    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
+    const double s = 1.0 / pose[kPoseSig], ks = K_EXP2 * s;
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
+        Rec128 r;
+        float hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, cp[6] = {0, 0, 0, 0, 0, 0};
+        double g[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        float lv = -INFINITY;
+        if (j < M) {
+            double yp[3] = {0, 0, 0};
+            for (int a = 0; a < D; ++a) {
+                double v = R[a] * (double)y[(size_t)j * D] + R[a + D] * (double)y[(size_t)j * D + 1];
+                if (D == 3) v = v + R[a + 6] * (double)y[(size_t)j * D + 2];
+                yp[a] = v + t[a];
+                hi[a] = __double2float_rn(yp[a]);
+                lo[a] = __double2float_rn(yp[a] - (double)hi[a]);
+            }
+            monomials<D>(yp, g);
+            lv = lwy[j];
+            if (lv != -INFINITY) {
+                double A[3][3], T[3][3];
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0)
+                        A[r0][c0] = 0.5 * ((double)yinv[(size_t)j * D * D + r0 + D * c0] +
+                                           (double)yinv[(size_t)j * D * D + c0 + D * r0]);
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0) {
+                        double acc = 0;
+                        for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = acc;
+                    }
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    double acc = 0;
+                    for (int q = 0; q < D; ++q) acc += R[ra + D * q] * T[q][rb];
+                    cp[k] = __double2float_rn(ks * acc * (ra == rb ? 1.0 : 2.0));
+                }
+            }
+        }
+        r.v0 = make_float4(hi[0], hi[1], hi[2], lv);
+        r.v1 = make_float4(lo[0], lo[1], lo[2], 0.f);
+        r.v2 = D == 3 ? make_float4(cp[0], cp[1], cp[2], cp[3]) : make_float4(cp[0], cp[1], cp[2], 0.f);
+        r.v3 = D == 3 ? make_float4(cp[4], cp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(g[q]) : 0.f;
+        yr[j] = r;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
+        Rec128 r;
+        float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
+        double f[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        float lw = -INFINITY;
+        if (i < N) {
+            double xd[3] = {0, 0, 0};
+            for (int a = 0; a < D; ++a) {
+                xv[a] = x[(size_t)i * D + a];
+                xd[a] = xv[a];
+            }
+            monomials<D>(xd, f);
+            lw = lwx[i];
+            if (lw != -INFINITY)
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    const double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
+                                            (double)xinv[(size_t)i * D * D + rb + D * ra]);
+                    bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
+                }
+        }
+        r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+        r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        r.v2 = D == 3 ? make_float4(bp[0], bp[1], bp[2], bp[3]) : make_float4(bp[0], bp[1], bp[2], 0.f);
+        r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(f[q]) : 0.f;
+        xr[i] = r;
+    }
+}
+
+// Horner quadratic form of a packed (k-scaled, off-diagonal-doubled) matrix plus an offset
+template <int D>
+__device__ __forceinline__ float qform(const float* m, float d0, float d1, float d2, float off)
+{
+    if (D == 3) {
+        const float g0 = fmaf(m[4], d2, fmaf(m[3], d1, m[0] * d0));
+        const float g1 = fmaf(m[5], d2, m[1] * d1);
+        const float g2 = m[2] * d2;
+        return fmaf(d0, g0, fmaf(d1, g1, fmaf(d2, g2, off)));
+    } else {
+        const float g0 = fmaf(m[2], d1, m[0] * d0);
+        const float g1 = m[1] * d1;
+        return fmaf(d0, g0, fmaf(d1, g1, off));
+    }
+}
+
+// One body for both passes.  The stationary side keeps (pos hi, pos lo, matrix) in registers;
+// the streamed side supplies (pos hi, pos lo, matrix, log2 weight, monomials).  d = p_x - p_y' up
+// to sign (the quadratic forms do not see the sign).  H accumulates P * streamed monomials.
+template <int D, int IPT_>
+struct CoefBody {
+    using StreamRec = Rec128;
+    static constexpr int IPT = IPT_;
+    static constexpr int NV = 1;
+    static constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
+    float ph[IPT][D], pl[IPT][D], m[IPT][NS];
+    float h[IPT][NF];
+    double H[IPT][NF];
+    int row[IPT];
+    double G;
+
+    __device__ void setup(const PairArgs& a)
+    {
+        const double s = 1.0 / a.pose[kPoseSig];
+        G = pow(s, (double)D) * exp2(a.Lmax);
+    }
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        const Rec128* rr = static_cast<const Rec128*>(a.xrec);
+        row[ii] = i < a.i_end ? i : -1;
+        const Rec128 r = rr[i < a.i_end ? i : 0];
+        const bool ok = i < a.i_end;
+        const float hv[3] = {r.v0.x, r.v0.y, r.v0.z}, lv[3] = {r.v1.x, r.v1.y, r.v1.z};
+        const float mv[6] = {r.v2.x, r.v2.y, r.v2.z, r.v2.w, r.v3.x, r.v3.y};
+#pragma unroll
+        for (int q = 0; q < D; ++q) { ph[ii][q] = ok ? hv[q] : 0.f; pl[ii][q] = ok ? lv[q] : 0.f; }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) m[ii][q] = ok ? mv[q] : 0.f;
+    }
+    __device__ void zero_all()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii)
+#pragma unroll
+            for (int q = 0; q < NF; ++q) { h[ii][q] = 0.f; H[ii][q] = 0.0; }
+    }
+    __device__ __forceinline__ void consume(const Rec128& r, int)
+    {
+        const float4 v0 = r.v0, v1 = r.v1, v2 = r.v2, v3 = r.v3;
+        const float ms[6] = {v2.x, v2.y, v2.z, v2.w, v3.x, v3.y};
+        float g[NF];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) g[q] = r.g[q];
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            // (hi_s + lo_s) - (hi_t + lo_t); hi_s - hi_t is exact for near pairs
+            const float d0 = (ph[ii][0] - v0.x) + (pl[ii][0] - v1.x);
+            const float d1 = (ph[ii][1] - v0.y) + (pl[ii][1] - v1.y);
+            const float d2 = D == 3 ? (ph[ii][2] - v0.z) + (pl[ii][2] - v1.z) : 0.f;
+            const float t1 = qform<D>(m[ii], d0, d1, d2, v0.w);
+            const float t2 = qform<D>(ms, d0, d1, d2, v0.w);
+            const float p = ex2(t1) + ex2(t2);
+#pragma unroll
+            for (int q = 0; q < NF; ++q) h[ii][q] = fmaf(p, g[q], h[ii][q]);
+        }
+    }
+    __device__ void fold()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii)
+#pragma unroll
+            for (int q = 0; q < NF; ++q) { H[ii][q] += (double)h[ii][q]; h[ii][q] = 0.f; }
+    }
+    __device__ void finish(const PairArgs& a, int jc, double (&)[NV])
+    {
+        const int rows = a.i_end - a.i0;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            const double w = (double)a.wx[row[ii]] * G;   // wx: the stationary side's |Sigma|^-1/2
+            double* o = a.h_part + ((size_t)jc * rows + (row[ii] - a.i0)) * 16;
+#pragma unroll
+            for (int q = 0; q < NF; ++q) o[q] = w * H[ii][q];
+        }
+    }
+};
+
+template <class Body, int NT, int TJ>
+__global__ void __launch_bounds__(NT) coef_pass_kernel(PairArgs a)
+{
+    Body body;
+    run_pairs<Body, NT, TJ, 4>(a, body);
+}
+
+__constant__ signed char c_moment3[kNumMoments3D][4];
+__constant__ signed char c_moment2[kNumMoments2D][4];
+
+// Moments from the per-point H: kind 2 over sources (side = 0), kind 1 over targets (side = 1).
+// Per-warp partial sums in shared memory, then per-block partials in fixed order.
+template <int D>
+__global__ void moments_kernel(const double* __restrict__ hpart, int n_jc, int n, int side,
+                               const double* __restrict__ pose, const float* __restrict__ p,
+                               const float* __restrict__ cinv, double* __restrict__ block_out)
+{
+    constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
+    constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
+    const signed char(*tab)[4] = D == 3 ? c_moment3 : c_moment2;
+    __shared__ double wsum[8][NM];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < 8 * NM; k += blockDim.x) (&wsum[0][0])[k] = 0.0;
+    __syncthreads();
+    double R[9], t[3];
+    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
+    const double s = 1.0 / pose[kPoseSig];
+    const int kind = side == 0 ? 2 : 1;
+    const int per_block = (n + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
+    for (int base = b0; base < b1; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const bool ok = i < b1;
+        double H[NF], f[NF], mat[NS];
+        for (int q = 0; q < NF; ++q) H[q] = 0.0;
+        for (int q = 0; q < NS; ++q) mat[q] = 0.0;
+        for (int q = 0; q < NF; ++q) f[q] = 0.0;
+        if (ok) {
+            for (int c = 0; c < n_jc; ++c)
+                for (int q = 0; q < NF; ++q) H[q] += hpart[((size_t)c * n + i) * 16 + q];
+            double pt[3] = {0, 0, 0};
+            double A[3][3];
+            for (int r0 = 0; r0 < D; ++r0)
+                for (int c0 = 0; c0 < D; ++c0)
+                    A[r0][c0] = 0.5 * s * ((double)cinv[(size_t)i * D * D + r0 + D * c0] +
+                                           (double)cinv[(size_t)i * D * D + c0 + D * r0]);
+            if (side == 0) {
+                for (int a = 0; a < D; ++a) pt[a] = (double)p[(size_t)i * D + a];
+                for (int k = 0; k < NS; ++k) mat[k] = A[Sym<D>::a(k)][Sym<D>::b(k)];
+            } else {
+                for (int a = 0; a < D; ++a) {
+                    double v = R[a] * (double)p[(size_t)i * D] + R[a + D] * (double)p[(size_t)i * D + 1];
+                    if (D == 3) v = v + R[a + 6] * (double)p[(size_t)i * D + 2];
+                    pt[a] = v + t[a];
+                }
+                double T[3][3];
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0) {
+                        double acc = 0;
+                        for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = acc;
+                    }
+                for (int k = 0; k < NS; ++k) {
+                    double acc = 0;
+                    for (int q = 0; q < D; ++q) acc += R[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
+                    mat[k] = acc;
+                }
+            }
+            monomials<D>(pt, f);
+        }
+        for (int mi = 0; mi < NM; ++mi) {
+            if (tab[mi][0] != kind) continue;
+            double v = mat[tab[mi][1]] * f[tab[mi][2]] * H[tab[mi][3]];
+            v = warp_sum(v);
+            if (lane == 0) wsum[warp][mi] += v;
+        }
+    }
+    __syncthreads();
+    for (int mi = threadIdx.x; mi < NM; mi += blockDim.x) {
+        double v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += wsum[w][mi];
+        block_out[(size_t)blockIdx.x * NM + mi] = v;
+    }
+}
+
+__global__ void moments_reduce_kernel(const double* __restrict__ a, int na, const double* __restrict__ b, int nb,
+                                      int nm, double* __restrict__ out)
+{
+    for (int mi = threadIdx.x; mi < nm; mi += blockDim.x) {
+        double v = 0;
+        for (int k = 0; k < na; ++k) v += a[(size_t)k * nm + mi];
+        for (int k = 0; k < nb; ++k) v += b[(size_t)k * nm + mi];
+        out[mi] = v;
+    }
+}
+
+using KernelFn = void (*)(PairArgs);
+int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
+                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
+                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
+                        cudaStream_t s);
+
+int num_moments(int D) { return D == 3 ? kNumMoments3D : kNumMoments2D; }
+
+int Context::ensure_coef_records()
+{
+    if (yrec128) return DUGMA_OK;
+    DUGMA_CK(cudaMalloc(&yrec128, sizeof(Rec128) * (size_t)M_pad));
+    DUGMA_CK(cudaMalloc(&xrec128, sizeof(Rec128) * (size_t)N_pad));
+    return DUGMA_OK;
+}
+
+template <int D>
+static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+{
+    static bool tables = false;
+    if (!tables) {
+        DUGMA_CK(cudaMemcpyToSymbol(c_moment3, kMoment3D, sizeof(kMoment3D)));
+        DUGMA_CK(cudaMemcpyToSymbol(c_moment2, kMoment2D, sizeof(kMoment2D)));
+        tables = true;
+    }
+    DUGMA_RET(c.ensure_coef_records());
+    const int n = std::max(c.M_pad, c.N_pad);
+    coef_prologue_kernel<D><<<std::min((n + 255) / 256, c.num_sms * 4), 256, 0, s>>>(
+        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128);
+    DUGMA_CK(cudaGetLastError());
+    constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
+    const KernelShape sh{2, 128, 32};
+    KernelFn fn = coef_pass_kernel<CoefBody<D, 2>, 128, 32>;
+    const int nblk = std::min(c.num_sms, 64);
+    // the moment partials live in a dedicated device buffer (scratch is reused by each pass)
+    double* mom = nullptr;
+    DUGMA_CK(cudaMallocAsync(&mom, sizeof(double) * (size_t)2 * nblk * NM, s));
+    int rc = DUGMA_OK;
+    for (int side = 0; side < 2 && rc == DUGMA_OK; ++side) {
+        // side 0: sources stationary over streamed targets; side 1: the reverse
+        double* hp = nullptr;
+        int n_jc = 0;
+        PairArgs dummy{};
+        (void)dummy;
+        const Rec128* src = side == 0 ? c.xrec128 : c.yrec128;
+        const Rec128* str = side == 0 ? c.yrec128 : c.xrec128;
+        const int rows = side == 0 ? c.N : c.M;
+        const size_t nstr = side == 0 ? (size_t)c.M_pad : (size_t)c.N_pad;
+        const double Lmax = side == 0 ? c.Lmax_y : c.Lmax_x;
+        // launch_pair_variant reads the stationary weights from c.wx; swap for the target pass
+        float* wsave = c.wx;
+        if (side == 1) c.wx = c.wy;
+        rc = launch_pair_variant(c, fn, sh, src, str, nstr, 1, Lmax, pose_dev, 0, rows, nullptr, nullptr, &hp, 16,
+                                 &n_jc, s);
+        c.wx = wsave;
+        if (rc != DUGMA_OK) break;
+        if (side == 0)
+            moments_kernel<D><<<nblk, 256, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x, c.xinv, mom);
+        else
+            moments_kernel<D><<<nblk, 256, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y, c.yinv, mom + (size_t)nblk * NM);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moments kernel launch failed");
+    }
+    if (rc == DUGMA_OK) {
+        moments_reduce_kernel<<<1, 256, 0, s>>>(mom, nblk, mom + (size_t)nblk * NM, nblk, NM, moments_dev);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moment reduction launch failed");
+    }
+    cudaFreeAsync(mom, s);
+    return rc;
+}
+
+int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+{
+    return c.D == 3 ? coef_impl<3>(c, pose_dev, moments_dev, s) : coef_impl<2>(c, pose_dev, moments_dev, s);
+}
+
+int coef_from_moments(int D, const double* mom, double* out640)
+{
+    for (int k = 0; k < 640; ++k) out640[k] = 0.0;
+    const int K = D == 3 ? kNumCoef3D : kNumCoef2D;
+    const int* start = D == 3 ? kCoefStart3D : kCoefStart2D;
+    const int* mi = D == 3 ? kCoefMoment3D : kCoefMoment2D;
+    const double* wt = D == 3 ? kCoefWeight3D : kCoefWeight2D;
+    for (int k = 0; k < K; ++k) {
+        double v = 0;
+        for (int e = start[k]; e < start[k + 1]; ++e) v += wt[e] * mom[mi[e]];
+        out640[k] = v;
+    }
+    return DUGMA_OK;
+}
+
+}  // namespace dugma

@@ -1,0 +1,166 @@
+// common.cuh -- device helpers shared by the DUGMA sm_100a kernels.
+//
+// Conventions (identical to the C ABI in include/dugma.h):
+//   * points are point-major floats (MATLAB D x N column-major);
+//   * per-point covariances are D x D column-major blocks;
+//   * R is D x D column-major and moves Y: y' = R y + t (update_sig.cu:247-249);
+//   * symmetric matrices are packed (00,11,22,01,02,12) in 3D, (00,11,01) in 2D.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dugma.h"
+
+namespace dugma {
+
+// ---------------------------------------------------------------------------
+// Packed symmetric helpers
+// ---------------------------------------------------------------------------
+template <int D> struct Sym;
+template <> struct Sym<3> {
+    static constexpr int N = 6;
+    static constexpr int NR = 3;   // rotation degrees of freedom
+    __host__ __device__ static constexpr int a(int k) { return k < 3 ? k : (k == 5 ? 1 : 0); }
+    __host__ __device__ static constexpr int b(int k) { return k < 3 ? k : (k == 3 ? 1 : 2); }
+};
+template <> struct Sym<2> {
+    static constexpr int N = 3;
+    static constexpr int NR = 1;
+    __host__ __device__ static constexpr int a(int k) { return k < 2 ? k : 0; }
+    __host__ __device__ static constexpr int b(int k) { return k < 2 ? k : 1; }
+};
+
+// -1/2 * log2(e): exp(-m/2) = 2^(K_EXP2 * m)
+constexpr double K_EXP2 = -0.72134752044448170367996234050095;
+
+// 2^x on the SFU (PTX ex2.approx.ftz.f32; ~2 ulp, denormal results flush to 0)
+__device__ __forceinline__ float ex2(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// ---------------------------------------------------------------------------
+// Record layouts in HBM (16-byte aligned so tiles can be moved by bulk copy)
+// ---------------------------------------------------------------------------
+// Streamed target record, one per y_j and pose (64 B):
+//   v0 = (y'hi.x, y'hi.y, y'hi.z, lv)   y'hi = float(y'), lv = log2(v_j) - Lmax (<= 0, -inf: neglected/padding)
+//   v1 = (y'lo.x, y'lo.y, y'lo.z, 0)    y'lo = float(y' - y'hi)
+//   v2 = (c00, c11, c22, c01)           k * C'_j packed, k = -1/2 log2 e
+//   v3 = (c02, c12, 0, 0)               (off-diagonals doubled in the Horner layout)
+// In 2D the z components are 0 and v2 = (c00, c11, c01, 0).
+struct __align__(16) YRec {
+    float4 v0, v1, v2, v3;
+};
+
+// Source record, one per x_i and sigma (64 B):
+//   v0 = (x.x, x.y, x.z, lw)            lw = log2(w_i) - Lmax_x
+//   v1 = (0, 0, 0, 0)
+//   v2 = (b00, b11, b22, 2 b01)         k * B_i packed, off-diagonals doubled
+//   v3 = (2 b02, 2 b12, 0, 0)
+struct __align__(16) XRec {
+    float4 v0, v1, v2, v3;
+};
+
+// Coefficient-pass records (128 B): the 64-B record followed by the degree <= 2 monomials
+// of the point, g = (1, v_0..v_{D-1}, packed v_a v_b) (10 in 3D, 6 in 2D), zero padded.
+struct __align__(16) Rec128 {
+    float4 v0, v1, v2, v3;
+    float g[16];
+};
+
+// ---------------------------------------------------------------------------
+// Bulk copy (TMA engine, non-tensor form) + mbarrier with bounded waits
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy completing on an mbarrier (no multicast).
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls (each poll may suspend the thread for a
+// hardware-chosen interval), records DUGMA_ERR_TIMEOUT in *err and returns false.
+constexpr uint32_t kWaitPolls = 1u << 24;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err)
+{
+    for (uint32_t it = 0; it < kWaitPolls; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicOr(err, 1 << DUGMA_ERR_TIMEOUT);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum NV doubles per thread over the block (fixed order => deterministic); result valid in thread 0.
+template <int NV, int NT>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch /* [NT/32][NV] */)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) scratch[warp * NV + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double s = 0;
+            for (int w = 0; w < NT / 32; ++w) s += scratch[w * NV + k];
+            v[k] = s;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace dugma

@@ -1,0 +1,129 @@
+// context.hpp -- per-init device state of the DUGMA library.
+//
+// The reference keeps N, M, D, R, t and sigma in per-module __constant__ memory and
+// is therefore not re-entrant (compi.cu:14-16, update_sig.cu:15-16, init.cu:10).
+// Here every dugma_init creates a Context that owns its buffers and a stream; it is
+// found again from the Ptr[6] the caller passes back (keyed by Ptr[0]).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "dugma.h"
+
+namespace dugma {
+
+// Pose block on the device: R (D x D col-major, zero padded to 9), t (3), sig, pad.
+constexpr int kPoseDoubles = 16;
+constexpr int kPoseT = 9;
+constexpr int kPoseSig = 12;
+
+constexpr int kHostDoubles = 1024;
+constexpr int kPadI = 1024;   // source rows padded to a multiple (largest i-block)
+constexpr int kPadJ = 128;    // target rows padded to a multiple (largest j-tile)
+
+struct KernelShape {
+    int ipt = 0;      // source points per thread
+    int nt = 0;       // threads per block
+    int tj = 0;       // targets per shared-memory tile
+    bool valid() const { return ipt > 0; }
+};
+
+struct Context {
+    int N = 0, M = 0, D = 0, dev = 0;
+    int N_pad = 0, M_pad = 0;
+    int nonpd = 0;
+    // reference state (Ptr[0..5])
+    float *x = nullptr, *xinv = nullptr, *y = nullptr, *yinv = nullptr, *wx = nullptr, *wy = nullptr;
+    // extra state
+    float *xcov = nullptr, *ycov = nullptr;   // packed symmetric FP32 covariances (CONV model)
+    float *lwx = nullptr, *lwy = nullptr;     // log2(w) - Lmax, -inf when neglected
+    double Lmax_x = 0, Lmax_y = 0;
+    // per-evaluation records
+    YRec* yrec = nullptr;
+    XRec* xrec = nullptr;
+    Rec128* yrec128 = nullptr;
+    Rec128* xrec128 = nullptr;
+    float4* yp32 = nullptr;                   // float(y') for nearest neighbours
+    float* dmin = nullptr;                    // nearest squared distance per source (sigma)
+    double* pose = nullptr;                   // kPoseDoubles
+    double* out = nullptr;                    // 64 doubles of results
+    int* err = nullptr;                       // device error word
+    int* counter = nullptr;                   // work-queue counters (8)
+    double* dedx = nullptr;                   // dE/dx rows (allocated on first request)
+    double* mom = nullptr;                    // surrogate moments (512 doubles)
+    // growable scratch
+    double* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // pinned host staging
+    // [0,16) pose, [63] error word, [64,128) results, [256,512) multi-pose staging
+    double* host = nullptr;                   // kHostDoubles doubles
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    KernelShape shape_adj, shape_energy, shape_nn;
+    std::mutex mu;                            // one host call at a time per context
+    // optional timing of the main pairwise kernel (dugma_timing)
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tevents;
+    size_t tused = 0;
+
+    int ensure_scratch(size_t bytes);
+    int ensure_coef_records();
+};
+
+// registry
+Context* find_context(float* const* Ptr);
+void register_context(Context* c);
+void unregister_context(Context* c);
+
+// errors (thread-local message)
+int set_error(int code, const char* fmt, ...);
+const char* last_error();
+
+#define DUGMA_CK(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::dugma::set_error(DUGMA_ERR_CUDA, "%s failed: %s (%s:%d)", #call,     \
+                                      cudaGetErrorString(e_), __FILE__, __LINE__);        \
+    } while (0)
+
+#define DUGMA_RET(call)           \
+    do {                          \
+        int r_ = (call);          \
+        if (r_ != DUGMA_OK) return r_; \
+    } while (0)
+
+// ---- kernel launchers (energy.cu, nn.cu, coef.cu) ----
+// Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy), x records.
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s);
+// Pairwise energy (grad = false) or fused adjoint (grad = true) over source rows [i0, i1);
+// writes {E, g} to out_dev and, if dEdx_dev, dE/dx for rows [i0, i1) (relative index).
+int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1,
+                 double* out_dev, double* dEdx_dev, cudaStream_t s, const KernelShape* force = nullptr);
+// Nearest neighbours: writes idx/d2 (device) and optionally the per-point minimum only.
+int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
+              const KernelShape* force = nullptr);
+// sigma: out_dev[0] = exact FP64 sigma, out_dev[1] = quantised (reference) sigma.
+int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s);
+// Surrogate coefficient moments: out_dev receives kNumMoments doubles.
+int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s);
+int coef_from_moments(int D, const double* moments, double* coef640);
+int num_moments(int D);
+
+// init kernels
+int launch_init(Context& c, const double* X, const double* XC, const double* Y, const double* YC);
+
+// candidate kernel shapes for the autotuner
+std::vector<KernelShape> adjoint_shapes();
+std::vector<KernelShape> energy_shapes();
+std::vector<KernelShape> nn_shapes();
+
+}  // namespace dugma

@@ -1,0 +1,496 @@
+// energy.cu -- REF energy and fused adjoint (energy + pose gradient + dE/dx) kernels.
+//
+// Per pair (compi.cu:753-772 restated):  d = x_i - y'_j,
+//   e1 = exp(-1/2 d^T C'_j d),  e2 = exp(-1/2 d^T B_i d),  P_ij = w_i v_j (e1 + e2).
+// FP32 per pair; d from the double-float split of y' (y'hi, y'lo) so that the
+// cancellation x - y' is exact for near pairs; the -1/2 log2 e factor is folded into
+// C' and B, and log2 v_j into the exponent, so each exponential is one SFU ex2.
+//
+// Adjoint (left perturbation R <- exp([w]x) R, t <- t + dt), per source row i:
+//   S1 = sum_j e1' k C'd,   D2 = sum_j e2' d,   Q2 = sum_j e2' d d^T,   E = sum_j (e1' + e2')
+//   dE/dt     += w_i (S1/k + B_i D2)
+//   dE/dw     += w_i ((x_i - t) x (S1/k + B_i D2) - sum_j e2' d x B_i d)   [from Q2 and B_i]
+//   dE/dx_i    = -w_i (S1/k + B_i D2)
+// (e' = v_j e / 2^Lmax; w_i = |Sx|^-1/2 s^D 2^Lmax; the e2 rotation term uses R y_j = (x_i - t) - d.)
+// Accumulation: FP32 within a tile of TJ targets, then the energy in FP64 and the
+// gradient moments in a second FP32 level per item, FP64 across items.
+#include <cmath>
+#include <mutex>
+
+#include "context.hpp"
+#include "pairs.cuh"
+
+namespace dugma {
+
+template <int D>
+__device__ __forceinline__ void load_xrec(const XRec& r, float* x, float* b)
+{
+    x[0] = r.v0.x;
+    x[1] = r.v0.y;
+    if (D == 3) x[2] = r.v0.z;
+    b[0] = r.v2.x;
+    b[1] = r.v2.y;
+    b[2] = r.v2.z;
+    if (D == 3) {
+        b[3] = r.v2.w;
+        b[4] = r.v3.x;
+        b[5] = r.v3.y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Energy only (the "plain" form's kernel).  Horner quadratic forms: 26 FP32 + 2 SFU / pair (3D).
+// ---------------------------------------------------------------------------
+template <int D, int IPT_>
+struct RefEnergyBody {
+    using StreamRec = YRec;
+    static constexpr int IPT = IPT_;
+    static constexpr int NV = 1;
+    static constexpr int NS = Sym<D>::N;
+    float x[IPT][D], b[IPT][NS], e[IPT];
+    double E64[IPT];
+    int row[IPT];
+    double G;
+
+    __device__ void setup(const PairArgs& a)
+    {
+        const double s = 1.0 / a.pose[kPoseSig];
+        G = pow(s, (double)D) * exp2(a.Lmax);
+    }
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        if (i < a.i_end) {
+            row[ii] = i;
+            load_xrec<D>(static_cast<const XRec*>(a.xrec)[i], x[ii], b[ii]);
+        } else {
+            row[ii] = -1;
+#pragma unroll
+            for (int q = 0; q < D; ++q) x[ii][q] = 0.f;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) b[ii][q] = 0.f;
+        }
+    }
+    __device__ void zero_all()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) { e[ii] = 0.f; E64[ii] = 0.0; }
+    }
+    __device__ __forceinline__ void consume(const YRec& r, int)
+    {
+        const float4 v0 = r.v0, v1 = r.v1, v2 = r.v2, v3 = r.v3;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (D == 3) {
+                const float d0 = (x[ii][0] - v0.x) - v1.x, d1 = (x[ii][1] - v0.y) - v1.y,
+                            d2 = (x[ii][2] - v0.z) - v1.z;
+                const float g0 = fmaf(v3.x, d2, fmaf(v2.w, d1, v2.x * d0));
+                const float g1 = fmaf(v3.y, d2, v2.y * d1);
+                const float g2 = v2.z * d2;
+                const float t1 = fmaf(d0, g0, fmaf(d1, g1, fmaf(d2, g2, v0.w)));
+                const float* B = b[ii];
+                const float h0 = fmaf(B[4], d2, fmaf(B[3], d1, B[0] * d0));
+                const float h1 = fmaf(B[5], d2, B[1] * d1);
+                const float h2 = B[2] * d2;
+                const float t2 = fmaf(d0, h0, fmaf(d1, h1, fmaf(d2, h2, v0.w)));
+                e[ii] += ex2(t1);
+                e[ii] += ex2(t2);
+            } else {
+                const float d0 = (x[ii][0] - v0.x) - v1.x, d1 = (x[ii][1] - v0.y) - v1.y;
+                const float g0 = fmaf(v2.z, d1, v2.x * d0);
+                const float g1 = v2.y * d1;
+                const float t1 = fmaf(d0, g0, fmaf(d1, g1, v0.w));
+                const float* B = b[ii];
+                const float h0 = fmaf(B[2], d1, B[0] * d0);
+                const float h1 = B[1] * d1;
+                const float t2 = fmaf(d0, h0, fmaf(d1, h1, v0.w));
+                e[ii] += ex2(t1);
+                e[ii] += ex2(t2);
+            }
+        }
+    }
+    __device__ void fold()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) { E64[ii] += (double)e[ii]; e[ii] = 0.f; }
+    }
+    __device__ void finish(const PairArgs& a, int, double (&acc)[NV])
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii)
+            if (row[ii] >= 0) acc[0] += (double)a.wx[row[ii]] * G * E64[ii];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Fused adjoint.  Per pair (3D): d 6, u = kC'd 9, exponent 3, q = d d^T 6, exponent 6,
+// accumulations 14  -> 44 FP32 + 2 SFU.
+// ---------------------------------------------------------------------------
+template <int D, int IPT_>
+struct RefAdjointBody {
+    using StreamRec = YRec;
+    static constexpr int IPT = IPT_;
+    static constexpr int NS = Sym<D>::N;
+    static constexpr int NR = Sym<D>::NR;
+    static constexpr int NV = 1 + NR + D;
+    float x[IPT][D], b[IPT][NS];
+    float e[IPT], S1[IPT][D], D2[IPT][D], Q2[IPT][NS];        // tile level
+    float S1r[IPT][D], D2r[IPT][D], Q2r[IPT][NS];             // item level
+    double E64[IPT];
+    int row[IPT];
+    double G, t[3];
+
+    __device__ void setup(const PairArgs& a)
+    {
+        const double s = 1.0 / a.pose[kPoseSig];
+        G = pow(s, (double)D) * exp2(a.Lmax);
+#pragma unroll
+        for (int q = 0; q < D; ++q) t[q] = a.pose[kPoseT + q];
+    }
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        if (i < a.i_end) {
+            row[ii] = i;
+            load_xrec<D>(static_cast<const XRec*>(a.xrec)[i], x[ii], b[ii]);
+        } else {
+            row[ii] = -1;
+#pragma unroll
+            for (int q = 0; q < D; ++q) x[ii][q] = 0.f;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) b[ii][q] = 0.f;
+        }
+    }
+    __device__ void zero_tile()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            e[ii] = 0.f;
+#pragma unroll
+            for (int q = 0; q < D; ++q) { S1[ii][q] = 0.f; D2[ii][q] = 0.f; }
+#pragma unroll
+            for (int q = 0; q < NS; ++q) Q2[ii][q] = 0.f;
+        }
+    }
+    __device__ void zero_all()
+    {
+        zero_tile();
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            E64[ii] = 0.0;
+#pragma unroll
+            for (int q = 0; q < D; ++q) { S1r[ii][q] = 0.f; D2r[ii][q] = 0.f; }
+#pragma unroll
+            for (int q = 0; q < NS; ++q) Q2r[ii][q] = 0.f;
+        }
+    }
+    __device__ __forceinline__ void consume(const YRec& r, int)
+    {
+        const float4 v0 = r.v0, v1 = r.v1, v2 = r.v2, v3 = r.v3;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            const float* B = b[ii];
+            if (D == 3) {
+                const float d0 = (x[ii][0] - v0.x) - v1.x, d1 = (x[ii][1] - v0.y) - v1.y,
+                            d2 = (x[ii][2] - v0.z) - v1.z;
+                // u = k C' d with C' packed (c00, c11, c22, c01 | c02, c12)
+                const float u0 = fmaf(v3.x, d2, fmaf(v2.w, d1, v2.x * d0));
+                const float u1 = fmaf(v3.y, d2, fmaf(v2.y, d1, v2.w * d0));
+                const float u2 = fmaf(v2.z, d2, fmaf(v3.y, d1, v3.x * d0));
+                const float t1 = fmaf(d2, u2, fmaf(d1, u1, fmaf(d0, u0, v0.w)));
+                const float q00 = d0 * d0, q11 = d1 * d1, q22 = d2 * d2;
+                const float q01 = d0 * d1, q02 = d0 * d2, q12 = d1 * d2;
+                const float t2 =
+                    fmaf(B[5], q12, fmaf(B[4], q02, fmaf(B[3], q01, fmaf(B[2], q22, fmaf(B[1], q11, fmaf(B[0], q00, v0.w))))));
+                const float e1 = ex2(t1), e2 = ex2(t2);
+                e[ii] += e1;
+                e[ii] += e2;
+                S1[ii][0] = fmaf(e1, u0, S1[ii][0]);
+                S1[ii][1] = fmaf(e1, u1, S1[ii][1]);
+                S1[ii][2] = fmaf(e1, u2, S1[ii][2]);
+                D2[ii][0] = fmaf(e2, d0, D2[ii][0]);
+                D2[ii][1] = fmaf(e2, d1, D2[ii][1]);
+                D2[ii][2] = fmaf(e2, d2, D2[ii][2]);
+                Q2[ii][0] = fmaf(e2, q00, Q2[ii][0]);
+                Q2[ii][1] = fmaf(e2, q11, Q2[ii][1]);
+                Q2[ii][2] = fmaf(e2, q22, Q2[ii][2]);
+                Q2[ii][3] = fmaf(e2, q01, Q2[ii][3]);
+                Q2[ii][4] = fmaf(e2, q02, Q2[ii][4]);
+                Q2[ii][5] = fmaf(e2, q12, Q2[ii][5]);
+            } else {
+                const float d0 = (x[ii][0] - v0.x) - v1.x, d1 = (x[ii][1] - v0.y) - v1.y;
+                // C' packed (c00, c11, c01)
+                const float u0 = fmaf(v2.z, d1, v2.x * d0);
+                const float u1 = fmaf(v2.y, d1, v2.z * d0);
+                const float t1 = fmaf(d1, u1, fmaf(d0, u0, v0.w));
+                const float q00 = d0 * d0, q11 = d1 * d1, q01 = d0 * d1;
+                const float t2 = fmaf(B[2], q01, fmaf(B[1], q11, fmaf(B[0], q00, v0.w)));
+                const float e1 = ex2(t1), e2 = ex2(t2);
+                e[ii] += e1;
+                e[ii] += e2;
+                S1[ii][0] = fmaf(e1, u0, S1[ii][0]);
+                S1[ii][1] = fmaf(e1, u1, S1[ii][1]);
+                D2[ii][0] = fmaf(e2, d0, D2[ii][0]);
+                D2[ii][1] = fmaf(e2, d1, D2[ii][1]);
+                Q2[ii][0] = fmaf(e2, q00, Q2[ii][0]);
+                Q2[ii][1] = fmaf(e2, q11, Q2[ii][1]);
+                Q2[ii][2] = fmaf(e2, q01, Q2[ii][2]);
+            }
+        }
+    }
+    __device__ void fold()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            E64[ii] += (double)e[ii];
+#pragma unroll
+            for (int q = 0; q < D; ++q) { S1r[ii][q] += S1[ii][q]; D2r[ii][q] += D2[ii][q]; }
+#pragma unroll
+            for (int q = 0; q < NS; ++q) Q2r[ii][q] += Q2[ii][q];
+        }
+        zero_tile();
+    }
+    __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
+    {
+        const double kinv = 1.0 / K_EXP2;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            const int i = row[ii];
+            const double w = (double)a.wx[i] * G;
+            double Bm[3][3], Qm[3][3];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                const int ra = Sym<D>::a(q), rb = Sym<D>::b(q);
+                const double bv = (double)b[ii][q] * kinv * (ra == rb ? 1.0 : 0.5);
+                Bm[ra][rb] = bv;
+                Bm[rb][ra] = bv;
+                Qm[ra][rb] = (double)Q2r[ii][q];
+                Qm[rb][ra] = (double)Q2r[ii][q];
+            }
+            double gt[3], p[3];
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                double bd = 0;
+#pragma unroll
+                for (int c = 0; c < D; ++c) bd += Bm[q][c] * (double)D2r[ii][c];
+                gt[q] = (double)S1r[ii][q] * kinv + bd;
+                p[q] = (double)x[ii][q] - t[q];
+            }
+            acc[0] += w * E64[ii];
+            if (D == 3) {
+                double qx[3] = {0, 0, 0};
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    qx[0] += Bm[2][c] * Qm[1][c] - Bm[1][c] * Qm[2][c];
+                    qx[1] += Bm[0][c] * Qm[2][c] - Bm[2][c] * Qm[0][c];
+                    qx[2] += Bm[1][c] * Qm[0][c] - Bm[0][c] * Qm[1][c];
+                }
+                acc[1] += w * (p[1] * gt[2] - p[2] * gt[1] - qx[0]);
+                acc[2] += w * (p[2] * gt[0] - p[0] * gt[2] - qx[1]);
+                acc[3] += w * (p[0] * gt[1] - p[1] * gt[0] - qx[2]);
+            } else {
+                double qx = 0;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) qx += Bm[1][c] * Qm[0][c] - Bm[0][c] * Qm[1][c];
+                acc[1] += w * (p[0] * gt[1] - p[1] * gt[0] - qx);
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) acc[1 + NR + q] += w * gt[q];
+            if (a.dx_part) {
+                const int rows = a.i_end - a.i0;
+#pragma unroll
+                for (int q = 0; q < D; ++q) a.dx_part[((size_t)jc * rows + (i - a.i0)) * D + q] = -w * gt[q];
+            }
+        }
+    }
+};
+
+template <class Body, int NT, int TJ>
+__global__ void __launch_bounds__(NT) pair_kernel(PairArgs a)
+{
+    Body body;
+    run_pairs<Body, NT, TJ, 4>(a, body);
+}
+
+// deterministic reduction of per-item partials: out[v] = sum_items partials[item][v]
+__global__ void reduce_items_kernel(const double* __restrict__ part, int n_items, int nv, double* __restrict__ out)
+{
+    __shared__ double red[256];
+    for (int v = 0; v < nv; ++v) {
+        double s = 0;
+        for (int it = threadIdx.x; it < n_items; it += blockDim.x) s += part[(size_t)it * 8 + v];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[v] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void reduce_chunks_kernel(const double* __restrict__ part, int n_jc, size_t n, double* __restrict__ out)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int c = 0; c < n_jc; ++c) s += part[(size_t)c * n + e];
+        out[e] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using KernelFn = void (*)(PairArgs);
+
+struct Variant {
+    KernelShape shape;
+    KernelFn fn;
+};
+
+template <int D>
+static const std::vector<Variant>& adjoint_variants()
+{
+    static const std::vector<Variant> v = {
+        {{2, 128, 64}, pair_kernel<RefAdjointBody<D, 2>, 128, 64>},
+        {{1, 128, 64}, pair_kernel<RefAdjointBody<D, 1>, 128, 64>},
+        {{1, 256, 64}, pair_kernel<RefAdjointBody<D, 1>, 256, 64>},
+        {{2, 256, 32}, pair_kernel<RefAdjointBody<D, 2>, 256, 32>},
+    };
+    return v;
+}
+
+template <int D>
+static const std::vector<Variant>& energy_variants()
+{
+    static const std::vector<Variant> v = {
+        {{4, 128, 64}, pair_kernel<RefEnergyBody<D, 4>, 128, 64>},
+        {{2, 128, 64}, pair_kernel<RefEnergyBody<D, 2>, 128, 64>},
+        {{2, 256, 64}, pair_kernel<RefEnergyBody<D, 2>, 256, 64>},
+        {{4, 256, 32}, pair_kernel<RefEnergyBody<D, 4>, 256, 32>},
+    };
+    return v;
+}
+
+std::vector<KernelShape> adjoint_shapes()
+{
+    std::vector<KernelShape> s;
+    for (auto& v : adjoint_variants<3>()) s.push_back(v.shape);
+    return s;
+}
+std::vector<KernelShape> energy_shapes()
+{
+    std::vector<KernelShape> s;
+    for (auto& v : energy_variants<3>()) s.push_back(v.shape);
+    return s;
+}
+
+int conv_launch(Context& c, const double* pose_dev, bool grad, int i0, int i1, double* out_dev, double* dEdx_dev,
+                cudaStream_t s, const KernelShape* force);   // conv.cu
+
+static int occupancy_blocks(KernelFn fn, int nt)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<KernelFn, int>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& e : cache)
+        if (e.first == fn) return e.second;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, nt, 0) != cudaSuccess || nb < 1) nb = 1;
+    cache.push_back({fn, nb});
+    return nb;
+}
+
+// Splits [i0, i1) x targets into items and launches `fn`, then the reductions.
+int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
+                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
+                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
+                        cudaStream_t s)
+{
+    const int rows = i1 - i0;
+    const int BI = sh.ipt * sh.nt;
+    const int n_ib = (rows + BI - 1) / BI;
+    const int total_tiles = (int)(yrec_size / sh.tj);
+    const int resident = c.num_sms * occupancy_blocks(fn, sh.nt);
+    const int target = 4 * resident;
+    int n_jc = std::max(1, std::min(total_tiles, (target + n_ib - 1) / n_ib));
+    const int jc_tiles = (total_tiles + n_jc - 1) / n_jc;
+    n_jc = (total_tiles + jc_tiles - 1) / jc_tiles;
+    const int n_items = n_ib * n_jc;
+    size_t need = sizeof(double) * (size_t)n_items * 8;
+    const size_t dx_off = need;
+    if (dEdx_dev) need += sizeof(double) * (size_t)n_jc * rows * c.D;
+    const size_t h_off = need;
+    if (h_part) need += sizeof(double) * (size_t)n_jc * rows * h_width;
+    DUGMA_RET(c.ensure_scratch(need));
+    PairArgs a{};
+    a.xrec = xrec;
+    a.yrec = yrec;
+    a.wx = c.wx;
+    a.wy = c.wy;
+    a.xcov = c.xcov;
+    a.pose = pose_dev;
+    a.Lmax = Lmax;
+    a.N = c.N;
+    a.i0 = i0;
+    a.i_end = i1;
+    a.n_ib = n_ib;
+    a.n_jc = n_jc;
+    a.jc_tiles = jc_tiles;
+    a.total_tiles = total_tiles;
+    a.partials = c.scratch;
+    a.dx_part = dEdx_dev ? reinterpret_cast<double*>(reinterpret_cast<char*>(c.scratch) + dx_off) : nullptr;
+    a.h_part = h_part ? reinterpret_cast<double*>(reinterpret_cast<char*>(c.scratch) + h_off) : nullptr;
+    a.counter = c.counter;
+    a.err = c.err;
+    if (h_part) *h_part = a.h_part;
+    if (n_jc_out) *n_jc_out = n_jc;
+    DUGMA_CK(cudaMemsetAsync(c.counter, 0, sizeof(int), s));
+    const int grid = std::min(resident, n_items);
+    cudaEvent_t ev1 = nullptr;
+    if (c.timing) {
+        if (c.tused == c.tevents.size()) {
+            cudaEvent_t e0, e1;
+            DUGMA_CK(cudaEventCreate(&e0));
+            DUGMA_CK(cudaEventCreate(&e1));
+            c.tevents.push_back({e0, e1});
+        }
+        DUGMA_CK(cudaEventRecord(c.tevents[c.tused].first, s));
+        ev1 = c.tevents[c.tused].second;
+        ++c.tused;
+    }
+    fn<<<grid, sh.nt, 0, s>>>(a);
+    DUGMA_CK(cudaGetLastError());
+    if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
+    if (out_dev) {
+        reduce_items_kernel<<<1, 256, 0, s>>>(a.partials, n_items, nv, out_dev);
+        DUGMA_CK(cudaGetLastError());
+    }
+    if (dEdx_dev) {
+        const size_t n = (size_t)rows * c.D;
+        const int g = (int)std::min<size_t>((n + 255) / 256, (size_t)c.num_sms * 8);
+        reduce_chunks_kernel<<<g, 256, 0, s>>>(a.dx_part, n_jc, n, dEdx_dev);
+        DUGMA_CK(cudaGetLastError());
+    }
+    return DUGMA_OK;
+}
+
+int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1, double* out_dev,
+                 double* dEdx_dev, cudaStream_t s, const KernelShape* force)
+{
+    if (i0 < 0 || i1 > c.N || i0 >= i1) return set_error(DUGMA_ERR_ARG, "bad source row range [%d, %d)", i0, i1);
+    if (model == DUGMA_MODEL_CONV) return conv_launch(c, pose_dev, grad, i0, i1, out_dev, dEdx_dev, s, force);
+    if (model != DUGMA_MODEL_REF) return set_error(DUGMA_ERR_ARG, "unknown model %d", model);
+    DUGMA_RET(launch_prologue(c, pose_dev, grad ? 0 : 1, s));
+    const KernelShape want = force ? *force : (grad ? c.shape_adj : c.shape_energy);
+    const std::vector<Variant>& vars =
+        c.D == 3 ? (grad ? adjoint_variants<3>() : energy_variants<3>()) : (grad ? adjoint_variants<2>() : energy_variants<2>());
+    const Variant* v = &vars[0];
+    for (auto& cand : vars)
+        if (cand.shape.ipt == want.ipt && cand.shape.nt == want.nt && cand.shape.tj == want.tj) v = &cand;
+    const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
+    return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad, nv, c.Lmax_y, pose_dev, i0, i1,
+                               out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
+}
+
+}  // namespace dugma

@@ -1,0 +1,285 @@
+// prepare.cu -- init-time and per-evaluation prologue kernels.
+//
+// This file is compiled with -fmad=false: every FP64 expression below is evaluated
+// as written (no fused multiply-add), so the FP32 state written by init and the
+// FP32 rounding of y' match the CPU oracle bit for bit.
+#include <cmath>
+#include <cstdio>
+
+#include "context.hpp"
+
+namespace dugma {
+
+// ---------------------------------------------------------------------------
+// init: FP64 -> FP32 conversion (init.cu:192-234) fused with the per-point inverse
+// covariance and |Sigma|^-1/2 (init.cu:22-190).  The inverse is evaluated in FP64 from
+// the FP32-rounded covariance by the adjugate, in the order of the reference's formula,
+// and rounded to FP32.  det <= 0: all entries 1e5, weight 0 (init.cu:48-57, 86-100).
+// Also writes the packed symmetric FP32 covariance used by the CONV model.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void init_points_kernel(const double* __restrict__ P, const double* __restrict__ C, int n,
+                                   float* __restrict__ p32, float* __restrict__ cinv,
+                                   float* __restrict__ w, float* __restrict__ cpack, int* nonpd)
+{
+    constexpr int NS = Sym<D>::N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) p32[(size_t)i * D + a] = __double2float_rn(P[(size_t)i * D + a]);
+        double a_[D * D];
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) a_[k] = (double)__double2float_rn(C[(size_t)i * D * D + k]);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+            cpack[(size_t)i * NS + k] = __double2float_rn(0.5 * (a_[ra + D * rb] + a_[rb + D * ra]));
+        }
+        float* o = cinv + (size_t)i * D * D;
+        if (D == 3) {
+            const double a11 = a_[0], a21 = a_[1], a31 = a_[2], a12 = a_[3], a22 = a_[4], a32 = a_[5],
+                         a13 = a_[6], a23 = a_[7], a33 = a_[8];
+            const double d = a11 * a22 * a33 - a11 * a23 * a32 - a12 * a21 * a33 + a12 * a23 * a31 +
+                             a13 * a21 * a32 - a13 * a22 * a31;
+            if (d > 0) {
+                o[0] = __double2float_rn((a22 * a33 - a23 * a32) / d);
+                o[1] = __double2float_rn(-(a21 * a33 - a23 * a31) / d);
+                o[2] = __double2float_rn((a21 * a32 - a22 * a31) / d);
+                o[3] = __double2float_rn(-(a12 * a33 - a13 * a32) / d);
+                o[4] = __double2float_rn((a11 * a33 - a13 * a31) / d);
+                o[5] = __double2float_rn(-(a11 * a32 - a12 * a31) / d);
+                o[6] = __double2float_rn((a12 * a23 - a13 * a22) / d);
+                o[7] = __double2float_rn(-(a11 * a23 - a13 * a21) / d);
+                o[8] = __double2float_rn((a11 * a22 - a12 * a21) / d);
+                w[i] = __double2float_rn(sqrt(1.0 / d));
+            } else {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) o[k] = 100000.0f;
+                w[i] = 0.0f;
+                atomicAdd(nonpd, 1);
+            }
+        } else {
+            const double a1 = a_[0], a2 = a_[1], a3 = a_[2], a4 = a_[3];
+            const double d = a1 * a4 - a2 * a3;
+            if (d > 0) {
+                o[0] = __double2float_rn(a4 / d);
+                o[1] = __double2float_rn(-a2 / d);
+                o[2] = __double2float_rn(-a3 / d);
+                o[3] = __double2float_rn(a1 / d);
+                w[i] = __double2float_rn(sqrt(1.0 / d));
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) o[k] = 100000.0f;
+                w[i] = 0.0f;
+                atomicAdd(nonpd, 1);
+            }
+        }
+    }
+}
+
+// max_i log2(w_i) over positive weights (single block, fixed reduction order)
+__global__ void max_log2_kernel(const float* __restrict__ w, int n, double* out)
+{
+    __shared__ double red[1024];
+    double m = -INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (w[i] > 0.0f) m = fmax(m, log2((double)w[i]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+__global__ void norm_log2_kernel(const float* __restrict__ w, int n, const double* Lmax, float* __restrict__ lw)
+{
+    const double L = *Lmax;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        lw[i] = w[i] > 0.0f ? __double2float_rn(log2((double)w[i]) - L) : -INFINITY;
+}
+
+int launch_init(Context& c, const double* X, const double* XC, const double* Y, const double* YC)
+{
+    const int D = c.D, N = c.N, M = c.M;
+    const size_t nd = (size_t)N * D, md = (size_t)M * D;
+    const size_t bytes = sizeof(double) * (nd + nd * D + md + md * D);
+    double* tmp = nullptr;
+    DUGMA_CK(cudaMalloc(&tmp, bytes));
+    double *tX = tmp, *tXC = tX + nd, *tY = tXC + nd * D, *tYC = tY + md;
+    cudaStream_t s = c.stream;
+    int rc = DUGMA_OK;
+    auto ck = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && rc == DUGMA_OK)
+            rc = set_error(DUGMA_ERR_CUDA, "init: %s failed: %s", what, cudaGetErrorString(e));
+    };
+    ck(cudaMemcpyAsync(tX, X, sizeof(double) * nd, cudaMemcpyHostToDevice, s), "copy X");
+    ck(cudaMemcpyAsync(tXC, XC, sizeof(double) * nd * D, cudaMemcpyHostToDevice, s), "copy X_C");
+    ck(cudaMemcpyAsync(tY, Y, sizeof(double) * md, cudaMemcpyHostToDevice, s), "copy Y");
+    ck(cudaMemcpyAsync(tYC, YC, sizeof(double) * md * D, cudaMemcpyHostToDevice, s), "copy Y_C");
+    ck(cudaMemsetAsync(c.counter, 0, sizeof(int) * 8, s), "memset");
+    const int bs = 256;
+    const int gx = std::min((N + bs - 1) / bs, c.num_sms * 8), gy = std::min((M + bs - 1) / bs, c.num_sms * 8);
+    double* Lm = c.out;   // scratch: out[0], out[1]
+    if (D == 3) {
+        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, c.counter);
+        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, c.counter);
+    } else {
+        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, c.counter);
+        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, c.counter);
+    }
+    max_log2_kernel<<<1, 1024, 0, s>>>(c.wx, N, Lm);
+    max_log2_kernel<<<1, 1024, 0, s>>>(c.wy, M, Lm + 1);
+    norm_log2_kernel<<<gx, bs, 0, s>>>(c.wx, N, Lm, c.lwx);
+    norm_log2_kernel<<<gy, bs, 0, s>>>(c.wy, M, Lm + 1, c.lwy);
+    ck(cudaGetLastError(), "init kernels");
+    ck(cudaMemcpyAsync(c.host, Lm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax");
+    ck(cudaMemcpyAsync(c.host + 2, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
+    ck(cudaStreamSynchronize(s), "sync");
+    cudaFree(tmp);
+    if (rc != DUGMA_OK) return rc;
+    c.Lmax_x = std::isfinite(c.host[0]) ? c.host[0] : 0.0;
+    c.Lmax_y = std::isfinite(c.host[1]) ? c.host[1] : 0.0;
+    int nonpd = 0;
+    memcpy(&nonpd, c.host + 2, sizeof(int));
+    c.nonpd = nonpd;
+    return DUGMA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Per-evaluation prologue.
+//   y records: y' = R y + t in FP64 in the order of update_sig.cu:247-249 / compi.cu:784-786,
+//              split into y'hi = float(y'), y'lo = float(y' - y'hi);
+//              C'_j = R (s sym(Sigma_y_j^-1)) R^T (compi.cu:757-765) scaled by k = -1/2 log2 e
+//              (layout 0: packed as is; layout 1: off-diagonals doubled for the Horner form);
+//              lv_j = log2(w_j) - Lmax_y.
+//   x records: x_i, lw_i, k * s * sym(Sigma_x_i^-1) with doubled off-diagonals.
+// Rows past N / M are null records (lw = -inf, zero matrices): they contribute exactly 0.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
+                                const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
+                                int ylayout, YRec* __restrict__ yrec, float4* __restrict__ yp32,
+                                const float* __restrict__ x, const float* __restrict__ xinv,
+                                const float* __restrict__ lwx, int N, int N_pad, XRec* __restrict__ xrec)
+{
+    constexpr int NS = Sym<D>::N;
+    double R[9], t[3];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+#pragma unroll
+    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
+    const double s = 1.0 / pose[kPoseSig];
+    const double ks = K_EXP2 * s;
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
+        YRec r;
+        float hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, cp[6] = {0, 0, 0, 0, 0, 0};
+        float lv = -INFINITY;
+        if (j < M) {
+            double yj[3];
+#pragma unroll
+            for (int a = 0; a < D; ++a) yj[a] = (double)y[(size_t)j * D + a];
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double v = R[a] * yj[0] + R[a + D] * yj[1];
+                if (D == 3) v = v + R[a + 6] * yj[2];
+                v = v + t[a];
+                hi[a] = __double2float_rn(v);
+                lo[a] = __double2float_rn(v - (double)hi[a]);
+            }
+            lv = lwy[j];
+            if (lv != -INFINITY) {
+                double A[D][D];
+#pragma unroll
+                for (int r0 = 0; r0 < D; ++r0)
+#pragma unroll
+                    for (int c0 = 0; c0 < D; ++c0)
+                        A[r0][c0] = 0.5 * ((double)yinv[(size_t)j * D * D + r0 + D * c0] +
+                                           (double)yinv[(size_t)j * D * D + c0 + D * r0]);
+                double T[D][D];   // A R^T
+#pragma unroll
+                for (int r0 = 0; r0 < D; ++r0)
+#pragma unroll
+                    for (int c0 = 0; c0 < D; ++c0) {
+                        double acc = 0;
+#pragma unroll
+                        for (int k = 0; k < D; ++k) acc = acc + A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = acc;
+                    }
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    double acc = 0;
+#pragma unroll
+                    for (int q = 0; q < D; ++q) acc = acc + R[ra + D * q] * T[q][rb];
+                    double v = ks * acc;
+                    if (ylayout == 1 && ra != rb) v = 2.0 * v;
+                    cp[k] = __double2float_rn(v);
+                }
+            }
+        }
+        r.v0 = make_float4(hi[0], hi[1], hi[2], lv);
+        r.v1 = make_float4(lo[0], lo[1], lo[2], 0.f);
+        if (D == 3) {
+            r.v2 = make_float4(cp[0], cp[1], cp[2], cp[3]);
+            r.v3 = make_float4(cp[4], cp[5], 0.f, 0.f);
+        } else {
+            r.v2 = make_float4(cp[0], cp[1], cp[2], 0.f);
+            r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        yrec[j] = r;
+        // padding targets sit at +inf so that no source ever picks them as a neighbour
+        if (yp32)
+            yp32[j] = j < M ? make_float4(hi[0], hi[1], hi[2], 0.f)
+                            : make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
+        XRec r;
+        float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
+        float lw = -INFINITY;
+        if (i < N) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) xv[a] = x[(size_t)i * D + a];
+            lw = lwx[i];
+            if (lw != -INFINITY) {
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
+                                      (double)xinv[(size_t)i * D * D + rb + D * ra]);
+                    double v = ks * b;
+                    if (ra != rb) v = 2.0 * v;
+                    bp[k] = __double2float_rn(v);
+                }
+            }
+        }
+        r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+        r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (D == 3) {
+            r.v2 = make_float4(bp[0], bp[1], bp[2], bp[3]);
+            r.v3 = make_float4(bp[4], bp[5], 0.f, 0.f);
+        } else {
+            r.v2 = make_float4(bp[0], bp[1], bp[2], 0.f);
+            r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        xrec[i] = r;
+    }
+}
+
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s)
+{
+    const int n = std::max(c.M_pad, c.N_pad);
+    const int bs = 256;
+    const int g = std::min((n + bs - 1) / bs, c.num_sms * 4);
+    if (c.D == 3)
+        prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec);
+    else
+        prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
+}  // namespace dugma

@@ -132,11 +132,11 @@ def _move(rng, S, max_angle_deg, tmax, noise):
     return Y, R_G, t_G
 
 
-def workload0(trial: int = 0) -> Problem:
+def workload0(trial: int = 0, n: int = 1000) -> Problem:
     """1000 x 1000 bumpy sphere, diag sensor-frame covariances from 8-NN spacing."""
     rng = rng_for(0, trial)
-    X = bumpy_sphere(rng, 1000)
-    S = bumpy_sphere(rng, 1000)
+    X = bumpy_sphere(rng, n)
+    S = bumpy_sphere(rng, n)
     Y, R_G, t_G = _move(rng, S, 60.0, 0.3, 0.01)
     return Problem(X, Y, _sensor_diag_cov(X), _sensor_diag_cov(Y), R_G, t_G, "sphere1k")
 

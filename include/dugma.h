@@ -1,0 +1,171 @@
+/*
+ * dugma.h -- C ABI of libdugma_b200.so, the B200 (sm_100a) implementation of the
+ * DUGMA registration hot path (Canpu999/DUGMA: init.cu, update_sig.cu, compi.cu,
+ * fr_m.cu and their MEX gateways).
+ *
+ * Data layout (the MATLAB layout the reference's MEX gateways pass through):
+ *   X, Y      D x N column-major doubles   = N points, D coordinates each, contiguous
+ *   X_C, Y_C  D x (D*N) column-major doubles = one D x D column-major block per point
+ *   R         D x D column-major doubles, applied to Y: y' = R y + t
+ *   Ptr[6]    device pointers {x, x_cov_inv, y, y_cov_inv, det_x, det_y} (FP32), the
+ *             reference's device state after init (init.cu:326-331); Ptr[4], Ptr[5]
+ *             hold |Sigma|^-1/2 per point.
+ * Every call returns a status (DUGMA_OK = 0) instead of exiting the process;
+ * dugma_last_error() describes the last failure on the calling thread.
+ * Pose gradients are g = [dE/domega (NR), dE/dt (D)] with the left perturbation
+ * R <- exp([omega]x) R, t <- t + dt; NR = 3 in 3D, 1 in 2D.
+ */
+#ifndef DUGMA_H
+#define DUGMA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  They are also the bit positions of the device error word. */
+enum {
+    DUGMA_OK = 0,
+    DUGMA_ERR_ARG = 1,     /* bad argument: sizes, D, null pointer, unknown context */
+    DUGMA_ERR_CUDA = 2,    /* a CUDA runtime call failed */
+    DUGMA_ERR_NONPD = 3,   /* warning: some covariances had det <= 0 and were neglected */
+    DUGMA_ERR_TIMEOUT = 4, /* a bounded device wait gave up */
+    DUGMA_ERR_NOMEM = 5,   /* device allocation failed */
+    DUGMA_ERR_NUMERIC = 6, /* non-finite result */
+    DUGMA_ERR_STATE = 7    /* call out of order (e.g. graph replay of a released graph) */
+};
+
+/* Per-pair models. */
+enum {
+    DUGMA_MODEL_REF = 0, /* the reference: w_i v_j [exp(-d'C'd/2) + exp(-d'Bd/2)] (compi.cu:753-772) */
+    DUGMA_MODEL_CONV = 1 /* convolved GMM: N(d; 0, sig (R Sy R' + Sx)) with its own 3x3 inverse */
+};
+
+/* Largest supported cloud size (the reference stops at 3e6 points, compi.cu:535). */
+#define DUGMA_MAX_POINTS 16777216
+
+/* ---------------- reference entry points (C linkage) ---------------- */
+
+/* Replaces init(X, X_C, Y, Y_C, Coef, N, M, D, Ptr) (init.cu:249-259, bound by init.cpp:9-19):
+ * uploads both clouds, inverts each covariance, stores |Sigma|^-1/2; *Coef = 1 on success.
+ * A covariance with det <= 0 is neglected exactly as init.cu:48-57 does (entries 1e5, weight 0)
+ * and the call returns DUGMA_ERR_NONPD (a warning; the state is usable). */
+int dugma_init(const double* X, const double* X_C, const double* Y, const double* Y_C,
+               double* Coef, int N, int M, int D, float* Ptr[6]);
+
+/* Replaces cpd(Ptr, R, t, N, M, D, float sig[1]) of update_sig.cu:319-321 (update_sig.cpp:7):
+ * sig = mean_i min_j |x_i - (R y_j + t)|^2 / D, with the reference's 1e-6 quantisation. */
+int dugma_update_sig(float* Ptr[6], const double* R, const double* t, const double* N,
+                     const double* M, const double* D, float sig[1]);
+
+/* Replaces cpd(Ptr, R, t, N, M, D, sig, double coefficient[640]) of compi.cu:511-513
+ * (compi.cpp:7): the 637 (3D) / 45 (2D) surrogate coefficients in the energy3D.m /
+ * energy2D.m monomial order; the remaining slots of the 640 are zero. */
+int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N,
+                const double* M, const double* D, const double* sig, double coefficient[640]);
+
+/* Replaces fr_m(Ptr) (fr_m.cu:14-16): frees the six buffers and the context behind them.
+ * Unlike the reference it does not call cudaDeviceReset (that would destroy every other
+ * allocation of the process). */
+int dugma_fr_m(float* Ptr[6]);
+
+/* Message for the last non-OK status on this thread. */
+const char* dugma_last_error(void);
+
+/* ---------------- energy, adjoint, nearest neighbours ---------------- */
+
+/* E(R, t) = sum_ij P_ij for `model`; sig is sigma-bar (update_sig output). */
+int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, int model, double* E);
+
+/* Fused adjoint: E and g (NR + D doubles) in one pass; dEdx (N*D doubles, nullable) = dE/dx_i. */
+int dugma_energy_grad(float* Ptr[6], const double* R, const double* t, double sig, int model,
+                      double* E, double* g, double* dEdx);
+
+/* Same over source rows [i_begin, i_end) only (partial sums, for sharding the rows across GPUs). */
+int dugma_energy_grad_range(float* Ptr[6], const double* R, const double* t, double sig, int model,
+                            int i_begin, int i_end, double* E, double* g);
+
+/* The plain form: E plus central finite differences of step h over the NR + D pose
+ * coordinates (1 + 2 (NR + D) energy evaluations). */
+int dugma_energy_fd_grad(float* Ptr[6], const double* R, const double* t, double sig, int model,
+                         double h, double* E, double* g);
+
+/* k (1..16) nearest targets of every source point: idx (N*k, ascending distance, ties to the
+ * lowest index) and squared distances d2 (N*k FP32, exactly
+ * fmaf(dz,dz, fmaf(dy,dy, dx*dx)) with y' = float(FP64(R y + t))). */
+int dugma_nn(float* Ptr[6], const double* R, const double* t, int k, int* idx, float* d2);
+
+/* sigma without quantisation (FP64 sum of the exact nearest squared distances / (D N)). */
+int dugma_sigma(float* Ptr[6], const double* R, const double* t, double* sig);
+
+/* ---------------- asynchronous device-side form (CUDA graphs, torch harness) ---------------- */
+
+/* pose_dev: 16 doubles on the device {R (D*D col-major), pad to 9, t (3, 2D uses 2), sig}
+ * laid out as R[0..8], t[9..11], sig[12]; out_dev: 1 + NR + D doubles on the device;
+ * dEdx_dev: N*D doubles on the device or NULL.  Work is enqueued on `stream`
+ * (a cudaStream_t, NULL = the context's stream) and the call returns without synchronising. */
+int dugma_energy_grad_async(float* Ptr[6], const double* pose_dev, int model, double* out_dev,
+                            double* dEdx_dev, void* stream);
+int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double* out_dev, void* stream);
+
+/* ---------------- tuning and graphs ---------------- */
+
+/* Times the kernel shapes of `what` (0 = adjoint, 1 = energy, 2 = nearest neighbour) on this
+ * context and keeps the fastest; writes a one-line report into `report` (may be NULL). */
+int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t report_len);
+
+/* Captures one energy+gradient evaluation (prologue, pair kernel, reduction) as a CUDA graph
+ * reading its pose from the context's pose buffer; dugma_graph_eval replays it for a new
+ * pose and returns E and g. */
+int dugma_graph_create(float* Ptr[6], int model, void** graph);
+int dugma_graph_eval(void* graph, const double* R, const double* t, double sig, double* E, double* g);
+int dugma_graph_destroy(void* graph);
+
+/* ---------------- batched problems ---------------- */
+
+/* Many independent registration problems of uneven sizes in one persistent launch.
+ * Problem p has N[p] source and M[p] target points; X[p], X_C[p], Y[p], Y_C[p] as in dugma_init. */
+int dugma_batch_create(int n_problems, int D, const int* N, const int* M, const double* const* X,
+                       const double* const* X_C, const double* const* Y, const double* const* Y_C,
+                       void** batch);
+/* poses: n_problems * n_poses records of 13 doubles {R (9, col-major), t (3), sig};
+ * out: n_problems * n_poses * (1 + NR + D) doubles {E, g}. */
+int dugma_batch_energy_grad(void* batch, int n_poses, const double* poses, int model, double* out);
+int dugma_batch_destroy(void* batch);
+
+/* ---------------- registration driver ---------------- */
+
+enum {
+    DUGMA_DRIVE_REFERENCE = 0, /* DUGMA.m loop: compi -> minimise the surrogate on SO(D) -> update sig */
+    DUGMA_DRIVE_DIRECT = 1     /* maximise E(R, t) with the fused adjoint, sig annealed by update_sig */
+};
+
+/* The registration loop of DUGMA.m:19-137 with a quasi-Newton solver in place of fmincon.
+ * Inputs as dugma_init plus the initial pose (R0, t0) and the stopping rules of DUGMA.m:57.
+ * Writes the final pose (denormalised, DUGMA.m:122) and stats[8] =
+ * {iterations, final sigma, final energy, exit flag, seconds, evaluations, 0, 0}. */
+int dugma_register(const double* X, const double* X_C, const double* Y, const double* Y_C, int N,
+                   int M, int D, const double* R0, const double* t0, int max_iter,
+                   double acc_rot, double acc_trans, double acc_sig, int mode, double* R_out,
+                   double* t_out, double* stats);
+
+/* ---------------- measurement ---------------- */
+
+/* Records CUDA events around every launch of the main pairwise kernel on this context
+ * (mode 1: start and clear, 0: stop, 2: synchronise and return the summed duration in ms
+ * and the number of launches since mode 1). */
+int dugma_timing(float* Ptr[6], int mode, double* total_ms, int* launches);
+
+/* Measured peak of a GPU pipe on the current device: what = 0 FP32 fused multiply-add,
+ * 1 SFU ex2; returns lane operations per second (and the kernel time in ms). */
+int dugma_calibrate(int what, double* lane_ops_per_s, double* ms);
+
+/* Library build/version string. */
+const char* dugma_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DUGMA_H */

@@ -1,0 +1,65 @@
+"""The C-ABI library loads and exports every entry point its headers declare (no GPU needed).
+
+include/dugma.h declares the extern "C" surface; include/dugma_mex.hpp declares
+the reference's four C++ entry points (init, cpd x2, fr_m) with their exact
+signatures, which must be exported under their C++ mangled names so that the
+reference's MEX gateways (init.cpp:9-19, update_sig.cpp:7, compi.cpp:7,
+fr_m.cpp:7) link against the library unchanged."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from dugma_b200 import _lib, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _exported():
+    path = build.build()
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_c_symbols_exported_and_bound():
+    hdr = open(os.path.join(ROOT, "include", "dugma.h")).read()
+    declared = set(re.findall(r"^\s*(?:int|const char\*)\s+(dugma_\w+)\s*\(", hdr, re.M))
+    assert len(declared) >= 20
+    syms = _exported()
+    missing = declared - syms
+    assert not missing, missing
+    # every declared function has a ctypes binding with an argtypes list
+    assert declared <= set(_lib.EXPORTS)
+    L = _lib.load()
+    for name in declared:
+        assert getattr(L, name).argtypes is not None
+
+
+def test_reference_cpp_signatures_exported():
+    syms = _exported()
+    # Itanium mangling of the reference's four functions
+    want = {
+        "_Z4initPdS_S_S_S_iiiPPf",          # void init(double*, double*, double*, double*, double*, int, int, int, float**)
+        "_Z3cpdPPfPdS1_S1_S1_S1_S_",        # void cpd(float**, double*, double*, double*, double*, double*, float*)
+        "_Z3cpdPPfPdS1_S1_S1_S1_S1_S1_",    # void cpd(float**, double* x7)
+        "_Z4fr_mPPf",                       # void fr_m(float**)
+    }
+    assert want <= syms, want - syms
+
+
+def test_version_string():
+    assert b"sm_100a" in _lib.load().dugma_version()
+
+
+def test_errors_are_returned_not_fatal():
+    """Bad arguments come back as status codes with a message (the reference exit()s)."""
+    import ctypes
+    L = _lib.load()
+    ptrs = _lib.PtrArray()
+    rc = L.dugma_fr_m(ptrs)
+    assert rc == _lib.ERR_ARG
+    assert b"context" in L.dugma_last_error()
+    coef = ctypes.c_double(5)
+    rc = L.dugma_init(None, None, None, None, ctypes.byref(coef), 10, 10, 3, ptrs)
+    assert rc == _lib.ERR_ARG and coef.value == 0

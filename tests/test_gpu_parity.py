@@ -1,0 +1,270 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 CPU oracle.
+
+Tolerances (written per assertion):
+  * init state (inverse covariances, |Sigma|^-1/2, FP32 coordinates): bit-exact;
+  * nearest-neighbour indices and squared distances: bit-exact (same FP32 sequence);
+  * sigma: bit-exact against the oracle's quantised and exact forms;
+  * energy: relative 1e-6; pose gradient: relative 1e-5 (norm-wise) on
+    well-conditioned covariances (1K sphere, 64K harmonic surface); the 6K
+    workload's noise-free source has covariances of condition up to ~7e3,
+    where FP32 per-pair arithmetic is good to ~3e-4 (its own assertion);
+  * surrogate coefficients: |A - A_oracle| <= 2e-6 max|A_oracle|.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from dugma_b200 import api, synth
+from dugma_b200.pose import expmap, rot2d
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem_small(D, n, m, seed=0, bad=(), dup=()):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, D)) * 0.5
+    R0 = expmap(rng.standard_normal(3) * 0.3) if D == 3 else rot2d(0.4)
+    Y = (X[np.arange(m) % n] - 0.1) @ R0 + rng.standard_normal((m, D)) * 0.05
+    for (a, b) in dup:
+        Y[a] = Y[b]
+
+    def covs(k):
+        A = rng.standard_normal((k, D, D)) * 0.1
+        return A @ np.transpose(A, (0, 2, 1)) + 0.01 * np.eye(D)
+
+    XC, YC = covs(n), covs(m)
+    for i in bad:
+        XC[i] = np.diag([-1.0] + [1.0] * (D - 1))
+        if i < m:
+            YC[i] = np.diag([1.0] * (D - 1) + [-2.0])
+    return X, XC, Y, YC
+
+
+def _pose(D, seed=1, scale=0.2):
+    rng = np.random.default_rng(seed)
+    if D == 3:
+        return expmap(rng.standard_normal(3) * scale), rng.standard_normal(3) * 0.05
+    return rot2d(scale), rng.standard_normal(2) * 0.05
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def w0():
+    P = synth.workload0()
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    yield P, st, h
+    api.fr_m(h)
+
+
+# ---------------------------------------------------------------- init
+@pytest.mark.parametrize("D", [3, 2])
+def test_init_state_bit_exact(D):
+    X, XC, Y, YC = _problem_small(D, 300, 257, bad=(4, 9))
+    st = orc.State(X, XC, Y, YC)
+    with pytest.warns(UserWarning):
+        _, h = api.init(X, XC, Y, YC)
+    try:
+        # read the six device buffers back through the library's own sizes
+        got = _read_state(h)
+        assert np.array_equal(got["x"], st.x.reshape(-1))
+        assert np.array_equal(got["y"], st.y.reshape(-1))
+        assert np.array_equal(got["xinv"], np.transpose(st.xinv, (0, 2, 1)).reshape(-1))
+        assert np.array_equal(got["yinv"], np.transpose(st.yinv, (0, 2, 1)).reshape(-1))
+        assert np.array_equal(got["wx"], st.wx)
+        assert np.array_equal(got["wy"], st.wy)
+        assert np.all(got["wx"][[4, 9]] == 0)
+    finally:
+        api.fr_m(h)
+
+
+def _read_state(h):
+    """Copy the six device buffers of a context back through torch (__cuda_array_interface__)."""
+    import torch
+    N, M, D = h.N, h.M, h.D
+    sizes = {"x": N * D, "xinv": N * D * D, "y": M * D, "yinv": M * D * D, "wx": N, "wy": M}
+    out = {}
+    for k, (name, n) in enumerate(sizes.items()):
+        out[name] = _device_f32(h.ptrs[k], n)
+    return out
+
+
+class _DevArray:
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+
+def _device_f32(ptr, n):
+    import torch
+    return torch.as_tensor(_DevArray(ptr, n), device="cuda").cpu().numpy().copy()
+
+
+# ---------------------------------------------------------------- nearest neighbours / sigma
+@pytest.mark.parametrize("D,k", [(3, 1), (3, 8), (2, 1), (2, 16)])
+def test_nn_bit_exact_with_ties(D, k):
+    X, XC, Y, YC = _problem_small(D, 1500, 1300, seed=3, dup=((700, 5), (1299, 5), (900, 901)))
+    st = orc.State(X, XC, Y, YC)
+    _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D)
+        idx, d2 = api.nn(h, R, t, k)
+        oi, od = st.nn(R, t, k)
+        assert np.array_equal(idx, oi)
+        assert np.array_equal(d2, od)
+    finally:
+        api.fr_m(h)
+
+
+def test_sigma_matches_oracle(w0):
+    P, st, h = w0
+    for (R, t) in [(np.eye(3), np.zeros(3)), _pose(3, 5)]:
+        s_ref = api.update_sig(h, R, t)
+        assert s_ref == np.float32(st.sigma(R, t, quantised=True))
+        assert api.sigma(h, R, t) == st.sigma(R, t, quantised=False)
+
+
+# ---------------------------------------------------------------- energy and adjoint
+def _check_energy(h, st, R, t, sig, e_tol, g_tol):
+    E, g, dx = api.energy_grad(h, R, t, sig, with_dx=True)
+    Eo, go, dxo = st.energy(R, t, sig, with_dx=True)
+    assert abs(E - Eo) <= e_tol * abs(Eo), (E, Eo)
+    assert _rel(g, go) <= g_tol, (g, go)
+    assert _rel(dx, dxo) <= g_tol * 10, _rel(dx, dxo)
+    Ep = api.energy(h, R, t, sig)
+    assert abs(Ep - Eo) <= e_tol * abs(Eo), (Ep, Eo)
+    return E, g
+
+
+def test_energy_adjoint_workload0(w0):
+    P, st, h = w0
+    R, t = P.R_G @ expmap([0.1, -0.2, 0.05]), P.t_G + 0.02
+    sig = api.update_sig(h, R, t)
+    _check_energy(h, st, R, t, sig, 1e-6, 1e-5)
+    # the initial pose of a registration (identity), where sigma is large
+    sig0 = api.update_sig(h, np.eye(3), np.zeros(3))
+    _check_energy(h, st, np.eye(3), np.zeros(3), sig0, 1e-6, 1e-5)
+
+
+@pytest.mark.parametrize("D", [3, 2])
+@pytest.mark.parametrize("n,m", [(1, 1), (1, 300), (300, 1), (1025, 130), (77, 1031)])
+def test_energy_adjoint_ragged_sizes(D, n, m):
+    X, XC, Y, YC = _problem_small(D, n, m, seed=n + m, bad=(0,) if n > 2 and m > 2 else ())
+    st = orc.State(X, XC, Y, YC)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D, seed=7)
+        _check_energy(h, st, R, t, 0.3, 1e-6, 1e-5)
+    finally:
+        api.fr_m(h)
+
+
+def test_energy_adjoint_workload1_ill_conditioned():
+    P = synth.workload1()
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    try:
+        R, t = P.R_G @ expmap([0.05, 0.1, -0.05]), P.t_G * 0.95
+        sig = api.update_sig(h, R, t)
+        E, g, _ = api.energy_grad(h, R, t, sig)
+        Eo, go, _ = st.energy(R, t, sig)
+        print(f"workload1: energy rel err {abs(E - Eo) / Eo:.3e}, grad rel err {_rel(g, go):.3e}")
+        assert abs(E - Eo) <= 3e-4 * Eo
+        assert _rel(g, go) <= 3e-3
+    finally:
+        api.fr_m(h)
+
+
+def test_sigma_extremes(w0):
+    P, st, h = w0
+    R, t = _pose(3, 11)
+    for sig in (1e-7, 1e-3, 10.0, 1e4):
+        E, g, _ = api.energy_grad(h, R, t, sig)
+        Eo, go, _ = st.energy(R, t, sig)
+        assert np.isfinite(E) and np.all(np.isfinite(g))
+        if Eo > 0:
+            assert abs(E - Eo) <= 1e-6 * Eo + 1e-300
+        else:
+            assert E == 0
+
+
+def test_fd_grad_plain_form(w0):
+    P, st, h = w0
+    R, t = P.R_G @ expmap([0.2, 0.1, 0.0]), P.t_G
+    sig = 0.05
+    E, g = api.energy_fd_grad(h, R, t, sig, step=1e-4)
+    Eo, go, _ = st.energy(R, t, sig)
+    assert abs(E - Eo) <= 1e-6 * Eo
+    assert _rel(g, go) <= 1e-4
+
+
+def test_range_partials_sum_to_total(w0):
+    P, st, h = w0
+    R, t = _pose(3, 2)
+    E, g, _ = api.energy_grad(h, R, t, 0.05)
+    parts = [api.energy_grad_range(h, R, t, 0.05, a, b) for (a, b) in [(0, 333), (333, 334), (334, 1000)]]
+    assert abs(sum(p[0] for p in parts) - E) <= 1e-12 * E
+    assert _rel(sum(p[1] for p in parts), g) <= 1e-12
+
+
+def test_results_deterministic(w0):
+    P, st, h = w0
+    R, t = _pose(3, 4)
+    a = api.energy_grad(h, R, t, 0.05)
+    b = api.energy_grad(h, R, t, 0.05)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def test_graph_replay_matches_eager(w0):
+    P, st, h = w0
+    gr = api.Graph(h)
+    try:
+        for s in range(3):
+            R, t = _pose(3, 20 + s)
+            E1, g1 = gr(R, t, 0.05)
+            E2, g2, _ = api.energy_grad(h, R, t, 0.05)
+            assert E1 == E2 and np.array_equal(g1, g2)
+    finally:
+        gr.close()
+
+
+def test_autotune_keeps_results(w0):
+    P, st, h = w0
+    R, t = _pose(3, 9)
+    rep = api.autotune(h, 0)
+    assert "ms" in rep
+    E, g, _ = api.energy_grad(h, R, t, 0.05)
+    Eo, go, _ = st.energy(R, t, 0.05)
+    assert abs(E - Eo) <= 1e-6 * Eo and _rel(g, go) <= 1e-5
+
+
+# ---------------------------------------------------------------- coefficients (compi)
+@pytest.mark.parametrize("D", [3, 2])
+def test_compi_coefficients(D):
+    if D == 3:
+        P = synth.workload0()
+        X, XC, Y, YC = P.X, P.X_C, P.Y, P.Y_C
+        R, t = P.R_G @ expmap([0.1, 0.0, -0.1]), P.t_G
+    else:
+        X, XC, Y, YC = _problem_small(2, 700, 650, seed=5, bad=(3,))
+        R, t = _pose(2)
+    st = orc.State(X, XC, Y, YC)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, h = api.init(X, XC, Y, YC)
+    try:
+        sig = api.update_sig(h, R, t)
+        A = api.compi(h, R, t, sig=sig)
+        Ao = st.coef(R, t, sig)[: A.size]
+        err = np.abs(A - Ao).max() / np.abs(Ao).max()
+        print(f"{D}D coefficients: max |dA| / max |A| = {err:.3e}")
+        assert err <= 2e-6
+    finally:
+        api.fr_m(h)
