@@ -46,6 +46,7 @@ struct Context {
     float *xcov = nullptr, *ycov = nullptr;   // packed symmetric FP32 covariances (CONV model)
     float *lwx = nullptr, *lwy = nullptr;     // log2(w) - Lmax, -inf when neglected
     double Lmax_x = 0, Lmax_y = 0;
+    double cscale = 1.0;                      // CONV covariances are stored divided by this
     // per-evaluation records
     YRec* yrec = nullptr;
     XRec* xrec = nullptr;

@@ -20,7 +20,7 @@ struct PairArgs {
     const float* wy;       // |Sigma_y|^-1/2 per target
     const float* xcov;     // packed FP32 covariances (CONV)
     const double* pose;    // R, t, sig
-    double Lmax;           // log2 weight offset of the streamed side
+    double Lmax;           // REF: log2 weight offset of the streamed side; CONV: covariance scale
     int N;                 // number of real source rows
     int i0, i_end;         // source row range [i0, i_end)
     int n_ib, n_jc, jc_tiles, total_tiles;

@@ -20,7 +20,7 @@ namespace dugma {
 template <int D>
 __global__ void init_points_kernel(const double* __restrict__ P, const double* __restrict__ C, int n,
                                    float* __restrict__ p32, float* __restrict__ cinv,
-                                   float* __restrict__ w, float* __restrict__ cpack, int* nonpd)
+                                   float* __restrict__ w, float* __restrict__ cpack, double inv_scale, int* nonpd)
 {
     constexpr int NS = Sym<D>::N;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -32,7 +32,7 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
             const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
-            cpack[(size_t)i * NS + k] = __double2float_rn(0.5 * (a_[ra + D * rb] + a_[rb + D * ra]));
+            cpack[(size_t)i * NS + k] = __double2float_rn(0.5 * (a_[ra + D * rb] + a_[rb + D * ra]) * inv_scale);
         }
         float* o = cinv + (size_t)i * D * D;
         if (D == 3) {
@@ -121,12 +121,21 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     const int bs = 256;
     const int gx = std::min((N + bs - 1) / bs, c.num_sms * 8), gy = std::min((M + bs - 1) / bs, c.num_sms * 8);
     double* Lm = c.out;   // scratch: out[0], out[1]
+    // CONV covariances are kept divided by the mean of trace / D over both clouds
+    double tr = 0;
+    for (size_t i = 0; i < (size_t)N; ++i)
+        for (int a = 0; a < D; ++a) tr += XC[i * D * D + a * (D + 1)];
+    for (size_t i = 0; i < (size_t)M; ++i)
+        for (int a = 0; a < D; ++a) tr += YC[i * D * D + a * (D + 1)];
+    tr /= (double)D * (N + M);
+    c.cscale = (std::isfinite(tr) && tr > 0) ? tr : 1.0;
+    const double inv = 1.0 / c.cscale;
     if (D == 3) {
-        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, c.counter);
-        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, c.counter);
+        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, inv, c.counter);
+        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, inv, c.counter);
     } else {
-        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, c.counter);
-        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, c.counter);
+        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, inv, c.counter);
+        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, inv, c.counter);
     }
     max_log2_kernel<<<1, 1024, 0, s>>>(c.wx, N, Lm);
     max_log2_kernel<<<1, 1024, 0, s>>>(c.wy, M, Lm + 1);
