@@ -45,13 +45,15 @@ SFU_PER_PAIR = 2            # two ex2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fd", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shape (profiling runs)")
+    ap.add_argument("--n", type=int, default=0, help="override the cloud size (small profiling cases)")
     return ap.parse_args()
 
 
@@ -64,9 +66,9 @@ def dist_setup(n):
     return rank, world, local
 
 
-def workload(wl):
+def workload(wl, n=0):
     from dugma_b200 import synth
-    return synth.WORKLOADS[wl]()
+    return synth.WORKLOADS[wl](n=n) if n else synth.WORKLOADS[wl]()
 
 
 def eval_pose(P, rank):
@@ -94,7 +96,7 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
@@ -150,10 +152,9 @@ def run_reference(args, rank, world):
     CPU code of its own), all host threads, rank 0 only, a bounded sample of rows per step."""
     if rank != 0:
         return
-    from dugma_b200 import synth
-    P = workload(args.workload)
-    R, t = eval_pose(P, 0)
     from oracle import oracle as orc
+    P = workload(args.workload, args.n)
+    R, t = eval_pose(P, 0)
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
     _, d2 = st.nn(R, t, 1)
     sig = float(np.mean(d2) / 3.0)
@@ -192,14 +193,16 @@ def main():
     from dugma_b200 import _lib, api
     L = _lib.load(build_if_missing=False)
 
-    P = workload(args.workload)
+    P = workload(args.workload, args.n)
     R, t = eval_pose(P, rank)
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
     sig = api.update_sig(h, R, t)
-    tune = api.autotune(h, 0)
+    tune = "" if args.no_tune else api.autotune(h, 0)
     pairs = P.N * P.M
 
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: handle 0 (the legacy default stream) means 'the context stream' in the C ABI
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     pose = torch.zeros(16, dtype=torch.float64, device="cuda")
     pose[:9] = torch.tensor(np.asarray(R).T.reshape(-1))
     pose[9:12] = torch.tensor(t)
@@ -279,14 +282,24 @@ def main():
         api.energy_grad(h2, R, t, sig)
         api.fr_m(h2)
         ksteps = max(3, min(args.steps, 10))
+        ph = [0.0, 0.0, 0.0]
         t0 = time.perf_counter()
         for _ in range(ksteps):
+            a = time.perf_counter()
             _, h2 = api.init(P.X, X_C, P.Y, Y_C)
+            b = time.perf_counter()
             api.energy_grad(h2, R, t, sig)
+            c = time.perf_counter()
             api.fr_m(h2)
+            d = time.perf_counter()
+            ph[0] += b - a
+            ph[1] += c - b
+            ph[2] += d - c
         el = time.perf_counter() - t0
         e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps}
+               "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps,
+               "ms_per_step": {"init": 1e3 * ph[0] / ksteps, "energy_grad": 1e3 * ph[1] / ksteps,
+                               "fr_m": 1e3 * ph[2] / ksteps}}
 
     cpu = None
     if not args.no_cpu and rank == 0:

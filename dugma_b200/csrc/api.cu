@@ -72,28 +72,60 @@ int Context::ensure_scratch(size_t bytes)
         return set_error(DUGMA_ERR_STATE, "scratch must be sized before graph capture (%zu > %zu bytes)", bytes,
                          scratch_bytes);
     DUGMA_CK(cudaStreamSynchronize(stream));
-    if (scratch) cudaFree(scratch);
-    scratch = nullptr;
-    scratch_bytes = 0;
-    const size_t want = std::max(bytes, (size_t)1 << 20);
-    if (cudaMalloc(&scratch, want) != cudaSuccess) {
+    if (scratch_extra) cudaFree(scratch_extra);
+    scratch_extra = nullptr;
+    const size_t want = std::max(bytes, 2 * scratch_bytes);
+    if (cudaMalloc(&scratch_extra, want) != cudaSuccess) {
         cudaGetLastError();
+        scratch_extra = nullptr;
+        scratch = arena_scratch;
+        scratch_bytes = arena_scratch_bytes;
         return set_error(DUGMA_ERR_NOMEM, "cannot allocate %zu bytes of scratch", want);
     }
+    scratch = reinterpret_cast<double*>(scratch_extra);
     scratch_bytes = want;
     return DUGMA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pinned host staging: a process-wide pool of fixed-size blocks, so that creating a
+// context does not pay for a pinned allocation every time
+// ---------------------------------------------------------------------------
+static std::mutex g_pin_mu;
+static std::vector<double*> g_pin_free;
+
+static double* pinned_acquire()
+{
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) {
+        constexpr int kSlab = 16;
+        double* slab = nullptr;
+        if (cudaMallocHost((void**)&slab, sizeof(double) * kHostDoubles * kSlab) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (int k = 0; k < kSlab; ++k) g_pin_free.push_back(slab + (size_t)k * kHostDoubles);
+    }
+    double* p = g_pin_free.back();
+    g_pin_free.pop_back();
+    return p;
+}
+
+static void pinned_release(double* p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
 }
 
 static void destroy_context(Context* c)
 {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->x, c->xinv, c->y, c->yinv, c->wx, c->wy, c->xcov, c->ycov, c->lwx, c->lwy, c->yrec,
-                    c->xrec, c->yrec128, c->xrec128, c->yp32, c->dmin, c->pose, c->out, c->err, c->counter,
-                    c->scratch, c->dedx, c->mom};
+    void* bufs[] = {c->arena, c->scratch_extra, c->yrec128, c->xrec128, c->dedx};
     for (void* b : bufs)
         if (b) cudaFree(b);
-    if (c->host) cudaFreeHost(c->host);
+    pinned_release(c->host);
     for (auto& e : c->tevents) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -226,15 +258,6 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
         destroy_context(c);
         return code;
     };
-    auto al = [&](void** p, size_t bytes) -> bool {
-        if (rc != DUGMA_OK) return false;
-        if (cudaMalloc(p, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            rc = set_error(DUGMA_ERR_NOMEM, "init: cudaMalloc of %zu bytes failed", bytes);
-            return false;
-        }
-        return true;
-    };
     if (cudaGetDevice(&c->dev) != cudaSuccess) {
         cudaGetLastError();
         delete c;
@@ -243,31 +266,44 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(set_error(DUGMA_ERR_CUDA, "init: stream creation failed"));
+    // One device arena holds every per-context buffer.  Its scratch region first receives
+    // the FP64 host inputs during init and afterwards the kernels' partial sums.
     const int NS = D == 3 ? 6 : 3;
-    al((void**)&c->x, sizeof(float) * N * D);
-    al((void**)&c->xinv, sizeof(float) * N * D * D);
-    al((void**)&c->y, sizeof(float) * M * D);
-    al((void**)&c->yinv, sizeof(float) * M * D * D);
-    al((void**)&c->wx, sizeof(float) * N);
-    al((void**)&c->wy, sizeof(float) * M);
-    al((void**)&c->xcov, sizeof(float) * N * NS);
-    al((void**)&c->ycov, sizeof(float) * M * NS);
-    al((void**)&c->lwx, sizeof(float) * N);
-    al((void**)&c->lwy, sizeof(float) * M);
-    al((void**)&c->yrec, sizeof(YRec) * c->M_pad);
-    al((void**)&c->xrec, sizeof(XRec) * c->N_pad);
-    al((void**)&c->yp32, sizeof(float4) * c->M_pad);
-    al((void**)&c->dmin, sizeof(float) * N);
-    al((void**)&c->pose, sizeof(double) * kPoseDoubles * 2);
-    al((void**)&c->out, sizeof(double) * 64);
-    al((void**)&c->err, sizeof(int) * 4);
-    al((void**)&c->counter, sizeof(int) * 8);
-    al((void**)&c->mom, sizeof(double) * 512);
-    if (rc != DUGMA_OK) return fail(rc);
-    if (cudaMallocHost((void**)&c->host, sizeof(double) * kHostDoubles) != cudaSuccess) {
+    const size_t staging = sizeof(double) * ((size_t)N * D * (D + 1) + (size_t)M * D * (D + 1));
+    const size_t scratch_bytes = std::max(staging, (size_t)4 << 20);
+    struct Slot {
+        void** p;
+        size_t bytes;
+    };
+    const Slot slots[] = {
+        {(void**)&c->x, sizeof(float) * N * D},         {(void**)&c->xinv, sizeof(float) * N * D * D},
+        {(void**)&c->y, sizeof(float) * M * D},         {(void**)&c->yinv, sizeof(float) * M * D * D},
+        {(void**)&c->wx, sizeof(float) * N},            {(void**)&c->wy, sizeof(float) * M},
+        {(void**)&c->xcov, sizeof(float) * N * NS},     {(void**)&c->ycov, sizeof(float) * M * NS},
+        {(void**)&c->lwx, sizeof(float) * N},           {(void**)&c->lwy, sizeof(float) * M},
+        {(void**)&c->yrec, sizeof(YRec) * c->M_pad},    {(void**)&c->xrec, sizeof(XRec) * c->N_pad},
+        {(void**)&c->yp32, sizeof(float4) * c->M_pad},  {(void**)&c->dmin, sizeof(float) * N},
+        {(void**)&c->pose, sizeof(double) * kPoseDoubles * 2}, {(void**)&c->out, sizeof(double) * 64},
+        {(void**)&c->err, sizeof(int) * 4},             {(void**)&c->counter, sizeof(int) * 8},
+        {(void**)&c->mom, sizeof(double) * 512},        {(void**)&c->arena_scratch, scratch_bytes},
+    };
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    size_t total = 0;
+    for (const Slot& s : slots) total += up(s.bytes);
+    if (cudaMalloc(&c->arena, total) != cudaSuccess) {
         cudaGetLastError();
-        return fail(set_error(DUGMA_ERR_NOMEM, "init: pinned staging allocation failed"));
+        c->arena = nullptr;
+        return fail(set_error(DUGMA_ERR_NOMEM, "init: cannot allocate %zu bytes of device memory", total));
     }
+    size_t off = 0;
+    for (const Slot& s : slots) {
+        *s.p = static_cast<char*>(c->arena) + off;
+        off += up(s.bytes);
+    }
+    c->scratch = c->arena_scratch;
+    c->scratch_bytes = c->arena_scratch_bytes = scratch_bytes;
+    c->host = pinned_acquire();
+    if (!c->host) return fail(set_error(DUGMA_ERR_NOMEM, "init: pinned staging allocation failed"));
     if (cudaMemsetAsync(c->err, 0, sizeof(int) * 4, c->stream) != cudaSuccess)
         return fail(set_error(DUGMA_ERR_CUDA, "init: memset failed"));
     rc = launch_init(*c, X, X_C, Y, Y_C);

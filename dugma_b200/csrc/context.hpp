@@ -60,7 +60,11 @@ struct Context {
     int* counter = nullptr;                   // work-queue counters (8)
     double* dedx = nullptr;                   // dE/dx rows (allocated on first request)
     double* mom = nullptr;                    // surrogate moments (512 doubles)
-    // growable scratch
+    // scratch: a region of the arena, replaced by a separate allocation if a launch needs more
+    void* arena = nullptr;                    // one cudaMalloc for every buffer above
+    double* arena_scratch = nullptr;
+    size_t arena_scratch_bytes = 0;
+    void* scratch_extra = nullptr;
     double* scratch = nullptr;
     size_t scratch_bytes = 0;
     // pinned host staging

@@ -104,8 +104,8 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     const int D = c.D, N = c.N, M = c.M;
     const size_t nd = (size_t)N * D, md = (size_t)M * D;
     const size_t bytes = sizeof(double) * (nd + nd * D + md + md * D);
-    double* tmp = nullptr;
-    DUGMA_CK(cudaMalloc(&tmp, bytes));
+    if (bytes > c.scratch_bytes) return set_error(DUGMA_ERR_STATE, "init: staging does not fit the scratch region");
+    double* tmp = c.scratch;   // the FP64 inputs are staged in the (still unused) scratch region
     double *tX = tmp, *tXC = tX + nd, *tY = tXC + nd * D, *tYC = tY + md;
     cudaStream_t s = c.stream;
     int rc = DUGMA_OK;
@@ -145,7 +145,6 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     ck(cudaMemcpyAsync(c.host, Lm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax");
     ck(cudaMemcpyAsync(c.host + 2, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
     ck(cudaStreamSynchronize(s), "sync");
-    cudaFree(tmp);
     if (rc != DUGMA_OK) return rc;
     c.Lmax_x = std::isfinite(c.host[0]) ? c.host[0] : 0.0;
     c.Lmax_y = std::isfinite(c.host[1]) ? c.host[1] : 0.0;
