@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-fd", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shape (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="override the cloud size (small profiling cases)")
+    ap.add_argument("--shape", default="", help="pin the adjoint kernel shape ipt,nt,tj,pack (skips tuning)")
     return ap.parse_args()
 
 
@@ -197,7 +198,13 @@ def main():
     R, t = eval_pose(P, rank)
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
     sig = api.update_sig(h, R, t)
-    tune = "" if args.no_tune else api.autotune(h, 0)
+    if args.shape:
+        api.set_shape(h, 0, [int(v) for v in args.shape.split(",")])
+        tune = f"pinned {args.shape}"
+    else:
+        tune = "" if args.no_tune else api.autotune(h, 0)
+    if not args.no_fd and not args.shape and not args.no_tune:
+        api.autotune(h, 1)     # the plain form's energy kernel gets the same treatment
     pairs = P.N * P.M
 
     # a dedicated stream: handle 0 (the legacy default stream) means 'the context stream' in the C ABI

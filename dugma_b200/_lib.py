@@ -49,6 +49,8 @@ EXPORTS = {
                                c_int, dp, dp, dp]),
     "dugma_version": (ctypes.c_char_p, []),
     "dugma_timing": (c_int, [PtrArray, c_int, dp, ip]),
+    "dugma_shapes": (c_int, [c_int, ip, c_int]),
+    "dugma_set_shape": (c_int, [PtrArray, c_int, c_int, c_int, c_int, c_int]),
     "dugma_calibrate": (c_int, [c_int, dp, dp]),
 }
 

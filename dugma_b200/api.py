@@ -171,6 +171,19 @@ def autotune(h: Handles, what=0, model=_lib.MODEL_REF) -> str:
     return buf.value.decode()
 
 
+def shapes(what=0):
+    """Compiled kernel shapes for `what` (0 adjoint, 1 energy, 2 nearest neighbour): (ipt, nt, tj, pack)."""
+    buf = (ctypes.c_int * 256)()
+    n = _lib.load().dugma_shapes(int(what), buf, 64)
+    if n < 0:
+        check(-n)
+    return [tuple(buf[4 * k:4 * k + 4]) for k in range(n)]
+
+
+def set_shape(h: Handles, what, shape):
+    check(_lib.load().dugma_set_shape(h.arr, int(what), *[int(v) for v in shape]))
+
+
 class Graph:
     """A captured energy+gradient evaluation, replayed per pose."""
 

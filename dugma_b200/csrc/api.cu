@@ -118,11 +118,68 @@ static void pinned_release(double* p)
     g_pin_free.push_back(p);
 }
 
+// ---------------------------------------------------------------------------
+// device arenas of freed contexts are kept (per device, up to kArenaCacheBytes) and
+// handed to the next init that fits, the way a caching allocator would
+// ---------------------------------------------------------------------------
+constexpr size_t kArenaCacheBytes = (size_t)8 << 30;
+struct CachedArena {
+    int dev;
+    size_t bytes;
+    void* p;
+};
+static std::mutex g_arena_mu;
+static std::vector<CachedArena> g_arenas;
+static size_t g_arena_bytes = 0;
+
+static void* arena_acquire(int dev, size_t bytes, size_t* got)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        int best = -1;
+        for (int k = 0; k < (int)g_arenas.size(); ++k) {
+            const CachedArena& a = g_arenas[k];
+            if (a.dev == dev && a.bytes >= bytes && a.bytes <= 2 * bytes + ((size_t)64 << 20) &&
+                (best < 0 || a.bytes < g_arenas[best].bytes))
+                best = k;
+        }
+        if (best >= 0) {
+            void* p = g_arenas[best].p;
+            *got = g_arenas[best].bytes;
+            g_arena_bytes -= g_arenas[best].bytes;
+            g_arenas.erase(g_arenas.begin() + best);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *got = bytes;
+    return p;
+}
+
+static void arena_release(int dev, void* p, size_t bytes)
+{
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        if (g_arena_bytes + bytes <= kArenaCacheBytes) {
+            g_arenas.push_back({dev, bytes, p});
+            g_arena_bytes += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
 static void destroy_context(Context* c)
 {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->arena, c->scratch_extra, c->yrec128, c->xrec128, c->dedx};
+    arena_release(c->dev, c->arena, c->arena_bytes);
+    void* bufs[] = {c->scratch_extra, c->yrec128, c->xrec128, c->dedx};
     for (void* b : bufs)
         if (b) cudaFree(b);
     pinned_release(c->host);
@@ -290,11 +347,8 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     auto up = [](size_t v) { return (v + 255) / 256 * 256; };
     size_t total = 0;
     for (const Slot& s : slots) total += up(s.bytes);
-    if (cudaMalloc(&c->arena, total) != cudaSuccess) {
-        cudaGetLastError();
-        c->arena = nullptr;
-        return fail(set_error(DUGMA_ERR_NOMEM, "init: cannot allocate %zu bytes of device memory", total));
-    }
+    c->arena = arena_acquire(c->dev, total, &c->arena_bytes);
+    if (!c->arena) return fail(set_error(DUGMA_ERR_NOMEM, "init: cannot allocate %zu bytes of device memory", total));
     size_t off = 0;
     for (const Slot& s : slots) {
         *s.p = static_cast<char*>(c->arena) + off;
@@ -547,7 +601,8 @@ int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t repo
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= reps;
         char buf[96];
-        snprintf(buf, sizeof(buf), "%s(ipt=%d,nt=%d,tj=%d):%.3fms", rep.empty() ? "" : " ", sh.ipt, sh.nt, sh.tj, ms);
+        snprintf(buf, sizeof(buf), "%s(ipt=%d,nt=%d,tj=%d,pack=%d):%.3fms", rep.empty() ? "" : " ", sh.ipt, sh.nt,
+                 sh.tj, sh.pack, ms);
         rep += buf;
         if (ms < best) {
             best = ms;
@@ -564,6 +619,38 @@ int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t repo
     else c->shape_nn = best_shape;
     if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
     return DUGMA_OK;
+}
+
+int dugma_shapes(int what, int* shapes, int max)
+{
+    if (what < 0 || what > 2) return -set_error(DUGMA_ERR_ARG, "shapes: what must be 0, 1 or 2");
+    std::vector<KernelShape> cand = what == 0 ? adjoint_shapes() : (what == 1 ? energy_shapes() : nn_shapes());
+    const int n = (int)cand.size();
+    for (int k = 0; k < n && k < max && shapes; ++k) {
+        shapes[4 * k] = cand[k].ipt;
+        shapes[4 * k + 1] = cand[k].nt;
+        shapes[4 * k + 2] = cand[k].tj;
+        shapes[4 * k + 3] = cand[k].pack;
+    }
+    return n;
+}
+
+int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack)
+{
+    GET_CTX(c, Ptr);
+    if (what < 0 || what > 2) return set_error(DUGMA_ERR_ARG, "set_shape: what must be 0, 1 or 2");
+    std::vector<KernelShape> cand = what == 0 ? adjoint_shapes() : (what == 1 ? energy_shapes() : nn_shapes());
+    KernelShape want;
+    want.ipt = ipt;
+    want.nt = nt;
+    want.tj = tj;
+    want.pack = pack;
+    for (const KernelShape& s : cand)
+        if (s.same(want)) {
+            (what == 0 ? c->shape_adj : what == 1 ? c->shape_energy : c->shape_nn) = s;
+            return DUGMA_OK;
+        }
+    return set_error(DUGMA_ERR_ARG, "set_shape: (%d, %d, %d, %d) is not a compiled shape", ipt, nt, tj, pack);
 }
 
 // mode 1: start recording (clears), 0: stop, 2: synchronise and report the total duration

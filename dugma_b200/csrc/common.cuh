@@ -43,6 +43,42 @@ __device__ __forceinline__ float ex2(float x)
 }
 
 // ---------------------------------------------------------------------------
+// Packed FP32 pairs (sm_100 f32x2 arithmetic: two lanes' worth of FP32 work per instruction)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// ---------------------------------------------------------------------------
 // Record layouts in HBM (16-byte aligned so tiles can be moved by bulk copy)
 // ---------------------------------------------------------------------------
 // Streamed target record, one per y_j and pose (64 B):
@@ -53,6 +89,14 @@ __device__ __forceinline__ float ex2(float x)
 // In 2D the z components are 0 and v2 = (c00, c11, c01, 0).
 struct __align__(16) YRec {
     float4 v0, v1, v2, v3;
+};
+
+// Paired target record (128 B) for the packed f32x2 kernels: targets 2p and 2p+1 side by side.
+// Field f (f = 0..15) is the float2 (value of target 2p, value of target 2p+1):
+//   f0..f2  -y'hi,  f3 lv,  f4..f6  -y'lo,  f7 + k  k C'_j packed entry k (Sym order), rest 0.
+// Coordinates are stored negated so that d = (x + f0) + f4 needs only packed adds.
+struct __align__(16) YRec2 {
+    float4 q[8];   // q[k] = (field 2k even, field 2k odd, field 2k+1 even, field 2k+1 odd)
 };
 
 // Source record, one per x_i and sigma (64 B):

@@ -32,8 +32,11 @@ constexpr int kPadJ = 128;    // target rows padded to a multiple (largest j-til
 struct KernelShape {
     int ipt = 0;      // source points per thread
     int nt = 0;       // threads per block
-    int tj = 0;       // targets per shared-memory tile
+    int tj = 0;       // streamed records per shared-memory tile
+    int pack = 1;     // targets per streamed record (2: packed f32x2 kernels on pair records)
+    int max_chunk = 0;   // most streamed records one work item may cover (0: no limit)
     bool valid() const { return ipt > 0; }
+    bool same(const KernelShape& o) const { return ipt == o.ipt && nt == o.nt && tj == o.tj && pack == o.pack; }
 };
 
 struct Context {
@@ -61,7 +64,8 @@ struct Context {
     double* dedx = nullptr;                   // dE/dx rows (allocated on first request)
     double* mom = nullptr;                    // surrogate moments (512 doubles)
     // scratch: a region of the arena, replaced by a separate allocation if a launch needs more
-    void* arena = nullptr;                    // one cudaMalloc for every buffer above
+    void* arena = nullptr;                    // one allocation for every buffer above
+    size_t arena_bytes = 0;
     double* arena_scratch = nullptr;
     size_t arena_scratch_bytes = 0;
     void* scratch_extra = nullptr;

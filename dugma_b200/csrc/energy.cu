@@ -304,6 +304,198 @@ struct RefAdjointBody {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Packed-pair forms: the same per-pair arithmetic on two targets at once with the sm_100
+// f32x2 instructions (each lane computes pair (i, 2p) in the low half and (i, 2p+1) in
+// the high half), so each FP32 instruction issue does two pairs' work.  The algorithmic
+// FP32 work per pair is unchanged; issue slots per pair drop from ~50 to ~27, leaving the
+// FP32 pipe itself as the bound.  Targets arrive as YRec2 pair records.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 fld(const YRec2& r, int f)
+{
+    const float4 q = r.q[f >> 1];
+    return (f & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+}
+
+template <int D, int IPT_, bool GRAD>
+struct PackedBody {
+    using StreamRec = YRec2;
+    static constexpr int IPT = IPT_;
+    static constexpr int NS = Sym<D>::N;
+    static constexpr int NR = Sym<D>::NR;
+    static constexpr int NV = GRAD ? 1 + NR + D : 1;
+    float2 X[IPT][D], B[IPT][NS];                 // source coordinates and k B_i, duplicated in both halves
+    float2 e[IPT];                                // energy, tile level
+    float2 S1[IPT][GRAD ? D : 1], D2[IPT][GRAD ? D : 1], Q2[IPT][GRAD ? NS : 1];   // item level
+    double E64[IPT];
+    int row[IPT];
+    double G, t[3];
+
+    __device__ void setup(const PairArgs& a)
+    {
+        const double s = 1.0 / a.pose[kPoseSig];
+        G = pow(s, (double)D) * exp2(a.Lmax);
+#pragma unroll
+        for (int q = 0; q < D; ++q) t[q] = a.pose[kPoseT + q];
+    }
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        float x[3] = {0, 0, 0}, b[6] = {0, 0, 0, 0, 0, 0};
+        row[ii] = i < a.i_end ? i : -1;
+        if (i < a.i_end) load_xrec<D>(static_cast<const XRec*>(a.xrec)[i], x, b);
+#pragma unroll
+        for (int q = 0; q < D; ++q) X[ii][q] = make_float2(x[q], x[q]);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) B[ii][q] = make_float2(b[q], b[q]);
+    }
+    __device__ void zero_all()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            e[ii] = make_float2(0.f, 0.f);
+            E64[ii] = 0.0;
+            if (GRAD) {
+#pragma unroll
+                for (int q = 0; q < D; ++q) { S1[ii][q] = make_float2(0.f, 0.f); D2[ii][q] = make_float2(0.f, 0.f); }
+#pragma unroll
+                for (int q = 0; q < NS; ++q) Q2[ii][q] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+    __device__ __forceinline__ void consume(const YRec2& r, int)
+    {
+        float2 ny[3], nl[3], c[6];
+#pragma unroll
+        for (int q = 0; q < D; ++q) { ny[q] = fld(r, q); nl[q] = fld(r, 4 + q); }
+        const float2 lv = fld(r, 3);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) c[k] = fld(r, 7 + k);
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            float2 d[3];
+#pragma unroll
+            for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(X[ii][q], ny[q]), nl[q]);
+            const float2* b = B[ii];
+            float2 t1, t2;
+            float2 u[3], qq[6];
+            if (!GRAD) {
+                // Horner forms (off-diagonals doubled in both matrices)
+                if (D == 3) {
+                    const float2 g0 = ffma2(c[4], d[2], ffma2(c[3], d[1], fmul2(c[0], d[0])));
+                    const float2 g1 = ffma2(c[5], d[2], fmul2(c[1], d[1]));
+                    const float2 g2 = fmul2(c[2], d[2]);
+                    t1 = ffma2(d[0], g0, ffma2(d[1], g1, ffma2(d[2], g2, lv)));
+                    const float2 h0 = ffma2(b[4], d[2], ffma2(b[3], d[1], fmul2(b[0], d[0])));
+                    const float2 h1 = ffma2(b[5], d[2], fmul2(b[1], d[1]));
+                    const float2 h2 = fmul2(b[2], d[2]);
+                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, ffma2(d[2], h2, lv)));
+                } else {
+                    const float2 g0 = ffma2(c[2], d[1], fmul2(c[0], d[0]));
+                    const float2 g1 = fmul2(c[1], d[1]);
+                    t1 = ffma2(d[0], g0, ffma2(d[1], g1, lv));
+                    const float2 h0 = ffma2(b[2], d[1], fmul2(b[0], d[0]));
+                    const float2 h1 = fmul2(b[1], d[1]);
+                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, lv));
+                }
+            } else {
+                if (D == 3) {
+                    u[0] = ffma2(c[4], d[2], ffma2(c[3], d[1], fmul2(c[0], d[0])));
+                    u[1] = ffma2(c[5], d[2], ffma2(c[1], d[1], fmul2(c[3], d[0])));
+                    u[2] = ffma2(c[2], d[2], ffma2(c[5], d[1], fmul2(c[4], d[0])));
+                    t1 = ffma2(d[2], u[2], ffma2(d[1], u[1], ffma2(d[0], u[0], lv)));
+                } else {
+                    u[0] = ffma2(c[2], d[1], fmul2(c[0], d[0]));
+                    u[1] = ffma2(c[1], d[1], fmul2(c[2], d[0]));
+                    t1 = ffma2(d[1], u[1], ffma2(d[0], u[0], lv));
+                }
+#pragma unroll
+                for (int k = 0; k < NS; ++k) qq[k] = fmul2(d[Sym<D>::a(k)], d[Sym<D>::b(k)]);
+                t2 = lv;
+#pragma unroll
+                for (int k = 0; k < NS; ++k) t2 = ffma2(b[k], qq[k], t2);
+            }
+            const float2 e1 = make_float2(ex2(t1.x), ex2(t1.y));
+            const float2 e2 = make_float2(ex2(t2.x), ex2(t2.y));
+            e[ii] = fadd2(fadd2(e[ii], e1), e2);
+            if (GRAD) {
+#pragma unroll
+                for (int q = 0; q < D; ++q) {
+                    S1[ii][q] = ffma2(e1, u[q], S1[ii][q]);
+                    D2[ii][q] = ffma2(e2, d[q], D2[ii][q]);
+                }
+#pragma unroll
+                for (int k = 0; k < NS; ++k) Q2[ii][k] = ffma2(e2, qq[k], Q2[ii][k]);
+            }
+        }
+    }
+    __device__ void fold()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            E64[ii] += (double)e[ii].x + (double)e[ii].y;
+            e[ii] = make_float2(0.f, 0.f);
+        }
+    }
+    __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
+    {
+        const double kinv = 1.0 / K_EXP2;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            const int i = row[ii];
+            const double w = (double)a.wx[i] * G;
+            acc[0] += w * E64[ii];
+            if (!GRAD) continue;
+            double Bm[3][3], Qm[3][3], s1[3], d2[3];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                const int ra = Sym<D>::a(q), rb = Sym<D>::b(q);
+                const double bv = (double)B[ii][q].x * kinv * (ra == rb ? 1.0 : 0.5);
+                Bm[ra][rb] = Bm[rb][ra] = bv;
+                Qm[ra][rb] = Qm[rb][ra] = (double)Q2[ii][q].x + (double)Q2[ii][q].y;
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                s1[q] = (double)S1[ii][q].x + (double)S1[ii][q].y;
+                d2[q] = (double)D2[ii][q].x + (double)D2[ii][q].y;
+            }
+            double gt[3], p[3];
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                double bd = 0;
+#pragma unroll
+                for (int cc = 0; cc < D; ++cc) bd += Bm[q][cc] * d2[cc];
+                gt[q] = s1[q] * kinv + bd;
+                p[q] = (double)X[ii][q].x - t[q];
+            }
+            if (D == 3) {
+                double qx[3] = {0, 0, 0};
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    qx[0] += Bm[2][cc] * Qm[1][cc] - Bm[1][cc] * Qm[2][cc];
+                    qx[1] += Bm[0][cc] * Qm[2][cc] - Bm[2][cc] * Qm[0][cc];
+                    qx[2] += Bm[1][cc] * Qm[0][cc] - Bm[0][cc] * Qm[1][cc];
+                }
+                acc[1] += w * (p[1] * gt[2] - p[2] * gt[1] - qx[0]);
+                acc[2] += w * (p[2] * gt[0] - p[0] * gt[2] - qx[1]);
+                acc[3] += w * (p[0] * gt[1] - p[1] * gt[0] - qx[2]);
+            } else {
+                double qx = 0;
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) qx += Bm[1][cc] * Qm[0][cc] - Bm[0][cc] * Qm[1][cc];
+                acc[1] += w * (p[0] * gt[1] - p[1] * gt[0] - qx);
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) acc[1 + NR + q] += w * gt[q];
+            if (a.dx_part) {
+                const int rows = a.i_end - a.i0;
+#pragma unroll
+                for (int q = 0; q < D; ++q) a.dx_part[((size_t)jc * rows + (i - a.i0)) * D + q] = -w * gt[q];
+            }
+        }
+    }
+};
+
 template <class Body, int NT, int TJ>
 __global__ void __launch_bounds__(NT) pair_kernel(PairArgs a)
 {
@@ -351,11 +543,16 @@ struct Variant {
 template <int D>
 static const std::vector<Variant>& adjoint_variants()
 {
+    // packed gradient variants keep their moment sums in FP32 over one item: at most 512 pair
+    // records (1024 targets) per item bounds that sum's rounding error
     static const std::vector<Variant> v = {
         {{2, 128, 64}, pair_kernel<RefAdjointBody<D, 2>, 128, 64>},
         {{1, 128, 64}, pair_kernel<RefAdjointBody<D, 1>, 128, 64>},
         {{1, 256, 64}, pair_kernel<RefAdjointBody<D, 1>, 256, 64>},
         {{2, 256, 32}, pair_kernel<RefAdjointBody<D, 2>, 256, 32>},
+        {{1, 128, 32, 2, 512}, pair_kernel<PackedBody<D, 1, true>, 128, 32>},
+        {{2, 128, 32, 2, 512}, pair_kernel<PackedBody<D, 2, true>, 128, 32>},
+        {{1, 256, 32, 2, 512}, pair_kernel<PackedBody<D, 1, true>, 256, 32>},
     };
     return v;
 }
@@ -368,6 +565,9 @@ static const std::vector<Variant>& energy_variants()
         {{2, 128, 64}, pair_kernel<RefEnergyBody<D, 2>, 128, 64>},
         {{2, 256, 64}, pair_kernel<RefEnergyBody<D, 2>, 256, 64>},
         {{4, 256, 32}, pair_kernel<RefEnergyBody<D, 4>, 256, 32>},
+        {{2, 128, 32, 2}, pair_kernel<PackedBody<D, 2, false>, 128, 32>},
+        {{4, 128, 32, 2}, pair_kernel<PackedBody<D, 4, false>, 128, 32>},
+        {{2, 256, 32, 2}, pair_kernel<PackedBody<D, 2, false>, 256, 32>},
     };
     return v;
 }
@@ -414,6 +614,8 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     const int resident = c.num_sms * occupancy_blocks(fn, sh.nt);
     const int target = 4 * resident;
     int n_jc = std::max(1, std::min(total_tiles, (target + n_ib - 1) / n_ib));
+    if (sh.max_chunk > 0) n_jc = std::max(n_jc, (total_tiles * sh.tj + sh.max_chunk - 1) / sh.max_chunk);
+    n_jc = std::min(n_jc, total_tiles);
     const int jc_tiles = (total_tiles + n_jc - 1) / n_jc;
     n_jc = (total_tiles + jc_tiles - 1) / jc_tiles;
     const int n_items = n_ib * n_jc;
@@ -481,16 +683,18 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
     if (i0 < 0 || i1 > c.N || i0 >= i1) return set_error(DUGMA_ERR_ARG, "bad source row range [%d, %d)", i0, i1);
     if (model == DUGMA_MODEL_CONV) return conv_launch(c, pose_dev, grad, i0, i1, out_dev, dEdx_dev, s, force);
     if (model != DUGMA_MODEL_REF) return set_error(DUGMA_ERR_ARG, "unknown model %d", model);
-    DUGMA_RET(launch_prologue(c, pose_dev, grad ? 0 : 1, s));
     const KernelShape want = force ? *force : (grad ? c.shape_adj : c.shape_energy);
     const std::vector<Variant>& vars =
         c.D == 3 ? (grad ? adjoint_variants<3>() : energy_variants<3>()) : (grad ? adjoint_variants<2>() : energy_variants<2>());
     const Variant* v = &vars[0];
     for (auto& cand : vars)
-        if (cand.shape.ipt == want.ipt && cand.shape.nt == want.nt && cand.shape.tj == want.tj) v = &cand;
+        if (cand.shape.same(want)) v = &cand;
+    // record layout: 0 scalar adjoint, 1 scalar Horner energy, 2 / 3 their packed-pair forms
+    const int layout = (grad ? 0 : 1) + (v->shape.pack == 2 ? 2 : 0);
+    DUGMA_RET(launch_prologue(c, pose_dev, layout, s));
     const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
-    return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad, nv, c.Lmax_y, pose_dev, i0, i1,
-                               out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
+    return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad / v->shape.pack, nv, c.Lmax_y,
+                               pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
 }
 
 }  // namespace dugma

@@ -222,21 +222,39 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
 #pragma unroll
                     for (int q = 0; q < D; ++q) acc = acc + R[ra + D * q] * T[q][rb];
                     double v = ks * acc;
-                    if (ylayout == 1 && ra != rb) v = 2.0 * v;
+                    if ((ylayout & 1) && ra != rb) v = 2.0 * v;   // Horner layouts (1, 3)
                     cp[k] = __double2float_rn(v);
                 }
             }
         }
-        r.v0 = make_float4(hi[0], hi[1], hi[2], lv);
-        r.v1 = make_float4(lo[0], lo[1], lo[2], 0.f);
-        if (D == 3) {
-            r.v2 = make_float4(cp[0], cp[1], cp[2], cp[3]);
-            r.v3 = make_float4(cp[4], cp[5], 0.f, 0.f);
+        if (ylayout >= 2) {
+            // paired layout: this target fills its half of pair record j / 2
+            float f[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) f[q] = 0.f;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                f[a] = -hi[a];
+                f[4 + a] = -lo[a];
+            }
+            f[3] = lv;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) f[7 + k] = cp[k];
+            float* base = reinterpret_cast<float*>(yrec) + (size_t)(j >> 1) * 32 + (j & 1);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) base[(q >> 1) * 4 + (q & 1) * 2] = f[q];
         } else {
-            r.v2 = make_float4(cp[0], cp[1], cp[2], 0.f);
-            r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
+            r.v0 = make_float4(hi[0], hi[1], hi[2], lv);
+            r.v1 = make_float4(lo[0], lo[1], lo[2], 0.f);
+            if (D == 3) {
+                r.v2 = make_float4(cp[0], cp[1], cp[2], cp[3]);
+                r.v3 = make_float4(cp[4], cp[5], 0.f, 0.f);
+            } else {
+                r.v2 = make_float4(cp[0], cp[1], cp[2], 0.f);
+                r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            yrec[j] = r;
         }
-        yrec[j] = r;
         // padding targets sit at +inf so that no source ever picks them as a neighbour
         if (yp32)
             yp32[j] = j < M ? make_float4(hi[0], hi[1], hi[2], 0.f)

@@ -115,6 +115,14 @@ int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double*
  * context and keeps the fastest; writes a one-line report into `report` (may be NULL). */
 int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t report_len);
 
+/* Kernel shapes available for `what` (0 adjoint, 1 energy, 2 nearest neighbour): writes up to
+ * `max` tuples {source points per thread, threads per block, records per tile, targets per
+ * record} into shapes[4 * k] and returns the count (negative status on error). */
+int dugma_shapes(int what, int* shapes, int max);
+
+/* Pins the kernel shape used for `what` on this context (one of dugma_shapes' tuples). */
+int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack);
+
 /* Captures one energy+gradient evaluation (prologue, pair kernel, reduction) as a CUDA graph
  * reading its pose from the context's pose buffer; dugma_graph_eval replays it for a new
  * pose and returns E and g. */
@@ -158,7 +166,8 @@ int dugma_register(const double* X, const double* X_C, const double* Y, const do
 int dugma_timing(float* Ptr[6], int mode, double* total_ms, int* launches);
 
 /* Measured peak of a GPU pipe on the current device: what = 0 FP32 fused multiply-add,
- * 1 SFU ex2; returns lane operations per second (and the kernel time in ms). */
+ * 1 SFU ex2, 2 packed f32x2 fused multiply-add; returns lane operations per second (and the
+ * kernel time in ms). */
 int dugma_calibrate(int what, double* lane_ops_per_s, double* ms);
 
 /* Library build/version string. */
