@@ -1,0 +1,58 @@
+"""Multi-GPU use of the hot path: one process per GPU, torch.distributed for the plumbing.
+
+Two ways the path divides (no collective is on the data path of either):
+  * independent units — multistart poses of a problem, or whole problems — one per
+    rank, nothing exchanged (bench.py --gpus N);
+  * one large problem split by source rows: each rank evaluates its rows
+    (dugma_energy_grad_range) and the partial energies and pose gradients (7 doubles in
+    3D) are summed with one all-reduce.  The sum over rows is exactly the full sum up to
+    FP64 rounding of the final additions.
+"""
+from __future__ import annotations
+
+from typing import Callable, Sequence
+
+import numpy as np
+
+
+def row_ranges(n: int, world: int) -> list[tuple[int, int]]:
+    """Contiguous, balanced source-row ranges for `world` ranks."""
+    base, extra = divmod(n, world)
+    out, i = [], 0
+    for r in range(world):
+        k = base + (1 if r < extra else 0)
+        out.append((i, i + k))
+        i += k
+    return out
+
+
+def energy_grad_sharded(n_rows: int, rank: int, world: int,
+                        compute: Callable[[int, int], tuple[float, Sequence[float]]], group=None):
+    """Sum of compute(i0, i1) over the ranks' row ranges; every rank returns (E, g).
+
+    `compute` is the per-rank evaluation, normally
+    lambda i0, i1: dugma_b200.api.energy_grad_range(handles, R, t, sig, i0, i1)."""
+    import torch
+    import torch.distributed as dist
+
+    i0, i1 = row_ranges(n_rows, world)[rank]
+    if i1 > i0:
+        E, g = compute(i0, i1)
+    else:
+        E, g = 0.0, None
+    g = np.zeros(0) if g is None else np.asarray(g, dtype=np.float64)
+    ng = torch.tensor([g.size], dtype=torch.int64)
+    if world > 1:
+        dist.all_reduce(ng, op=dist.ReduceOp.MAX, group=group)
+    buf = np.zeros(1 + int(ng.item()))
+    buf[0] = E
+    buf[1:1 + g.size] = g
+    t = torch.from_numpy(buf)
+    if world > 1:
+        backend = dist.get_backend(group)
+        if backend == "nccl":
+            t = t.cuda()
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        t = t.cpu()
+    out = t.numpy()
+    return float(out[0]), out[1:].copy()
