@@ -697,4 +697,139 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
                                pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free fused adjoint.
+//
+// For callers that cannot allocate device memory while they evaluate: code that runs
+// while a CUDA graph is being captured (allocation calls are not allowed there), loops
+// with a latency budget that must never enter an allocator, and host applications that
+// own every device allocation themselves.  They pass the six input arrays and the
+// output buffer; everything the evaluation needs besides them (per-pose records,
+// normalised weights, work-queue counter, per-item partial sums) lives in one
+// file-scope device array of kNoAllocScratchBytes, which every GPU that loads this
+// library holds until the process exits.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;   // 4 MiB
+constexpr int kNoAllocMaxPadded = 16384;                     // N and M, after padding to 1024 / 128
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// max_j log2(w_j) over positive weights into *out (one block, fixed order)
+__global__ void noalloc_max_log2_kernel(const float* __restrict__ w, int n, double* out)
+{
+    __shared__ double red[256];
+    double m = -INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (w[i] > 0.0f) m = fmax(m, log2((double)w[i]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = isfinite(red[0]) ? red[0] : 0.0;
+}
+
+__global__ void noalloc_norm_log2_kernel(const float* __restrict__ w, int n, const double* Lmax, float* __restrict__ lw)
+{
+    const double L = *Lmax;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        lw[i] = w[i] > 0.0f ? __double2float_rn(log2((double)w[i]) - L) : -INFINITY;
+}
+
+// the pair kernel ran with a zero weight offset: restore the 2^Lmax_y factor of every output
+__global__ void noalloc_scale_kernel(double* out, int n, const double* Lmax)
+{
+    if (threadIdx.x < n) out[threadIdx.x] *= exp2(*Lmax);
+}
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64];
+
+}  // namespace dugma
+
+extern "C" int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv, const float* y, const float* y_cov_inv,
+                                         const float* det_x, const float* det_y, int N, int M, int D,
+                                         const double* pose_dev, double* out_dev, void* stream)
+{
+    using namespace dugma;
+    if (!x || !x_cov_inv || !det_x || !y || !y_cov_inv || !det_y || !pose_dev || !out_dev)
+        return set_error(DUGMA_ERR_ARG, "energy_grad_noalloc: null argument");
+    if (D != 2 && D != 3) return set_error(DUGMA_ERR_ARG, "energy_grad_noalloc: D must be 2 or 3 (got %d)", D);
+    const int N_pad = (N + kPadI - 1) / kPadI * kPadI, M_pad = (M + kPadJ - 1) / kPadJ * kPadJ;
+    if (N < 1 || M < 1 || N_pad > kNoAllocMaxPadded || M_pad > kNoAllocMaxPadded)
+        return set_error(DUGMA_ERR_ARG,
+                         "energy_grad_noalloc: N = %d, M = %d; this entry point takes 1 <= N, M <= %d (its scratch is "
+                         "a fixed %zu-byte device array); use dugma_energy_grad for larger clouds",
+                         N, M, kNoAllocMaxPadded, kNoAllocScratchBytes);
+    int dev = 0;
+    DUGMA_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(DUGMA_ERR_ARG, "energy_grad_noalloc: device %d out of range", dev);
+    const Variant& var = D == 3 ? adjoint_variants<3>()[0] : adjoint_variants<2>()[0];
+    unsigned char* base = nullptr;
+    {
+        // once per device: the device address of the scratch array (a host-side name is not one)
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            DUGMA_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            occupancy_blocks(var.fn, var.shape.nt);   // fills the launch-shape cache before any capture
+            g_noalloc_addr[dev] = p;
+        }
+        base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    }
+    // carve: records, normalised log weights, offsets, counters, then partial sums
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + off;
+        off += (bytes + 255) / 256 * 256;
+        return p;
+    };
+    Context c;   // a view of the caller's arrays and the static scratch; owns nothing
+    c.N = N;
+    c.M = M;
+    c.D = D;
+    c.N_pad = N_pad;
+    c.M_pad = M_pad;
+    c.dev = dev;
+    cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, dev);
+    c.x = const_cast<float*>(x);
+    c.xinv = const_cast<float*>(x_cov_inv);
+    c.wx = const_cast<float*>(det_x);
+    c.y = const_cast<float*>(y);
+    c.yinv = const_cast<float*>(y_cov_inv);
+    c.wy = const_cast<float*>(det_y);
+    c.xrec = reinterpret_cast<XRec*>(take(sizeof(XRec) * (size_t)N_pad));
+    c.yrec = reinterpret_cast<YRec*>(take(sizeof(YRec) * (size_t)M_pad));
+    c.lwx = reinterpret_cast<float*>(take(sizeof(float) * (size_t)N));
+    c.lwy = reinterpret_cast<float*>(take(sizeof(float) * (size_t)M));
+    double* Lm = reinterpret_cast<double*>(take(2 * sizeof(double)));
+    c.counter = reinterpret_cast<int*>(take(8 * sizeof(int)));
+    c.err = reinterpret_cast<int*>(take(4 * sizeof(int)));
+    c.scratch = c.arena_scratch = reinterpret_cast<double*>(base + off);
+    c.scratch_bytes = c.arena_scratch_bytes = kNoAllocScratchBytes - off;
+    // partial sums: at most (source blocks + 4 items per resident block) x 8 doubles; check the
+    // worst case (32 resident blocks per SM) so the launch below can never ask for more
+    const int BI = var.shape.ipt * var.shape.nt;
+    const size_t worst_items = (size_t)(N_pad / BI + 1) + (size_t)4 * c.num_sms * 32;
+    if (worst_items * 8 * sizeof(double) > c.scratch_bytes)
+        return set_error(DUGMA_ERR_STATE, "energy_grad_noalloc: scratch layout does not fit");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DUGMA_CK(cudaMemsetAsync(c.err, 0, 4 * sizeof(int), s));   // the error word must start at zero
+    noalloc_max_log2_kernel<<<1, 256, 0, s>>>(det_x, N, Lm);
+    noalloc_max_log2_kernel<<<1, 256, 0, s>>>(det_y, M, Lm + 1);
+    const int g = std::min((std::max(N, M) + 255) / 256, c.num_sms * 4);
+    noalloc_norm_log2_kernel<<<g, 256, 0, s>>>(det_x, N, Lm, c.lwx);
+    noalloc_norm_log2_kernel<<<g, 256, 0, s>>>(det_y, M, Lm + 1, c.lwy);
+    DUGMA_CK(cudaGetLastError());
+    DUGMA_RET(launch_prologue(c, pose_dev, 0, s));   // c.yp32 is null: no nearest-neighbour records
+    const int nv = 1 + (D == 3 ? 6 : 3);
+    DUGMA_RET(launch_pair_variant(c, var.fn, var.shape, c.xrec, c.yrec, (size_t)M_pad, nv, 0.0, pose_dev, 0, N,
+                                  out_dev, nullptr, nullptr, 0, nullptr, s));
+    noalloc_scale_kernel<<<1, 32, 0, s>>>(out_dev, nv, Lm + 1);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
+namespace dugma {
 }  // namespace dugma

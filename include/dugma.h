@@ -109,6 +109,26 @@ int dugma_energy_grad_async(float* Ptr[6], const double* pose_dev, int model, do
                             double* dEdx_dev, void* stream);
 int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double* out_dev, void* stream);
 
+/* Allocation-free fused adjoint.  No counterpart in the reference: it is for callers that
+ * cannot allocate device memory while they evaluate — code running during CUDA-graph
+ * capture (allocation calls are not permitted there), latency-bounded loops that must never
+ * enter an allocator, and hosts that own every device allocation themselves.  The caller
+ * passes the six input arrays in the order and layout of Ptr[6] after dugma_init (source
+ * coordinates, source inverse covariances, target coordinates, target inverse covariances,
+ * source |Sigma|^-1/2, target |Sigma|^-1/2; e.g. the Ptr[6] of an init done beforehand), the pose
+ * block pose_dev (as dugma_energy_grad_async) and out_dev (1 + NR + D doubles on the
+ * device); nothing is allocated.  All other working memory is one 4 MiB file-scope device
+ * array that every GPU loading this library holds until exit, which limits N and M to 16384.
+ * Larger sizes are rejected with DUGMA_ERR_ARG.  The first call on each device looks up that
+ * array's device address (make the first call before any stream capture).  Every call
+ * reuses the same array, so calls whose work overlaps on the GPU (other streams, other
+ * threads) race; the array keeps the last call's contents and each call re-initialises what
+ * it needs.  Work is enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream)
+ * and the call returns without synchronising. */
+int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv, const float* y, const float* y_cov_inv,
+                              const float* det_x, const float* det_y, int N, int M, int D,
+                              const double* pose_dev, double* out_dev, void* stream);
+
 /* ---------------- tuning and graphs ---------------- */
 
 /* Times the kernel shapes of `what` (0 = adjoint, 1 = energy, 2 = nearest neighbour) on this
