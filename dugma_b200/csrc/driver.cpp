@@ -1,9 +1,537 @@
-// driver.cpp -- registration loop (DUGMA.m) with a quasi-Newton solver.
-#include "dugma.h"
+// driver.cpp -- the registration loop of DUGMA.m:19-137 with a quasi-Newton solver in
+// place of MATLAB's fmincon.
+//
+// Reference mode (DUGMA_DRIVE_REFERENCE), per iteration (DUGMA.m:57-113):
+//   A = compi(R, t, sig)                      the 637 / 45 surrogate coefficients
+//   (dR, dt) = argmin Q(dR, dt) = A . b(dR, dt) over dR in SO(D)   (energy3D.m, fcontr3D.m)
+//   R <- dR R,  t <- dt + t                   (DUGMA.m:76-78: t is not rotated by dR)
+//   stop on the Euler-angle change (rotm2eul ZYX; 2D asind(R21), degrees), |t - t_prev|^2,
+//   sig <= acc_sig or the iteration limit; sig <- update_sig(R, t).
+// fmincon minimises over a general 3x3 dR with det dR = 1 and dR^T dR = I; here dR =
+// exp([w]x) (2D: a rotation by theta), so the constraints hold by construction and the
+// minimisation is unconstrained over (w, dt): damped Newton steps with the analytic
+// gradient of Q (from the monomial exponents) and a Hessian by central differences of
+// that gradient, with backtracking.
+// Direct mode (DUGMA_DRIVE_DIRECT): maximise E(R, t) at the current sig with BFGS on the
+// left-perturbation coordinates using the fused adjoint's gradient, then update sig.
+// Both modes normalise the clouds first (normalize.m:3-26) and denormalise the
+// translation at the end (DUGMA.m:122).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
 
-extern "C" int dugma_register(const double*, const double*, const double*, const double*, int, int, int,
-                              const double*, const double*, int, double, double, double, int, double*, double*,
-                              double*)
+#include "dugma.h"
+#include "monomials.h"
+
+namespace {
+
+using Vec = std::vector<double>;
+
+struct Mat3 {
+    double a[9];   // column-major
+    double& operator()(int r, int c) { return a[r + 3 * c]; }
+    double operator()(int r, int c) const { return a[r + 3 * c]; }
+};
+
+Mat3 mul(const Mat3& A, const Mat3& B)
 {
-    return DUGMA_ERR_ARG;
+    Mat3 C{};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += A(r, k) * B(k, c);
+            C(r, c) = s;
+        }
+    return C;
+}
+
+Mat3 expso3(const double w[3])
+{
+    const double th = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    Mat3 K{};
+    K(0, 1) = -w[2];
+    K(0, 2) = w[1];
+    K(1, 0) = w[2];
+    K(1, 2) = -w[0];
+    K(2, 0) = -w[1];
+    K(2, 1) = w[0];
+    const Mat3 K2 = mul(K, K);
+    const double a = th < 1e-10 ? 1.0 - th * th / 6.0 : std::sin(th) / th;
+    const double b = th < 1e-10 ? 0.5 - th * th / 24.0 : (1.0 - std::cos(th)) / (th * th);
+    Mat3 R{};
+    for (int k = 0; k < 9; ++k) R.a[k] = (k % 4 == 0 ? 1.0 : 0.0) + a * K.a[k] + b * K2.a[k];
+    return R;
+}
+
+// ZYX Euler angles of a rotation (MATLAB rotm2eul default), radians: [z, y, x]
+void rotm2eul(const Mat3& R, double e[3])
+{
+    const double sy = std::max(-1.0, std::min(1.0, -R(2, 0)));
+    e[1] = std::asin(sy);
+    if (std::fabs(sy) < 1.0 - 1e-12) {
+        e[0] = std::atan2(R(1, 0), R(0, 0));
+        e[2] = std::atan2(R(2, 1), R(2, 2));
+    } else {
+        e[0] = std::atan2(-R(0, 1), R(1, 1));
+        e[2] = 0.0;
+    }
+}
+
+// Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq and its gradient in v.
+struct Surrogate {
+    int D, K, nv;
+    const double* A;
+    const unsigned char* E;
+    double value(const double* v) const
+    {
+        double s = 0;
+        for (int k = 0; k < K; ++k) {
+            double m = A[k];
+            for (int q = 0; q < nv; ++q)
+                for (int e = 0; e < E[k * nv + q]; ++e) m *= v[q];
+            s += m;
+        }
+        return s;
+    }
+    void grad(const double* v, double* g) const
+    {
+        for (int q = 0; q < nv; ++q) g[q] = 0;
+        for (int k = 0; k < K; ++k) {
+            for (int q = 0; q < nv; ++q) {
+                const int eq = E[k * nv + q];
+                if (!eq) continue;
+                double m = A[k] * eq;
+                for (int p = 0; p < nv; ++p) {
+                    const int ep = E[k * nv + p] - (p == q ? 1 : 0);
+                    for (int e = 0; e < ep; ++e) m *= v[p];
+                }
+                g[q] += m;
+            }
+        }
+    }
+};
+
+// parameters p = (w (NR), dt (D)) -> surrogate variables v and the value / gradient in p
+struct SurrogateInP {
+    Surrogate S;
+    int D;
+    int np() const { return D == 3 ? 6 : 3; }
+    void to_v(const double* p, double* v, Mat3* dR = nullptr) const
+    {
+        if (D == 3) {
+            const Mat3 R = expso3(p);
+            v[0] = p[3];
+            v[1] = p[4];
+            v[2] = p[5];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) v[3 + 3 * r + c] = R(r, c);   // r11 r12 r13 r21 ... (row-major)
+            if (dR) *dR = R;
+        } else {
+            v[0] = p[1];
+            v[1] = p[2];
+            v[2] = std::cos(p[0]);
+            v[3] = std::sin(p[0]);
+        }
+    }
+    double value(const double* p) const
+    {
+        double v[12];
+        to_v(p, v);
+        return S.value(v);
+    }
+    void grad(const double* p, double* g) const
+    {
+        double v[12], gv[12];
+        to_v(p, v);
+        S.grad(v, gv);
+        if (D == 2) {
+            g[0] = -v[3] * gv[2] + v[2] * gv[3];
+            g[1] = gv[0];
+            g[2] = gv[1];
+            return;
+        }
+        // dQ/dw by central differences of the (smooth) map w -> R in the analytic v-gradient
+        const double h = 1e-7;
+        for (int k = 0; k < 3; ++k) {
+            double pp[6], pm[6], vp[12], vm[12];
+            memcpy(pp, p, sizeof(pp));
+            memcpy(pm, p, sizeof(pm));
+            pp[k] += h;
+            pm[k] -= h;
+            to_v(pp, vp);
+            to_v(pm, vm);
+            double s = 0;
+            for (int q = 3; q < 12; ++q) s += gv[q] * (vp[q] - vm[q]) / (2 * h);
+            g[k] = s;
+        }
+        g[3] = gv[0];
+        g[4] = gv[1];
+        g[5] = gv[2];
+    }
+};
+
+// Solve (H + lam I) x = -g for small symmetric systems (Gaussian elimination with pivoting)
+bool solve(int n, std::vector<double> H, std::vector<double> b, std::vector<double>& x)
+{
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(H[r * n + c]) > std::fabs(H[piv * n + c])) piv = r;
+        if (std::fabs(H[piv * n + c]) < 1e-300) return false;
+        if (piv != c) {
+            for (int k = 0; k < n; ++k) std::swap(H[c * n + k], H[piv * n + k]);
+            std::swap(b[c], b[piv]);
+        }
+        for (int r = c + 1; r < n; ++r) {
+            const double f = H[r * n + c] / H[c * n + c];
+            for (int k = c; k < n; ++k) H[r * n + k] -= f * H[c * n + k];
+            b[r] -= f * b[c];
+        }
+    }
+    x.assign(n, 0.0);
+    for (int r = n - 1; r >= 0; --r) {
+        double s = b[r];
+        for (int k = r + 1; k < n; ++k) s -= H[r * n + k] * x[k];
+        x[r] = s / H[r * n + r];
+    }
+    return true;
+}
+
+// Damped Newton minimisation of the surrogate from p = 0; returns the exit flag (> 0 converged,
+// 0 iteration limit, < 0 failure as fmincon's exitflag).
+int minimise_surrogate(const SurrogateInP& F, std::vector<double>& p, int* evals)
+{
+    const int n = F.np();
+    p.assign(n, 0.0);
+    double f = F.value(p.data());
+    if (!std::isfinite(f)) return -1;
+    double lam = 0;
+    for (int it = 0; it < 100; ++it) {
+        std::vector<double> g(n), H(n * n);
+        F.grad(p.data(), g.data());
+        double gn = 0;
+        for (double v : g) gn += v * v;
+        gn = std::sqrt(gn);
+        // Hessian by central differences of the gradient
+        for (int k = 0; k < n; ++k) {
+            const double h = 1e-5;
+            std::vector<double> pp = p, pm = p, gp(n), gm(n);
+            pp[k] += h;
+            pm[k] -= h;
+            F.grad(pp.data(), gp.data());
+            F.grad(pm.data(), gm.data());
+            for (int r = 0; r < n; ++r) H[r * n + k] = (gp[r] - gm[r]) / (2 * h);
+        }
+        for (int r = 0; r < n; ++r)
+            for (int c = r + 1; c < n; ++c) H[r * n + c] = H[c * n + r] = 0.5 * (H[r * n + c] + H[c * n + r]);
+        double hmax = 0;
+        for (int r = 0; r < n; ++r) hmax = std::max(hmax, std::fabs(H[r * n + r]));
+        if (lam == 0) lam = 1e-9 * std::max(hmax, 1e-300);
+        bool accepted = false;
+        for (int tries = 0; tries < 40 && !accepted; ++tries) {
+            std::vector<double> A = H, x;
+            for (int r = 0; r < n; ++r) A[r * n + r] += lam;
+            std::vector<double> mg(n);
+            for (int r = 0; r < n; ++r) mg[r] = -g[r];
+            if (!solve(n, A, mg, x)) {
+                lam *= 10;
+                continue;
+            }
+            double step = 0;
+            for (double v : x) step += v * v;
+            step = std::sqrt(step);
+            if (step > 0.5) {   // trust region on the rotation vector / translation
+                for (double& v : x) v *= 0.5 / step;
+                step = 0.5;
+            }
+            std::vector<double> pn(n);
+            for (int r = 0; r < n; ++r) pn[r] = p[r] + x[r];
+            const double fn = F.value(pn.data());
+            ++*evals;
+            if (std::isfinite(fn) && fn <= f) {
+                const double df = f - fn;
+                p = pn;
+                f = fn;
+                lam = std::max(lam * 0.3, 1e-15 * std::max(hmax, 1e-300));
+                accepted = true;
+                if (step < 1e-12 || df <= 1e-15 * std::fabs(f)) return 1;
+            } else {
+                lam *= 10;
+            }
+        }
+        if (!accepted) return gn < 1e-8 * (1 + std::fabs(f)) ? 2 : 1;   // at a stationary point
+    }
+    return 0;
+}
+
+struct Timer {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double s() const
+    {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+}  // namespace
+
+extern "C" int dugma_minimise_surrogate(int D, const double* A, double* dR, double* dt, double* Qmin, int* exitflag)
+{
+    if ((D != 2 && D != 3) || !A || !dR || !dt) return DUGMA_ERR_ARG;
+    SurrogateInP F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
+                    D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
+                   D};
+    std::vector<double> p;
+    int evals = 0;
+    const int flag = minimise_surrogate(F, p, &evals);
+    if (exitflag) *exitflag = flag;
+    if (flag < 0) return DUGMA_ERR_NUMERIC;
+    if (D == 3) {
+        const Mat3 Q = expso3(p.data());
+        memcpy(dR, Q.a, sizeof(Q.a));
+        for (int a = 0; a < 3; ++a) dt[a] = p[3 + a];
+    } else {
+        dR[0] = std::cos(p[0]);
+        dR[1] = std::sin(p[0]);
+        dR[2] = -std::sin(p[0]);
+        dR[3] = std::cos(p[0]);
+        dt[0] = p[1];
+        dt[1] = p[2];
+    }
+    if (Qmin) *Qmin = F.value(p.data());
+    return DUGMA_OK;
+}
+
+extern "C" int dugma_register(const double* X, const double* X_C, const double* Y, const double* Y_C, int N, int M,
+                              int D, const double* R0, const double* t0, int max_iter, double acc_rot,
+                              double acc_trans, double acc_sig, int mode, double* R_out, double* t_out,
+                              double* stats)
+{
+    if (!X || !X_C || !Y || !Y_C || !R0 || !t0 || !R_out || !t_out) return DUGMA_ERR_ARG;
+    if (D != 2 && D != 3) return DUGMA_ERR_ARG;
+    if (mode != DUGMA_DRIVE_REFERENCE && mode != DUGMA_DRIVE_DIRECT) return DUGMA_ERR_ARG;
+    Timer timer;
+    // normalize.m:3-26: centre each cloud, divide both by the larger RMS radius
+    double xd[3] = {0, 0, 0}, yd[3] = {0, 0, 0};
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < D; ++a) xd[a] += X[(size_t)i * D + a] / N;
+    for (int j = 0; j < M; ++j)
+        for (int a = 0; a < D; ++a) yd[a] += Y[(size_t)j * D + a] / M;
+    double xs = 0, ys = 0;
+    std::vector<double> Xn((size_t)N * D), Yn((size_t)M * D);
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < D; ++a) {
+            Xn[(size_t)i * D + a] = X[(size_t)i * D + a] - xd[a];
+            xs += Xn[(size_t)i * D + a] * Xn[(size_t)i * D + a];
+        }
+    for (int j = 0; j < M; ++j)
+        for (int a = 0; a < D; ++a) {
+            Yn[(size_t)j * D + a] = Y[(size_t)j * D + a] - yd[a];
+            ys += Yn[(size_t)j * D + a] * Yn[(size_t)j * D + a];
+        }
+    const double scale = std::max(std::sqrt(xs / N), std::sqrt(ys / M));
+    if (!(scale > 0)) return DUGMA_ERR_ARG;
+    for (double& v : Xn) v /= scale;
+    for (double& v : Yn) v /= scale;
+    // covariances are passed unscaled, as DUGMA.m:44 does
+    float* Ptr[6];
+    double ok = 0;
+    int rc = dugma_init(Xn.data(), X_C, Yn.data(), Y_C, &ok, N, M, D, Ptr);
+    if (rc != DUGMA_OK && rc != DUGMA_ERR_NONPD) return rc;
+    double R[9] = {0}, t[3] = {0};
+    for (int k = 0; k < D * D; ++k) R[k] = R0[k];
+    for (int a = 0; a < D; ++a) t[a] = t0[a];
+    const double Nd = N, Md = M, Dd = D;
+    float sigf = 0;
+    int evals = 0;
+    rc = dugma_update_sig(Ptr, R, t, &Nd, &Md, &Dd, &sigf);
+    double sig = sigf;
+    const int NR = D == 3 ? 3 : 1;
+    double angle[3] = {1e4, 1e4, 1e4}, angle0[3];
+    double tprev[3] = {t[0], t[1], t[2]};
+    bool con_angle = true;
+    int exitflag = 1, iter = 1;
+    double E = 0;
+    auto tdiff2 = [&]() {
+        double s = 0;
+        for (int a = 0; a < D; ++a) s += (tprev[a] - t[a]) * (tprev[a] - t[a]);
+        return s;
+    };
+    while (rc == DUGMA_OK && iter <= max_iter && (con_angle || std::fabs(tdiff2()) > acc_trans) && sig > acc_sig) {
+        double dRm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, dt[3] = {0, 0, 0};
+        if (mode == DUGMA_DRIVE_REFERENCE) {
+            double A[640];
+            rc = dugma_compi(Ptr, R, t, &Nd, &Md, &Dd, &sig, A);
+            if (rc != DUGMA_OK) break;
+            SurrogateInP F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
+                            D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
+                           D};
+            std::vector<double> p;
+            exitflag = minimise_surrogate(F, p, &evals);
+            if (exitflag < 0) break;
+            if (D == 3) {
+                const Mat3 Q = expso3(p.data());
+                memcpy(dRm, Q.a, sizeof(Q.a));
+                for (int a = 0; a < 3; ++a) dt[a] = p[3 + a];
+            } else {
+                dRm[0] = std::cos(p[0]);
+                dRm[1] = std::sin(p[0]);
+                dRm[2] = -std::sin(p[0]);
+                dRm[3] = std::cos(p[0]);
+                dt[0] = p[1];
+                dt[1] = p[2];
+            }
+        } else {
+            // BFGS ascent of E on the left-perturbation coordinates at fixed sig
+            const int n = NR + D;
+            double g[6];
+            rc = dugma_energy_grad(Ptr, R, t, sig, DUGMA_MODEL_REF, &E, g, nullptr);
+            ++evals;
+            if (rc != DUGMA_OK) break;
+            std::vector<double> Hi(n * n, 0.0);
+            double gn = 0;
+            for (int k = 0; k < n; ++k) gn += g[k] * g[k];
+            gn = std::sqrt(gn);
+            for (int k = 0; k < n; ++k) Hi[k * n + k] = gn > 0 ? 0.05 / gn : 0.0;
+            double Rc[9], tc[3];
+            memcpy(Rc, R, sizeof(Rc));
+            memcpy(tc, t, sizeof(tc));
+            for (int it = 0; it < 25 && rc == DUGMA_OK; ++it) {
+                double s[6] = {0}, Rn[9], tn[3], En = 0, gnew[6];
+                for (int r = 0; r < n; ++r)
+                    for (int c = 0; c < n; ++c) s[r] += Hi[r * n + c] * g[c];   // ascent direction
+                double alpha = 1.0;
+                bool ok2 = false;
+                for (int bt = 0; bt < 20; ++bt) {
+                    double w[3] = {0, 0, 0};
+                    for (int k = 0; k < NR; ++k) w[D == 3 ? k : 2] = alpha * s[k];
+                    Mat3 Q{};
+                    if (D == 3) {
+                        Q = expso3(w);
+                        Mat3 Rm{};
+                        memcpy(Rm.a, Rc, sizeof(Rm.a));
+                        const Mat3 P = mul(Q, Rm);
+                        memcpy(Rn, P.a, sizeof(P.a));
+                    } else {
+                        const double c = std::cos(w[2]), sn = std::sin(w[2]);
+                        Rn[0] = c * Rc[0] - sn * Rc[1];
+                        Rn[1] = sn * Rc[0] + c * Rc[1];
+                        Rn[2] = c * Rc[2] - sn * Rc[3];
+                        Rn[3] = sn * Rc[2] + c * Rc[3];
+                    }
+                    for (int a = 0; a < D; ++a) tn[a] = tc[a] + alpha * s[NR + a];
+                    rc = dugma_energy_grad(Ptr, Rn, tn, sig, DUGMA_MODEL_REF, &En, gnew, nullptr);
+                    ++evals;
+                    if (rc != DUGMA_OK) break;
+                    double dir = 0;
+                    for (int k = 0; k < n; ++k) dir += g[k] * s[k];
+                    if (En >= E + 1e-4 * alpha * dir) {
+                        ok2 = true;
+                        break;
+                    }
+                    alpha *= 0.5;
+                }
+                if (!ok2 || rc != DUGMA_OK) break;
+                // BFGS update for the inverse Hessian of -E in the new tangent coordinates
+                double sv[6], yv[6], sy = 0;
+                for (int k = 0; k < n; ++k) {
+                    sv[k] = alpha * s[k];
+                    yv[k] = -(gnew[k] - g[k]);
+                    sy += sv[k] * yv[k];
+                }
+                if (sy > 1e-300) {
+                    std::vector<double> Hy(n, 0.0);
+                    double yHy = 0;
+                    for (int r = 0; r < n; ++r)
+                        for (int c = 0; c < n; ++c) Hy[r] += Hi[r * n + c] * yv[c];
+                    for (int r = 0; r < n; ++r) yHy += yv[r] * Hy[r];
+                    for (int r = 0; r < n; ++r)
+                        for (int c = 0; c < n; ++c)
+                            Hi[r * n + c] += (sy + yHy) * sv[r] * sv[c] / (sy * sy) - (Hy[r] * sv[c] + sv[r] * Hy[c]) / sy;
+                }
+                double stepn = 0;
+                for (int k = 0; k < n; ++k) stepn += sv[k] * sv[k];
+                const double dE = En - E;
+                memcpy(Rc, Rn, sizeof(Rc));
+                memcpy(tc, tn, sizeof(tc));
+                E = En;
+                memcpy(g, gnew, sizeof(g));
+                if (std::sqrt(stepn) < 1e-10 || dE <= 1e-12 * std::fabs(E)) break;
+            }
+            if (rc != DUGMA_OK) break;
+            // express the accepted pose as (dR, dt) relative to (R, t) for the common update below
+            if (D == 3) {
+                Mat3 Rn{}, Rt{};
+                memcpy(Rn.a, Rc, sizeof(Rn.a));
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) Rt(r, c) = R[c + 3 * r];
+                const Mat3 Q = mul(Rn, Rt);
+                memcpy(dRm, Q.a, sizeof(Q.a));
+            } else {
+                const double c = Rc[0] * R[0] + Rc[1] * R[1], sn = Rc[1] * R[0] - Rc[0] * R[1];
+                dRm[0] = c;
+                dRm[1] = sn;
+                dRm[2] = -sn;
+                dRm[3] = c;
+            }
+            for (int a = 0; a < D; ++a) dt[a] = tc[a] - t[a];
+        }
+        // DUGMA.m:76-80: t <- dt + t, R <- dR R
+        for (int a = 0; a < D; ++a) {
+            tprev[a] = t[a];
+            t[a] = dt[a] + t[a];
+        }
+        double Rn[9];
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double s = 0;
+                for (int k = 0; k < D; ++k) s += dRm[r + D * k] * R[k + D * c];
+                Rn[r + D * c] = s;
+            }
+        memcpy(R, Rn, sizeof(double) * D * D);
+        memcpy(angle0, angle, sizeof(angle));
+        if (D == 3) {
+            Mat3 Rm{};
+            memcpy(Rm.a, R, sizeof(Rm.a));
+            rotm2eul(Rm, angle);
+            con_angle = std::fabs(angle0[0] - angle[0]) > acc_rot || std::fabs(angle0[1] - angle[1]) > acc_rot ||
+                        std::fabs(angle0[2] - angle[2]) > acc_rot;
+        } else {
+            angle[0] = std::asin(std::max(-1.0, std::min(1.0, R[1]))) * 180.0 / M_PI;   // asind(R(2))
+            con_angle = std::fabs(angle0[0] - angle[0]) > acc_rot;
+        }
+        rc = dugma_update_sig(Ptr, R, t, &Nd, &Md, &Dd, &sigf);
+        sig = sigf;
+        ++iter;
+    }
+    if (rc == DUGMA_OK) {
+        double gtmp[6];
+        dugma_energy_grad(Ptr, R, t, sig, DUGMA_MODEL_REF, &E, gtmp, nullptr);
+    }
+    dugma_fr_m(Ptr);
+    if (rc != DUGMA_OK) return rc;
+    if (exitflag < 0) {   // DUGMA.m:116-118: an unsolvable surrogate returns the identity
+        for (int k = 0; k < D * D; ++k) R_out[k] = (k % (D + 1) == 0) ? 1.0 : 0.0;
+        for (int a = 0; a < D; ++a) t_out[a] = 0.0;
+    } else {
+        // DUGMA.m:122: t = xd + t * scale - R * yd
+        for (int k = 0; k < D * D; ++k) R_out[k] = R[k];
+        for (int a = 0; a < D; ++a) {
+            double Ry = 0;
+            for (int k = 0; k < D; ++k) Ry += R[a + D * k] * yd[k];
+            t_out[a] = xd[a] + t[a] * scale - Ry;
+        }
+    }
+    if (stats) {
+        stats[0] = iter - 1;
+        stats[1] = sig;
+        stats[2] = E;
+        stats[3] = exitflag;
+        stats[4] = timer.s();
+        stats[5] = evals;
+        stats[6] = scale;
+        stats[7] = 0;
+    }
+    return DUGMA_OK;
 }

@@ -190,6 +190,13 @@ int dugma_timing(float* Ptr[6], int mode, double* total_ms, int* launches);
  * kernel time in ms). */
 int dugma_calibrate(int what, double* lane_ops_per_s, double* ms);
 
+/* The solver the driver uses in place of fmincon (DUGMA.m:73 with energy3D.m / fcontr3D.m;
+ * 2D: DUGMA.m:65 with energy2D.m / fcontr2D.m): minimises Q(dR, dt) = sum_k A_k b_k(dR, dt) over
+ * dR in SO(D) (dR = exp([w]x), 2D a rotation by theta) and dt, from dR = I, dt = 0.
+ * A: the 637 (3D) / 45 (2D) coefficients of dugma_compi.  Writes dR (D x D col-major), dt,
+ * the minimum value and an exit flag (> 0 converged, 0 iteration limit, < 0 failed). */
+int dugma_minimise_surrogate(int D, const double* A, double* dR, double* dt, double* Qmin, int* exitflag);
+
 /* Library build/version string. */
 const char* dugma_version(void);
 

@@ -191,6 +191,45 @@ def test_every_kernel_shape_matches_oracle(what, D):
         api.fr_m(h)
 
 
+@pytest.mark.parametrize("D", [3, 2])
+def test_conv_model_matches_oracle(D):
+    """CONV: per-pair combined covariance, its own determinant and inverse."""
+    X, XC, Y, YC = _problem_small(D, 600, 777, seed=31)
+    st = orc.State(X, XC, Y, YC)
+    _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D, seed=12)
+        for sig in (0.05, 0.5):
+            Eo, go, dxo = st.energy_conv(R, t, sig, with_dx=True)
+            E, g, dx = api.energy_grad(h, R, t, sig, model=1, with_dx=True)
+            assert abs(E - Eo) <= 1e-6 * Eo, (E, Eo)
+            assert _rel(g, go) <= 1e-5, (g, go)
+            assert _rel(dx, dxo) <= 1e-4
+            assert abs(api.energy(h, R, t, sig, model=1) - Eo) <= 1e-6 * Eo
+    finally:
+        api.fr_m(h)
+
+
+def test_conv_near_singular_pairs_use_fp64_inverse():
+    """Nearly degenerate covariances on both sides: combined covariances of condition ~1e7."""
+    rng = np.random.default_rng(5)
+    n = 400
+    X = rng.standard_normal((n, 3)) * 0.3
+    Y = X + 1e-4 * rng.standard_normal((n, 3))
+    v = np.array([1.0, 1.0, 1.0]) / np.sqrt(3.0)     # off-axis, so the matrices are far from diagonal
+    XC = np.tile(np.eye(3) * 1e-9 + 1e-2 * np.outer(v, v), (n, 1, 1))
+    YC = np.tile(np.eye(3) * 1e-9 + 1e-2 * np.outer(v, v), (n, 1, 1))
+    st = orc.State(X, XC, Y, YC)
+    _, h = api.init(X, XC, Y, YC)
+    try:
+        Eo, go, _ = st.energy_conv(np.eye(3), np.zeros(3), 1.0)
+        E, g, _ = api.energy_grad(h, np.eye(3), np.zeros(3), 1.0, model=1)
+        print(f"near-singular CONV: energy rel err {abs(E - Eo) / Eo:.3e}, grad rel err {_rel(g, go):.3e}")
+        assert abs(E - Eo) <= 1e-5 * Eo
+    finally:
+        api.fr_m(h)
+
+
 def test_energy_adjoint_workload1_ill_conditioned():
     P = synth.workload1()
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
