@@ -88,26 +88,67 @@ __global__ void conv_prologue_kernel(const double* __restrict__ pose, const floa
     }
 }
 
-// adjugate (packed) and determinant of a packed symmetric matrix, FP64 (ill-conditioned pairs)
+// A near-singular pair recomputed entirely in FP64 from the stored FP32 inputs: the target
+// covariance is rotated again from Sigma_y_j (packed, / c) with R in FP64, added to the
+// source covariance, and the difference d is formed from x and the y' split exactly.
+// Returns false (no contribution) when the combined covariance is not positive definite.
 template <int D>
-__device__ __forceinline__ void adj_det_f64(const float* s, double* adj, double& det)
+__device__ __noinline__ bool conv_pair_f64(const float* xi, const float* sxi, float4 v0, float4 v1,
+                                           const float* __restrict__ cy, const double* __restrict__ pose, double kl,
+                                           float* adj, float* h, float* rd, float* Nt)
 {
-    if (D == 3) {
-        const double a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5];
-        adj[0] = b * c - f * f;
-        adj[1] = a * c - e * e;
-        adj[2] = a * b - d * d;
-        adj[3] = e * f - d * c;
-        adj[4] = d * f - b * e;
-        adj[5] = d * e - a * f;
-        det = a * adj[0] + d * adj[3] + e * adj[4];
-    } else {
-        const double a = s[0], b = s[1], c = s[2];
-        adj[0] = b;
-        adj[1] = a;
-        adj[2] = -c;
-        det = a * b - c * c;
+    constexpr int NS = Sym<D>::N;
+    double A[3][3], T[3][3], S[6];
+    for (int k = 0; k < NS; ++k) {
+        const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+        A[ra][rb] = A[rb][ra] = (double)cy[k];
     }
+    for (int r0 = 0; r0 < D; ++r0)
+        for (int c0 = 0; c0 < D; ++c0) {
+            double acc = 0;
+            for (int k = 0; k < D; ++k) acc += A[r0][k] * pose[c0 + D * k];
+            T[r0][c0] = acc;
+        }
+    for (int k = 0; k < NS; ++k) {
+        double acc = 0;
+        for (int q = 0; q < D; ++q) acc += pose[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
+        S[k] = acc + (double)sxi[k];
+    }
+    const double yh[3] = {v0.x, v0.y, v0.z}, yl[3] = {v1.x, v1.y, v1.z};
+    double d[3], ad[6], det;
+    for (int q = 0; q < D; ++q) d[q] = ((double)xi[q] - yh[q]) - yl[q];
+    if (D == 3) {
+        const double a = S[0], b = S[1], c = S[2], e4 = S[3], f5 = S[4], g6 = S[5];
+        ad[0] = b * c - g6 * g6;
+        ad[1] = a * c - f5 * f5;
+        ad[2] = a * b - e4 * e4;
+        ad[3] = f5 * g6 - e4 * c;
+        ad[4] = e4 * g6 - b * f5;
+        ad[5] = e4 * f5 - a * g6;
+        det = a * ad[0] + e4 * ad[3] + f5 * ad[4];
+    } else {
+        ad[0] = S[1];
+        ad[1] = S[0];
+        ad[2] = -S[2];
+        det = S[0] * S[1] - S[2] * S[2];
+    }
+    if (!(det > 0)) return false;
+    double hh[3], m = 0;
+    if (D == 3) {
+        hh[0] = ad[0] * d[0] + ad[3] * d[1] + ad[4] * d[2];
+        hh[1] = ad[3] * d[0] + ad[1] * d[1] + ad[5] * d[2];
+        hh[2] = ad[4] * d[0] + ad[5] * d[1] + ad[2] * d[2];
+    } else {
+        hh[0] = ad[0] * d[0] + ad[2] * d[1];
+        hh[1] = ad[2] * d[0] + ad[1] * d[1];
+    }
+    for (int q = 0; q < D; ++q) m += d[q] * hh[q];
+    const double r = 1.0 / det;
+    *Nt = (float)(sqrt(r) * exp2(m * r * kl));
+    *rd = (float)r;
+    for (int q = 0; q < D; ++q) h[q] = (float)hh[q];
+    for (int k = 0; k < NS; ++k) adj[k] = (float)ad[k];
+    return true;
 }
 
 template <int D, int IPT_, bool GRAD>
@@ -122,11 +163,15 @@ struct ConvBody {
     int row[IPT];
     float kl;          // -1/2 log2(e) / lam
     double c0, lam, t[3];
+    const float* ycov;
+    const double* pose;
 
     __device__ void setup(const PairArgs& a)
     {
         lam = a.pose[kPoseSig] * a.Lmax;   // Lmax carries the covariance scale c for this body
         kl = (float)(K_EXP2 / lam);
+        ycov = a.ycov;
+        pose = a.pose;
         c0 = pow(2.0 * 3.14159265358979323846 * lam, -0.5 * D);
         for (int q = 0; q < D; ++q) t[q] = a.pose[kPoseT + q];
     }
@@ -169,16 +214,17 @@ struct ConvBody {
             }
         }
     }
-    __device__ __forceinline__ void consume(const YRec& r, int)
+    __device__ __forceinline__ void consume(const YRec& r, int j)
     {
         const float4 v0 = r.v0, v1 = r.v1, v2 = r.v2, v3 = r.v3;
         if (v0.w == 0.f) return;   // padding target (uniform across the block)
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
-            float d[3], s[6], adj[6], det, h[3];
+            float d[3], s[6], adj[6], det, h[3], rd, Nt;
             d[0] = (x[ii][0] - v0.x) - v1.x;
             d[1] = (x[ii][1] - v0.y) - v1.y;
             if (D == 3) d[2] = (x[ii][2] - v0.z) - v1.z;
+            bool near_singular;
             if (D == 3) {
                 s[0] = sx[ii][0] + v2.x; s[1] = sx[ii][1] + v2.y; s[2] = sx[ii][2] + v2.z;
                 s[3] = sx[ii][3] + v2.w; s[4] = sx[ii][4] + v3.x; s[5] = sx[ii][5] + v3.y;
@@ -189,13 +235,7 @@ struct ConvBody {
                 adj[4] = fmaf(s[3], s[5], -s[1] * s[4]);
                 adj[5] = fmaf(s[3], s[4], -s[0] * s[5]);
                 det = fmaf(s[4], adj[4], fmaf(s[3], adj[3], s[0] * adj[0]));
-                const float diag = s[0] * s[1] * s[2];
-                if (det < 1e-6f * diag) {   // near-singular: adjugate and determinant in FP64
-                    double ad[6], dd;
-                    adj_det_f64<3>(s, ad, dd);
-                    for (int q = 0; q < 6; ++q) adj[q] = (float)ad[q];
-                    det = (float)dd;
-                }
+                near_singular = det < 1e-6f * (s[0] * s[1] * s[2]);
                 h[0] = fmaf(adj[4], d[2], fmaf(adj[3], d[1], adj[0] * d[0]));
                 h[1] = fmaf(adj[5], d[2], fmaf(adj[1], d[1], adj[3] * d[0]));
                 h[2] = fmaf(adj[2], d[2], fmaf(adj[5], d[1], adj[4] * d[0]));
@@ -205,22 +245,24 @@ struct ConvBody {
                 adj[1] = s[0];
                 adj[2] = -s[2];
                 det = fmaf(s[0], s[1], -s[2] * s[2]);
-                if (det < 1e-6f * s[0] * s[1]) {
-                    double ad[3], dd;
-                    adj_det_f64<2>(s, ad, dd);
-                    for (int q = 0; q < 3; ++q) adj[q] = (float)ad[q];
-                    det = (float)dd;
-                }
+                near_singular = det < 1e-6f * (s[0] * s[1]);
                 h[0] = fmaf(adj[2], d[1], adj[0] * d[0]);
                 h[1] = fmaf(adj[1], d[1], adj[2] * d[0]);
             }
-            if (!(det > 0.f)) continue;   // not positive definite: no contribution (as the oracle)
-            float m = d[0] * h[0];
+            if (near_singular) {
+                // condition around 1e6 or worse: the whole pair in FP64
+                if (!conv_pair_f64<D>(x[ii], sx[ii], v0, v1, ycov + (size_t)j * NS, pose, (double)kl, adj, h, &rd,
+                                      &Nt))
+                    continue;
+            } else {
+                if (!(det > 0.f)) continue;   // not positive definite: no contribution (as the oracle)
+                float m = d[0] * h[0];
 #pragma unroll
-            for (int q = 1; q < D; ++q) m = fmaf(d[q], h[q], m);
-            const float rs = rsqrtf(det);
-            const float rd = rs * rs;
-            const float Nt = rs * ex2(m * (rd * kl));
+                for (int q = 1; q < D; ++q) m = fmaf(d[q], h[q], m);
+                const float rs = rsqrtf(det);
+                rd = rs * rs;
+                Nt = rs * ex2(m * (rd * kl));
+            }
             e[ii] += Nt;
             if (GRAD) {
                 const float nr = Nt * rd, nr2 = nr * rd;

@@ -25,6 +25,10 @@
 #include "dugma.h"
 #include "monomials.h"
 
+namespace dugma {
+int set_error(int code, const char* fmt, ...);
+}
+
 namespace {
 
 using Vec = std::vector<double>;
@@ -308,9 +312,12 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
                               double acc_trans, double acc_sig, int mode, double* R_out, double* t_out,
                               double* stats)
 {
-    if (!X || !X_C || !Y || !Y_C || !R0 || !t0 || !R_out || !t_out) return DUGMA_ERR_ARG;
-    if (D != 2 && D != 3) return DUGMA_ERR_ARG;
-    if (mode != DUGMA_DRIVE_REFERENCE && mode != DUGMA_DRIVE_DIRECT) return DUGMA_ERR_ARG;
+    if (!X || !X_C || !Y || !Y_C || !R0 || !t0 || !R_out || !t_out)
+        return dugma::set_error(DUGMA_ERR_ARG, "register: null argument");
+    if (D != 2 && D != 3) return dugma::set_error(DUGMA_ERR_ARG, "register: D must be 2 or 3");
+    if (mode != DUGMA_DRIVE_REFERENCE && mode != DUGMA_DRIVE_DIRECT)
+        return dugma::set_error(DUGMA_ERR_ARG, "register: unknown mode %d", mode);
+    if (N < 2 || M < 2) return dugma::set_error(DUGMA_ERR_ARG, "register: each cloud needs at least 2 points");
     Timer timer;
     // normalize.m:3-26: centre each cloud, divide both by the larger RMS radius
     double xd[3] = {0, 0, 0}, yd[3] = {0, 0, 0};
@@ -331,7 +338,7 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
             ys += Yn[(size_t)j * D + a] * Yn[(size_t)j * D + a];
         }
     const double scale = std::max(std::sqrt(xs / N), std::sqrt(ys / M));
-    if (!(scale > 0)) return DUGMA_ERR_ARG;
+    if (!(scale > 0)) return dugma::set_error(DUGMA_ERR_ARG, "register: both clouds collapse to a point");
     for (double& v : Xn) v /= scale;
     for (double& v : Yn) v /= scale;
     // covariances are passed unscaled, as DUGMA.m:44 does

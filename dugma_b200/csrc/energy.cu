@@ -631,6 +631,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     a.wx = c.wx;
     a.wy = c.wy;
     a.xcov = c.xcov;
+    a.ycov = c.ycov;
     a.pose = pose_dev;
     a.Lmax = Lmax;
     a.N = c.N;

@@ -19,6 +19,7 @@ struct PairArgs {
     const float* wx;       // |Sigma_x|^-1/2 per source (FP32 state)
     const float* wy;       // |Sigma_y|^-1/2 per target
     const float* xcov;     // packed FP32 covariances (CONV)
+    const float* ycov;
     const double* pose;    // R, t, sig
     double Lmax;           // REF: log2 weight offset of the streamed side; CONV: covariance scale
     int N;                 // number of real source rows

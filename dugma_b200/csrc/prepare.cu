@@ -128,7 +128,8 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     for (size_t i = 0; i < (size_t)M; ++i)
         for (int a = 0; a < D; ++a) tr += YC[i * D * D + a * (D + 1)];
     tr /= (double)D * (N + M);
-    c.cscale = (std::isfinite(tr) && tr > 0) ? tr : 1.0;
+    // a power of two, so that dividing by it is exact in FP32
+    c.cscale = (std::isfinite(tr) && tr > 0) ? std::exp2(std::round(std::log2(tr))) : 1.0;
     const double inv = 1.0 / c.cscale;
     if (D == 3) {
         init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, inv, c.counter);
