@@ -72,6 +72,24 @@ def workload(wl, n=0):
     return synth.WORKLOADS[wl](n=n) if n else synth.WORKLOADS[wl]()
 
 
+def config_for(P):
+    """The workload description, shared by both arms."""
+    return {"workload": f"{P.name}: N=M={P.N}, REF model energy + pose gradient per step, one multistart pose "
+                        "per GPU", "l2": "flushed between steps (256 MiB write)"}
+
+
+def profiled_traffic(shape_key):
+    """DRAM bytes per launch of the adjoint kernel from the committed ncu summary, when this run
+    uses the profiled kernel shape on the profiled workload; otherwise None."""
+    path = os.path.join(ROOT, "profiles", "adjoint_packed_harmonic64k.txt")
+    if shape_key != (2, 128, 32, 2) or not os.path.exists(path):
+        return None
+    for line in open(path):
+        if "traffic_bytes_per_launch:" in line:
+            return float(line.split(":")[1])
+    return None
+
+
 def eval_pose(P, rank):
     """The pose of rank r: ground truth perturbed by a seeded multistart offset (rank 0: 10 deg, 2 cm)."""
     from dugma_b200.pose import expmap
@@ -171,7 +189,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "energy+grad pair-terms/s", "value": val, "unit": "pair-terms/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{P.name} N=M={P.N}, energy + pose gradient, REF model"},
+            "config": config_for(P),
             "cpu_baseline": {"value": val, "unit": "pair-terms/s", "cores": orc.num_threads(), "kind": "port",
                              "sample": f"{rows} source rows x {st.M} targets per step"},
             "e2e": {"value": val, "unit": "pair-terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -199,10 +217,16 @@ def main():
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
     sig = api.update_sig(h, R, t)
     if args.shape:
-        api.set_shape(h, 0, [int(v) for v in args.shape.split(",")])
+        shape_key = tuple(int(v) for v in args.shape.split(","))
+        api.set_shape(h, 0, shape_key)
         tune = f"pinned {args.shape}"
     else:
         tune = "" if args.no_tune else api.autotune(h, 0)
+        shape_key = api.shapes(0)[0]
+        if tune:
+            import re
+            best = min(re.findall(r"\(ipt=(\d+),nt=(\d+),tj=(\d+),pack=(\d+)\):([0-9.]+)ms", tune), key=lambda m: float(m[4]))
+            shape_key = tuple(int(v) for v in best[:4])
     if not args.no_fd and not args.shape and not args.no_tune:
         api.autotune(h, 1)     # the plain form's energy kernel gets the same treatment
     pairs = P.N * P.M
@@ -320,12 +344,14 @@ def main():
             "metric": "energy+grad pair-terms/s", "value": value, "unit": "pair-terms/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{P.name}: N=M={P.N}, REF model energy + pose gradient (fused adjoint), "
-                                   "one multistart pose per GPU", "l2": "flushed between steps (256 MiB write)",
-                       "sigma": sig, "kernel_shape": tune.split(" ")[0] if tune else None},
+            "config": config_for(P),
+            "details": {"sigma": sig, "kernel_shape": list(shape_key)},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
                          "unit": "Tinstr/s (FP32 pipe, lane ops)", "frac": achieved / peak.value,
-                         "traffic": None, "peak_source": "FP32 FMA-chain kernel measured in this run",
+                         "traffic": profiled_traffic(shape_key) if (args.workload == 2 and not args.n) else None,
+                         "algorithmic_bytes": 64 * (P.N + P.M),
+                         "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json has "
+                                        "no FP32-pipe figure)",
                          "sfu_frac": sfu_frac, "kernel_ms": kernel_ms,
                          "instr_per_pair": FP32_INSTR_ADJOINT},
             "gpu_launches": 3 * args.steps,

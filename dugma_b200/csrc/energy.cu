@@ -503,22 +503,23 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
-// deterministic reduction of per-item partials: out[v] = sum_items partials[item][v]
-__global__ void reduce_items_kernel(const double* __restrict__ part, int n_items, int nv, double* __restrict__ out)
+// deterministic reduction of per-item partials: out[v] = sum_items partials[item][v];
+// block v sums value v in a fixed order (strided per thread, then a fixed tree)
+__global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __restrict__ part, int n_items, int nv,
+                                                             double* __restrict__ out)
 {
-    __shared__ double red[256];
-    for (int v = 0; v < nv; ++v) {
-        double s = 0;
-        for (int it = threadIdx.x; it < n_items; it += blockDim.x) s += part[(size_t)it * 8 + v];
-        red[threadIdx.x] = s;
-        __syncthreads();
-        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) out[v] = red[0];
+    __shared__ double red[1024];
+    const int v = blockIdx.x;
+    if (v >= nv) return;
+    double s = 0;
+    for (int it = threadIdx.x; it < n_items; it += blockDim.x) s += part[(size_t)it * 8 + v];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
         __syncthreads();
     }
+    if (threadIdx.x == 0) out[v] = red[0];
 }
 
 __global__ void reduce_chunks_kernel(const double* __restrict__ part, int n_jc, size_t n, double* __restrict__ out)
@@ -666,7 +667,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     DUGMA_CK(cudaGetLastError());
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
     if (out_dev) {
-        reduce_items_kernel<<<1, 256, 0, s>>>(a.partials, n_items, nv, out_dev);
+        reduce_items_kernel<<<nv, 1024, 0, s>>>(a.partials, n_items, nv, out_dev);
         DUGMA_CK(cudaGetLastError());
     }
     if (dEdx_dev) {
