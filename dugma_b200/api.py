@@ -184,6 +184,47 @@ def set_shape(h: Handles, what, shape):
     check(_lib.load().dugma_set_shape(h.arr, int(what), *[int(v) for v in shape]))
 
 
+class Batch:
+    """Many registration problems (uneven sizes) evaluated together: one persistent launch
+    per evaluation over every (problem, pose) pair, replayed as a CUDA graph after the first."""
+
+    def __init__(self, problems):
+        """problems: sequence of (X, X_C, Y, Y_C) in the layout of init."""
+        D = np.shape(problems[0][0])[1]
+        self.D = D
+        self._keep = []
+        arrs = []
+        for (X, XC, Y, YC) in problems:
+            a = (_d(X), _blocks(XC), _d(Y), _blocks(YC))
+            self._keep.append(a)
+            arrs.append(a)
+        P = len(arrs)
+        self.P = P
+        N = (ctypes.c_int * P)(*[a[0].shape[0] for a in arrs])
+        M = (ctypes.c_int * P)(*[a[2].shape[0] for a in arrs])
+        ptr = lambda k: (_dp * P)(*[_ptr(a[k]) for a in arrs])
+        self.b = ctypes.c_void_p()
+        check(_lib.load().dugma_batch_create(P, D, N, M, ptr(0), ptr(1), ptr(2), ptr(3), ctypes.byref(self.b)))
+
+    def energy_grad(self, R, t, sig):
+        """R (P, Q, D, D), t (P, Q, D), sig (P, Q) -> E (P, Q), g (P, Q, NG)."""
+        R, t, sig = np.asarray(R, float), np.asarray(t, float), np.asarray(sig, float)
+        P, Q = sig.shape
+        rec = np.zeros((P, Q, 13))
+        rec[:, :, : self.D * self.D] = np.transpose(R, (0, 1, 3, 2)).reshape(P, Q, -1)
+        rec[:, :, 9:9 + self.D] = t
+        rec[:, :, 12] = sig
+        ng = ngrad(self.D)
+        out = np.zeros((P, Q, 1 + ng))
+        check(_lib.load().dugma_batch_energy_grad(self.b, Q, _ptr(_d(rec)), 0, _ptr(out)))
+        return out[:, :, 0].copy(), out[:, :, 1:].copy()
+
+    def close(self):
+        if self.b:
+            check(_lib.load().dugma_batch_destroy(self.b))
+            self.b = ctypes.c_void_p()
+
+
 class Graph:
     """A captured energy+gradient evaluation, replayed per pose."""
 

@@ -1,15 +1,459 @@
-// batch.cu -- many registration problems in one persistent launch.
+// batch.cu -- many registration problems of uneven sizes, each with many multistart poses,
+// evaluated (energy + pose gradient, REF model) in one persistent launch.
+//
+// A batch owns one context per problem (the init state of each cloud pair).  An evaluation
+//   1. uploads the poses (problem p, pose q) -> pq = p * n_poses + q;
+//   2. runs one prologue over all (pq, target) and (pq, source) pairs, writing paired
+//      target records (YRec2) and source records per pq;
+//   3. runs one persistent adjoint launch over a global list of work items
+//      (pq, source block, target chunk) sorted by cost, largest first, handed out by an
+//      atomic counter, each item reducing into its own partial slot;
+//   4. sums each pq's item partials in a fixed order.
+// Steps 2-4 are captured once as a CUDA graph per pose count and replayed afterwards.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "bodies.cuh"
 #include "context.hpp"
 
+namespace dugma {
+
+constexpr int kBatchNT = 128, kBatchTJ = 32, kBatchIPT = 2, kBatchChunk = 512;   // chunk in pair records
+
+struct PQDesc {
+    const float *x, *xinv, *lwx, *y, *yinv, *lwy, *wx;
+    const double* pose;
+    XRec* xrec;
+    YRec2* yrec;
+    double Lmax;
+    int N, M, M_pad;
+};
+
+struct BatchItem {
+    int pq, ib, tile0, ntiles;
+};
+
+// one block row per pq: targets (paired layout, kC' unmodified) then sources
+template <int D>
+__global__ void batch_prologue_kernel(const PQDesc* __restrict__ desc, int max_span)
+{
+    constexpr int NS = Sym<D>::N;
+    const PQDesc pd = desc[blockIdx.y];
+    const double* pose = pd.pose;
+    double R[9], t[3];
+    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
+    const double s = 1.0 / pose[kPoseSig], ks = K_EXP2 * s;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < max_span; idx += gridDim.x * blockDim.x) {
+        if (idx < pd.M_pad) {
+            const int j = idx;
+            float f[16];
+            for (int q = 0; q < 16; ++q) f[q] = 0.f;
+            f[3] = -INFINITY;
+            if (j < pd.M && pd.lwy[j] != -INFINITY) {
+                double A[3][3], T[3][3];
+                for (int a = 0; a < D; ++a) {
+                    double v = R[a] * (double)pd.y[(size_t)j * D] + R[a + D] * (double)pd.y[(size_t)j * D + 1];
+                    if (D == 3) v += R[a + 6] * (double)pd.y[(size_t)j * D + 2];
+                    v += t[a];
+                    const float hi = __double2float_rn(v);
+                    f[a] = -hi;
+                    f[4 + a] = -__double2float_rn(v - (double)hi);
+                }
+                f[3] = pd.lwy[j];
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0)
+                        A[r0][c0] = 0.5 * ((double)pd.yinv[(size_t)j * D * D + r0 + D * c0] +
+                                           (double)pd.yinv[(size_t)j * D * D + c0 + D * r0]);
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0) {
+                        double acc = 0;
+                        for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = acc;
+                    }
+                for (int k = 0; k < NS; ++k) {
+                    double acc = 0;
+                    for (int q = 0; q < D; ++q) acc += R[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
+                    f[7 + k] = __double2float_rn(ks * acc);
+                }
+            } else if (j < pd.M) {
+                // neglected target: no contribution, but a finite position
+                for (int a = 0; a < D; ++a) f[a] = -pd.y[(size_t)j * D + a];
+            }
+            float* base = reinterpret_cast<float*>(pd.yrec) + (size_t)(j >> 1) * 32 + (j & 1);
+            for (int q = 0; q < 16; ++q) base[(q >> 1) * 4 + (q & 1) * 2] = f[q];
+        }
+        if (idx < pd.N) {
+            const int i = idx;
+            XRec r;
+            float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
+            for (int a = 0; a < D; ++a) xv[a] = pd.x[(size_t)i * D + a];
+            const float lw = pd.lwx[i];
+            if (lw != -INFINITY)
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    const double b = 0.5 * ((double)pd.xinv[(size_t)i * D * D + ra + D * rb] +
+                                            (double)pd.xinv[(size_t)i * D * D + rb + D * ra]);
+                    bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
+                }
+            r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+            r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+            r.v2 = D == 3 ? make_float4(bp[0], bp[1], bp[2], bp[3]) : make_float4(bp[0], bp[1], bp[2], 0.f);
+            r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            pd.xrec[i] = r;
+        }
+    }
+}
+
+// The persistent skeleton of run_pairs (pairs.cuh) with per-item problem/pose descriptors.
+template <class Body, int NT, int TJ, int STAGES>
+__global__ void __launch_bounds__(NT) batch_pairs_kernel(const PQDesc* __restrict__ desc,
+                                                         const BatchItem* __restrict__ items, int n_items,
+                                                         double* __restrict__ partials, int* counter, int* err)
+{
+    using Rec = typename Body::StreamRec;
+    constexpr int NV = Body::NV;
+    constexpr int BI = Body::IPT * NT;
+    constexpr uint32_t kTileBytes = TJ * sizeof(Rec);
+    __shared__ __align__(128) Rec ybuf[STAGES][TJ];
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ double red[NT / 32][NV];
+    __shared__ int s_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    Body body;
+    uint32_t tcount = 0;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= n_items) break;
+        const BatchItem it = items[item];
+        const PQDesc pd = desc[it.pq];
+        PairArgs a{};
+        a.xrec = pd.xrec;
+        a.yrec = pd.yrec;
+        a.wx = pd.wx;
+        a.pose = pd.pose;
+        a.Lmax = pd.Lmax;
+        a.N = pd.N;
+        a.i0 = 0;
+        a.i_end = pd.N;
+        body.setup(a);
+        const Rec* yg = reinterpret_cast<const Rec*>(pd.yrec);
+        if (tid == 0)
+            for (int k = 0; k < STAGES && k < it.ntiles; ++k) {
+                const int st = (tcount + k) % STAGES;
+                mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                bulk_g2s(&ybuf[st][0], yg + (size_t)(it.tile0 + k) * TJ, kTileBytes, &bars[st]);
+            }
+        for (int ii = 0; ii < Body::IPT; ++ii) body.load_src(a, ii, it.ib * BI + ii * NT + tid);
+        body.zero_all();
+        for (int k = 0; k < it.ntiles; ++k) {
+            const uint32_t u = tcount + k;
+            const int st = u % STAGES;
+            const bool ok = mbar_wait_bounded(&bars[st], (u / STAGES) & 1u, err);
+            const Rec* yb = ybuf[st];
+#pragma unroll 4
+            for (int jj = 0; jj < TJ; ++jj) body.consume(yb[jj], (it.tile0 + k) * TJ + jj);
+            body.fold();
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0)
+                    for (int q = k; q < it.ntiles && q < k + STAGES; ++q) {
+                        const uint32_t uq = tcount + q;
+                        mbar_wait_bounded(&bars[uq % STAGES], (uq / STAGES) & 1u, nullptr);
+                    }
+                return;
+            }
+            if (tid == 0 && k + STAGES < it.ntiles) {
+                mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                bulk_g2s(&ybuf[st][0], yg + (size_t)(it.tile0 + k + STAGES) * TJ, kTileBytes, &bars[st]);
+            }
+        }
+        tcount += it.ntiles;
+        double acc[NV];
+        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+        body.finish(a, 0, acc);
+        block_sum<NV, NT>(acc, &red[0][0]);
+        if (tid == 0)
+            for (int v = 0; v < NV; ++v) partials[(size_t)item * 8 + v] = acc[v];
+    }
+}
+
+// out[pq][v] = sum of the pq's item partials, in the fixed order of its item index list
+__global__ void batch_reduce_kernel(const double* __restrict__ partials, const int* __restrict__ pq_start,
+                                    const int* __restrict__ pq_items, int nv, double* __restrict__ out)
+{
+    __shared__ double red[128];
+    const int pq = blockIdx.x;
+    const int b = pq_start[pq], e = pq_start[pq + 1];
+    for (int v = 0; v < nv; ++v) {
+        double s = 0;
+        for (int k = b + threadIdx.x; k < e; k += blockDim.x) s += partials[(size_t)pq_items[k] * 8 + v];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)pq * nv + v] = red[0];
+        __syncthreads();
+    }
+}
+
+struct Batch {
+    int D = 3, P = 0;
+    std::vector<float*> ptrs;          // 6 per problem
+    std::vector<Context*> ctx;
+    cudaStream_t stream = nullptr;
+    // per pose-count state
+    int n_poses = 0, n_items = 0, nv = 0;
+    void* mem = nullptr;              // one allocation: poses, descriptors, records, items, partials, ...
+    double* poses = nullptr;
+    PQDesc* desc = nullptr;
+    BatchItem* items = nullptr;
+    int *pq_start = nullptr, *pq_items = nullptr, *counter = nullptr, *err = nullptr;
+    double *partials = nullptr, *out = nullptr;
+    double* host = nullptr;           // pinned: poses in, results out
+    size_t host_doubles = 0;
+    int max_span = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+
+    void release_pose_state()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (mem) cudaFree(mem);
+        if (host) cudaFreeHost(host);
+        exec = nullptr;
+        graph = nullptr;
+        mem = nullptr;
+        host = nullptr;
+        n_poses = 0;
+    }
+};
+
+static int batch_prepare(Batch& b, int n_poses)
+{
+    if (b.n_poses == n_poses) return DUGMA_OK;
+    cudaStreamSynchronize(b.stream);
+    b.release_pose_state();
+    const int D = b.D, NG = D == 3 ? 6 : 3;
+    b.nv = 1 + NG;
+    const int n_pq = b.P * n_poses;
+    constexpr int BI = kBatchIPT * kBatchNT;
+    // sizes and the work list (cost = rows x tiles; largest first)
+    std::vector<size_t> yoff(n_pq), xoff(n_pq);
+    size_t ybytes = 0, xbytes = 0;
+    std::vector<BatchItem> items;
+    std::vector<double> cost;
+    b.max_span = 0;
+    for (int p = 0; p < b.P; ++p) {
+        const Context& c = *b.ctx[p];
+        const int total_tiles = c.M_pad / 2 / kBatchTJ;
+        const int chunk_tiles = kBatchChunk / kBatchTJ;
+        b.max_span = std::max(b.max_span, std::max(c.M_pad, c.N));
+        for (int q = 0; q < n_poses; ++q) {
+            const int pq = p * n_poses + q;
+            yoff[pq] = ybytes;
+            ybytes += sizeof(YRec2) * (size_t)(c.M_pad / 2);
+            xoff[pq] = xbytes;
+            xbytes += sizeof(XRec) * (size_t)((c.N + 3) / 4 * 4);
+            for (int ib = 0; ib * BI < c.N; ++ib)
+                for (int t0 = 0; t0 < total_tiles; t0 += chunk_tiles) {
+                    const int nt = std::min(chunk_tiles, total_tiles - t0);
+                    items.push_back({pq, ib, t0, nt});
+                    cost.push_back((double)std::min(BI, c.N - ib * BI) * nt);
+                }
+        }
+    }
+    std::vector<int> order(items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return cost[a] > cost[b2]; });
+    std::vector<BatchItem> sorted(items.size());
+    for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
+    // per-pq item lists in sorted-position order (deterministic reduction order)
+    std::vector<int> pq_start(n_pq + 1, 0), pq_items(sorted.size());
+    for (const BatchItem& it : sorted) ++pq_start[it.pq + 1];
+    for (int k = 0; k < n_pq; ++k) pq_start[k + 1] += pq_start[k];
+    {
+        std::vector<int> fill(pq_start.begin(), pq_start.end() - 1);
+        for (size_t k = 0; k < sorted.size(); ++k) pq_items[fill[sorted[k].pq]++] = (int)k;
+    }
+    b.n_items = (int)sorted.size();
+    // one device allocation for everything pose-dependent
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    const size_t s_poses = up(sizeof(double) * 16 * n_pq), s_desc = up(sizeof(PQDesc) * n_pq),
+                 s_items = up(sizeof(BatchItem) * sorted.size()), s_start = up(sizeof(int) * (n_pq + 1)),
+                 s_list = up(sizeof(int) * sorted.size()), s_ctr = 256, s_part = up(sizeof(double) * 8 * sorted.size()),
+                 s_out = up(sizeof(double) * b.nv * n_pq), s_y = up(ybytes), s_x = up(xbytes);
+    const size_t total = s_poses + s_desc + s_items + s_start + s_list + s_ctr + s_part + s_out + s_y + s_x;
+    if (cudaMalloc(&b.mem, total) != cudaSuccess) {
+        cudaGetLastError();
+        b.mem = nullptr;
+        return set_error(DUGMA_ERR_NOMEM, "batch: cannot allocate %zu bytes", total);
+    }
+    char* m = static_cast<char*>(b.mem);
+    b.poses = reinterpret_cast<double*>(m); m += s_poses;
+    b.desc = reinterpret_cast<PQDesc*>(m); m += s_desc;
+    b.items = reinterpret_cast<BatchItem*>(m); m += s_items;
+    b.pq_start = reinterpret_cast<int*>(m); m += s_start;
+    b.pq_items = reinterpret_cast<int*>(m); m += s_list;
+    b.counter = reinterpret_cast<int*>(m);
+    b.err = b.counter + 4; m += s_ctr;
+    b.partials = reinterpret_cast<double*>(m); m += s_part;
+    b.out = reinterpret_cast<double*>(m); m += s_out;
+    char* ybase = m; m += s_y;
+    char* xbase = m;
+    std::vector<PQDesc> desc(n_pq);
+    for (int p = 0; p < b.P; ++p) {
+        const Context& c = *b.ctx[p];
+        for (int q = 0; q < n_poses; ++q) {
+            const int pq = p * n_poses + q;
+            PQDesc& d = desc[pq];
+            d.x = c.x;
+            d.xinv = c.xinv;
+            d.lwx = c.lwx;
+            d.y = c.y;
+            d.yinv = c.yinv;
+            d.lwy = c.lwy;
+            d.wx = c.wx;
+            d.pose = b.poses + 16 * (size_t)pq;
+            d.xrec = reinterpret_cast<XRec*>(xbase + xoff[pq]);
+            d.yrec = reinterpret_cast<YRec2*>(ybase + yoff[pq]);
+            d.Lmax = c.Lmax_y;
+            d.N = c.N;
+            d.M = c.M;
+            d.M_pad = c.M_pad;
+        }
+    }
+    DUGMA_CK(cudaMemcpy(b.desc, desc.data(), sizeof(PQDesc) * n_pq, cudaMemcpyHostToDevice));
+    DUGMA_CK(cudaMemcpy(b.items, sorted.data(), sizeof(BatchItem) * sorted.size(), cudaMemcpyHostToDevice));
+    DUGMA_CK(cudaMemcpy(b.pq_start, pq_start.data(), sizeof(int) * (n_pq + 1), cudaMemcpyHostToDevice));
+    DUGMA_CK(cudaMemcpy(b.pq_items, pq_items.data(), sizeof(int) * sorted.size(), cudaMemcpyHostToDevice));
+    b.host_doubles = (size_t)n_pq * 16 + 16;
+    if (cudaMallocHost((void**)&b.host, sizeof(double) * b.host_doubles) != cudaSuccess) {
+        cudaGetLastError();
+        b.host = nullptr;
+        return set_error(DUGMA_ERR_NOMEM, "batch: pinned staging allocation failed");
+    }
+    b.n_poses = n_poses;
+    return DUGMA_OK;
+}
+
+template <int D>
+static int batch_enqueue(Batch& b, cudaStream_t s)
+{
+    using Body = PackedBody<D, kBatchIPT, true>;
+    auto fn = batch_pairs_kernel<Body, kBatchNT, kBatchTJ, 4>;
+    const int n_pq = b.P * b.n_poses;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.ctx[0]->dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchNT, 0);
+    const int grid = std::min(std::max(per_sm, 1) * sms, b.n_items);
+    const int gx = std::min((b.max_span + 255) / 256, 64);
+    batch_prologue_kernel<D><<<dim3(gx, n_pq), 256, 0, s>>>(b.desc, b.max_span);
+    DUGMA_CK(cudaGetLastError());
+    DUGMA_CK(cudaMemsetAsync(b.counter, 0, 8 * sizeof(int), s));
+    fn<<<grid, kBatchNT, 0, s>>>(b.desc, b.items, b.n_items, b.partials, b.counter, b.err);
+    DUGMA_CK(cudaGetLastError());
+    batch_reduce_kernel<<<n_pq, 128, 0, s>>>(b.partials, b.pq_start, b.pq_items, b.nv, b.out);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
+}  // namespace dugma
+
+using namespace dugma;
+
 extern "C" {
-int dugma_batch_create(int, int, const int*, const int*, const double* const*, const double* const*,
-                       const double* const*, const double* const*, void**)
+
+int dugma_batch_create(int n_problems, int D, const int* N, const int* M, const double* const* X,
+                       const double* const* X_C, const double* const* Y, const double* const* Y_C, void** batch)
 {
-    return dugma::set_error(DUGMA_ERR_ARG, "batched problems are not available in this build");
+    if (n_problems < 1 || !N || !M || !X || !X_C || !Y || !Y_C || !batch)
+        return set_error(DUGMA_ERR_ARG, "batch_create: bad arguments");
+    if (D != 2 && D != 3) return set_error(DUGMA_ERR_ARG, "batch_create: D must be 2 or 3");
+    Batch* b = new Batch;
+    b->D = D;
+    b->P = n_problems;
+    b->ptrs.resize(6 * (size_t)n_problems);
+    for (int p = 0; p < n_problems; ++p) {
+        double ok = 0;
+        const int rc = dugma_init(X[p], X_C[p], Y[p], Y_C[p], &ok, N[p], M[p], D, &b->ptrs[6 * (size_t)p]);
+        if (rc != DUGMA_OK && rc != DUGMA_ERR_NONPD) {
+            for (int k = 0; k < p; ++k) dugma_fr_m(&b->ptrs[6 * (size_t)k]);
+            delete b;
+            return rc;
+        }
+        b->ctx.push_back(find_context(&b->ptrs[6 * (size_t)p]));
+    }
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        for (int k = 0; k < n_problems; ++k) dugma_fr_m(&b->ptrs[6 * (size_t)k]);
+        delete b;
+        return set_error(DUGMA_ERR_CUDA, "batch_create: stream creation failed");
+    }
+    *batch = b;
+    return DUGMA_OK;
 }
-int dugma_batch_energy_grad(void*, int, const double*, int, double*)
+
+int dugma_batch_energy_grad(void* batch, int n_poses, const double* poses, int model, double* out)
 {
-    return dugma::set_error(DUGMA_ERR_ARG, "batched problems are not available in this build");
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b || n_poses < 1 || !poses || !out) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: bad arguments");
+    if (model != DUGMA_MODEL_REF) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: the batched path is REF only");
+    DUGMA_RET(batch_prepare(*b, n_poses));
+    const int n_pq = b->P * n_poses, D = b->D;
+    for (int k = 0; k < n_pq; ++k) {
+        double* h = b->host + 16 * (size_t)k;
+        for (int q = 0; q < 16; ++q) h[q] = 0.0;
+        const double* src = poses + 13 * (size_t)k;
+        for (int q = 0; q < D * D; ++q) h[q] = src[q];
+        for (int a = 0; a < D; ++a) h[kPoseT + a] = src[9 + a];
+        h[kPoseSig] = src[12];
+        if (!(src[12] > 0)) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: sig of pose %d is not positive", k);
+    }
+    DUGMA_CK(cudaMemcpyAsync(b->poses, b->host, sizeof(double) * 16 * n_pq, cudaMemcpyHostToDevice, b->stream));
+    if (!b->exec) {
+        // first evaluation at this pose count: run eagerly, then capture the same work as a graph
+        DUGMA_RET(D == 3 ? batch_enqueue<3>(*b, b->stream) : batch_enqueue<2>(*b, b->stream));
+        DUGMA_CK(cudaStreamSynchronize(b->stream));
+        DUGMA_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = D == 3 ? batch_enqueue<3>(*b, b->stream) : batch_enqueue<2>(*b, b->stream);
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+        if (rc != DUGMA_OK || e != cudaSuccess) return rc != DUGMA_OK ? rc : set_error(DUGMA_ERR_CUDA, "batch capture failed");
+        DUGMA_CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    } else {
+        DUGMA_CK(cudaGraphLaunch(b->exec, b->stream));
+    }
+    const int nv = b->nv;
+    DUGMA_CK(cudaMemcpyAsync(out, b->out, sizeof(double) * nv * n_pq, cudaMemcpyDeviceToHost, b->stream));
+    int err = 0;
+    DUGMA_CK(cudaMemcpyAsync(b->host + 16 * (size_t)n_pq, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    DUGMA_CK(cudaStreamSynchronize(b->stream));
+    memcpy(&err, b->host + 16 * (size_t)n_pq, sizeof(int));
+    if (err) return set_error(DUGMA_ERR_TIMEOUT, "batch: a device wait gave up (0x%x)", err);
+    return DUGMA_OK;
 }
-int dugma_batch_destroy(void*) { return DUGMA_OK; }
+
+int dugma_batch_destroy(void* batch)
+{
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b) return set_error(DUGMA_ERR_ARG, "batch_destroy: null batch");
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    b->release_pose_state();
+    for (int p = 0; p < b->P; ++p) dugma_fr_m(&b->ptrs[6 * (size_t)p]);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return DUGMA_OK;
 }
+
+}  // extern "C"
