@@ -184,43 +184,48 @@ struct RefAdjointBody {
                 const float u1 = fmaf(v3.y, d2, fmaf(v2.y, d1, v2.w * d0));
                 const float u2 = fmaf(v2.z, d2, fmaf(v3.y, d1, v3.x * d0));
                 const float t1 = fmaf(d2, u2, fmaf(d1, u1, fmaf(d0, u0, v0.w)));
-                const float q00 = d0 * d0, q11 = d1 * d1, q22 = d2 * d2;
-                const float q01 = d0 * d1, q02 = d0 * d2, q12 = d1 * d2;
-                const float t2 =
-                    fmaf(B[5], q12, fmaf(B[4], q02, fmaf(B[3], q01, fmaf(B[2], q22, fmaf(B[1], q11, fmaf(B[0], q00, v0.w))))));
+                // B exponent in Horner form (off-diagonals doubled in the x record)
+                const float h0 = fmaf(B[4], d2, fmaf(B[3], d1, B[0] * d0));
+                const float h1 = fmaf(B[5], d2, B[1] * d1);
+                const float h2 = B[2] * d2;
+                const float t2 = fmaf(d0, h0, fmaf(d1, h1, fmaf(d2, h2, v0.w)));
                 const float e1 = ex2(t1), e2 = ex2(t2);
                 e[ii] += e1;
                 e[ii] += e2;
                 S1[ii][0] = fmaf(e1, u0, S1[ii][0]);
                 S1[ii][1] = fmaf(e1, u1, S1[ii][1]);
                 S1[ii][2] = fmaf(e1, u2, S1[ii][2]);
-                D2[ii][0] = fmaf(e2, d0, D2[ii][0]);
-                D2[ii][1] = fmaf(e2, d1, D2[ii][1]);
-                D2[ii][2] = fmaf(e2, d2, D2[ii][2]);
-                Q2[ii][0] = fmaf(e2, q00, Q2[ii][0]);
-                Q2[ii][1] = fmaf(e2, q11, Q2[ii][1]);
-                Q2[ii][2] = fmaf(e2, q22, Q2[ii][2]);
-                Q2[ii][3] = fmaf(e2, q01, Q2[ii][3]);
-                Q2[ii][4] = fmaf(e2, q02, Q2[ii][4]);
-                Q2[ii][5] = fmaf(e2, q12, Q2[ii][5]);
+                // moments of e2 through w = e2 d
+                const float w0 = e2 * d0, w1 = e2 * d1, w2 = e2 * d2;
+                D2[ii][0] += w0;
+                D2[ii][1] += w1;
+                D2[ii][2] += w2;
+                Q2[ii][0] = fmaf(w0, d0, Q2[ii][0]);
+                Q2[ii][1] = fmaf(w1, d1, Q2[ii][1]);
+                Q2[ii][2] = fmaf(w2, d2, Q2[ii][2]);
+                Q2[ii][3] = fmaf(w0, d1, Q2[ii][3]);
+                Q2[ii][4] = fmaf(w0, d2, Q2[ii][4]);
+                Q2[ii][5] = fmaf(w1, d2, Q2[ii][5]);
             } else {
                 const float d0 = (x[ii][0] - v0.x) - v1.x, d1 = (x[ii][1] - v0.y) - v1.y;
                 // C' packed (c00, c11, c01)
                 const float u0 = fmaf(v2.z, d1, v2.x * d0);
                 const float u1 = fmaf(v2.y, d1, v2.z * d0);
                 const float t1 = fmaf(d1, u1, fmaf(d0, u0, v0.w));
-                const float q00 = d0 * d0, q11 = d1 * d1, q01 = d0 * d1;
-                const float t2 = fmaf(B[2], q01, fmaf(B[1], q11, fmaf(B[0], q00, v0.w)));
+                const float h0 = fmaf(B[2], d1, B[0] * d0);
+                const float h1 = B[1] * d1;
+                const float t2 = fmaf(d0, h0, fmaf(d1, h1, v0.w));
                 const float e1 = ex2(t1), e2 = ex2(t2);
                 e[ii] += e1;
                 e[ii] += e2;
                 S1[ii][0] = fmaf(e1, u0, S1[ii][0]);
                 S1[ii][1] = fmaf(e1, u1, S1[ii][1]);
-                D2[ii][0] = fmaf(e2, d0, D2[ii][0]);
-                D2[ii][1] = fmaf(e2, d1, D2[ii][1]);
-                Q2[ii][0] = fmaf(e2, q00, Q2[ii][0]);
-                Q2[ii][1] = fmaf(e2, q11, Q2[ii][1]);
-                Q2[ii][2] = fmaf(e2, q01, Q2[ii][2]);
+                const float w0 = e2 * d0, w1 = e2 * d1;
+                D2[ii][0] += w0;
+                D2[ii][1] += w1;
+                Q2[ii][0] = fmaf(w0, d0, Q2[ii][0]);
+                Q2[ii][1] = fmaf(w1, d1, Q2[ii][1]);
+                Q2[ii][2] = fmaf(w0, d1, Q2[ii][2]);
             }
         }
     }
@@ -365,7 +370,7 @@ struct PackedBody {
             for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(X[ii][q], ny[q]), nl[q]);
             const float2* b = B[ii];
             float2 t1, t2;
-            float2 u[3], qq[6];
+            float2 u[3];
             if (!GRAD) {
                 // Horner forms (off-diagonals doubled in both matrices)
                 if (D == 3) {
@@ -391,28 +396,34 @@ struct PackedBody {
                     u[1] = ffma2(c[5], d[2], ffma2(c[1], d[1], fmul2(c[3], d[0])));
                     u[2] = ffma2(c[2], d[2], ffma2(c[5], d[1], fmul2(c[4], d[0])));
                     t1 = ffma2(d[2], u[2], ffma2(d[1], u[1], ffma2(d[0], u[0], lv)));
+                    // B exponent in Horner form (the x record's off-diagonals are doubled)
+                    const float2 h0 = ffma2(b[4], d[2], ffma2(b[3], d[1], fmul2(b[0], d[0])));
+                    const float2 h1 = ffma2(b[5], d[2], fmul2(b[1], d[1]));
+                    const float2 h2 = fmul2(b[2], d[2]);
+                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, ffma2(d[2], h2, lv)));
                 } else {
                     u[0] = ffma2(c[2], d[1], fmul2(c[0], d[0]));
                     u[1] = ffma2(c[1], d[1], fmul2(c[2], d[0]));
                     t1 = ffma2(d[1], u[1], ffma2(d[0], u[0], lv));
+                    const float2 h0 = ffma2(b[2], d[1], fmul2(b[0], d[0]));
+                    const float2 h1 = fmul2(b[1], d[1]);
+                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, lv));
                 }
-#pragma unroll
-                for (int k = 0; k < NS; ++k) qq[k] = fmul2(d[Sym<D>::a(k)], d[Sym<D>::b(k)]);
-                t2 = lv;
-#pragma unroll
-                for (int k = 0; k < NS; ++k) t2 = ffma2(b[k], qq[k], t2);
             }
             const float2 e1 = make_float2(ex2(t1.x), ex2(t1.y));
             const float2 e2 = make_float2(ex2(t2.x), ex2(t2.y));
             e[ii] = fadd2(fadd2(e[ii], e1), e2);
             if (GRAD) {
+                // moments of e2: w = e2 d, then sum w and w d^T (only d lives across the SFU latency)
+                float2 w[3];
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
                     S1[ii][q] = ffma2(e1, u[q], S1[ii][q]);
-                    D2[ii][q] = ffma2(e2, d[q], D2[ii][q]);
+                    w[q] = fmul2(e2, d[q]);
+                    D2[ii][q] = fadd2(D2[ii][q], w[q]);
                 }
 #pragma unroll
-                for (int k = 0; k < NS; ++k) Q2[ii][k] = ffma2(e2, qq[k], Q2[ii][k]);
+                for (int k = 0; k < NS; ++k) Q2[ii][k] = ffma2(w[Sym<D>::a(k)], d[Sym<D>::b(k)], Q2[ii][k]);
             }
         }
     }

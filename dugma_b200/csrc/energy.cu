@@ -30,6 +30,14 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
+// the same with a register budget that keeps MINB blocks resident per SM
+template <class Body, int NT, int TJ, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pair_kernel_occ(PairArgs a)
+{
+    Body body;
+    run_pairs<Body, NT, TJ, 4>(a, body);
+}
+
 // deterministic reduction of per-item partials: out[v] = sum_items partials[item][v];
 // block v sums value v in a fixed order (strided per thread, then a fixed tree)
 __global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __restrict__ part, int n_items, int nv,
@@ -81,6 +89,8 @@ static const std::vector<Variant>& adjoint_variants()
         {{1, 128, 32, 2, 512}, pair_kernel<PackedBody<D, 1, true>, 128, 32>},
         {{2, 128, 32, 2, 512}, pair_kernel<PackedBody<D, 2, true>, 128, 32>},
         {{1, 256, 32, 2, 512}, pair_kernel<PackedBody<D, 1, true>, 256, 32>},
+        {{2, 96, 32, 2, 512}, pair_kernel_occ<PackedBody<D, 2, true>, 96, 32, 5>},
+        {{2, 128, 64, 2, 512}, pair_kernel_occ<PackedBody<D, 2, true>, 128, 64, 4>},
     };
     return v;
 }
