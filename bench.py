@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--workload", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -80,14 +80,17 @@ def config_for(P):
 
 def profiled_traffic(shape_key):
     """DRAM bytes per launch of the adjoint kernel from the committed ncu summary, when this run
-    uses the profiled kernel shape on the profiled workload; otherwise None."""
+    uses the profiled kernel shape (its "shape:" line) on the profiled workload; otherwise None."""
     path = os.path.join(ROOT, "profiles", "adjoint_packed_harmonic64k.txt")
-    if shape_key != (2, 128, 32, 2) or not os.path.exists(path):
+    if not os.path.exists(path):
         return None
+    shape, traffic = None, None
     for line in open(path):
+        if line.strip().startswith("shape:"):
+            shape = tuple(int(v) for v in line.split(":")[1].split(","))
         if "traffic_bytes_per_launch:" in line:
-            return float(line.split(":")[1])
-    return None
+            traffic = float(line.split(":")[1])
+    return traffic if shape == tuple(shape_key) else None
 
 
 def eval_pose(P, rank):
@@ -196,6 +199,45 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args, rank):
+    """The reference's own CUDA plugins (init.cu / update_sig.cu / compi.cu compiled unmodified for
+    sm_100a into oracle/_ref) timed on this GPU beside this library's equivalents, on the 1K-sphere
+    generator at sizes that are multiples of 32 (the reference compi kernel needs them)."""
+    if rank != 0:
+        return
+    import torch
+    from oracle import ref_plugins
+    from dugma_b200 import api, synth
+    if not ref_plugins.available():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref was not built"}))
+        return
+    rows = []
+    for n in (1024, 4096):
+        P = synth.workload0(n=n)
+        R, t = P.R_G, P.t_G
+        ptr = ref_plugins.init(P.X, P.X_C, P.Y, P.Y_C)
+        _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+        res = {"N": n, "M": n}
+        for name, fn_ref, fn_ours in (
+                ("update_sig", lambda: ref_plugins.update_sig(ptr, R, t, n, n, 3), lambda: api.update_sig(h, R, t)),
+                ("compi", lambda: ref_plugins.compi(ptr, R, t, n, n, 3, 0.01), lambda: api.compi(h, R, t, sig=0.01))):
+            for tag, fn in (("reference", fn_ref), ("ours", fn_ours)):
+                fn()
+                torch.cuda.synchronize()
+                reps, el = 0, 0.0
+                t0 = time.perf_counter()
+                while reps < 3 or (time.perf_counter() - t0 < 2.0 and reps < 50):
+                    fn()
+                    reps += 1
+                el = time.perf_counter() - t0
+                res[f"{name}_{tag}_ms"] = 1e3 * el / reps
+                res[f"{name}_{tag}_pair_terms_per_s"] = n * n * reps / el
+        rows.append(res)
+        api.fr_m(h)
+    print(json.dumps({"impl": "reference-gpu", "unit": "pair-terms/s (one pair at one pose per term)",
+                      "note": "host-to-host calls of each plugin, wall clock", "results": rows}), flush=True)
+
+
 def run_batch(args, rank, world):
     """Workload 3: 256 problems (N, M uniform in [500, 8000]) x 32 multistart rotations on a uniform
     SO(3) grid, one persistent launch per evaluation (graph replay after the first); the problems
@@ -248,6 +290,9 @@ def main():
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.impl == "reference-gpu":
+        run_reference_gpu(args, rank)
         return
     if args.workload == 3:
         import torch
