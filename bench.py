@@ -19,7 +19,11 @@ roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instruc
 plain_fd    the plain form: energy + central finite differences (13 energy evaluations).
 cpu_baseline  the FP64 C/OpenMP oracle on a bounded sample of source rows, all host cores.
 
-Multi-GPU: each rank evaluates its own multistart pose of the same problem (independent
+With --poses P a step evaluates P multistart poses of the problem back to back (one
+launch sequence per pose); the depth-camera workload is quoted with P = 64.  The
+nearest-distance pass that sets sigma (update_sig) is timed separately (details).
+
+Multi-GPU: each rank evaluates its own multistart poses of the same problem (independent
 units, no collective on the data path): weak scaling, value = sum over ranks.
 """
 from __future__ import annotations
@@ -55,6 +59,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shape (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="override the cloud size (small profiling cases)")
     ap.add_argument("--shape", default="", help="pin the adjoint kernel shape ipt,nt,tj,pack (skips tuning)")
+    ap.add_argument("--poses", type=int, default=1,
+                    help="multistart poses evaluated per step and GPU (the depth workload uses 64)")
     return ap.parse_args()
 
 
@@ -72,10 +78,11 @@ def workload(wl, n=0):
     return synth.WORKLOADS[wl](n=n) if n else synth.WORKLOADS[wl]()
 
 
-def config_for(P):
+def config_for(P, poses=1):
     """The workload description, shared by both arms."""
-    return {"workload": f"{P.name}: N=M={P.N}, REF model energy + pose gradient per step, one multistart pose "
-                        "per GPU", "l2": "flushed between steps (256 MiB write)"}
+    per = "one multistart pose" if poses == 1 else f"{poses} multistart poses"
+    return {"workload": f"{P.name}: N={P.N}, M={P.M}, REF model energy + pose gradient, {per} per step and GPU",
+            "l2": "flushed between steps (256 MiB write)"}
 
 
 def profiled_traffic(shape_key):
@@ -93,10 +100,10 @@ def profiled_traffic(shape_key):
     return traffic if shape == tuple(shape_key) else None
 
 
-def eval_pose(P, rank):
-    """The pose of rank r: ground truth perturbed by a seeded multistart offset (rank 0: 10 deg, 2 cm)."""
+def eval_pose(P, unit):
+    """Multistart pose number `unit`: ground truth perturbed by a seeded 10 deg, 2 cm offset."""
     from dugma_b200.pose import expmap
-    rng = np.random.default_rng(100 + rank)
+    rng = np.random.default_rng(100 + unit)
     ax = rng.standard_normal(3)
     ax /= np.linalg.norm(ax)
     R = P.R_G @ expmap(ax * np.radians(10.0))
@@ -192,7 +199,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "energy+grad pair-terms/s", "value": val, "unit": "pair-terms/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_for(P),
+            "config": config_for(P, args.poses),
             "cpu_baseline": {"value": val, "unit": "pair-terms/s", "cores": orc.num_threads(), "kind": "port",
                              "sample": f"{rows} source rows x {st.M} targets per step"},
             "e2e": {"value": val, "unit": "pair-terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -318,7 +325,7 @@ def main():
     L = _lib.load(build_if_missing=False)
 
     P = workload(args.workload, args.n)
-    R, t = eval_pose(P, rank)
+    R, t = eval_pose(P, rank * max(1, args.poses))
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
     sig = api.update_sig(h, R, t)
     if args.shape:
@@ -341,17 +348,22 @@ def main():
     # a dedicated stream: handle 0 (the legacy default stream) means 'the context stream' in the C ABI
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    pose = torch.zeros(16, dtype=torch.float64, device="cuda")
-    pose[:9] = torch.tensor(np.asarray(R).T.reshape(-1))
-    pose[9:12] = torch.tensor(t)
-    pose[12] = sig
-    out = torch.zeros(8, dtype=torch.float64, device="cuda")
+    npose = max(1, args.poses)
+    pose = torch.zeros(npose, 16, dtype=torch.float64, device="cuda")
+    for k in range(npose):
+        Rk, tk = (R, t) if k == 0 else eval_pose(P, rank * npose + k)
+        pose[k, :9] = torch.tensor(np.asarray(Rk).T.reshape(-1))
+        pose[k, 9:12] = torch.tensor(tk)
+        pose[k, 12] = sig
+    out = torch.zeros(npose, 8, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
-        rc = L.dugma_energy_grad_async(h.arr, pose.data_ptr(), 0, out.data_ptr(), None, stream.cuda_stream)
-        if rc != 0:
-            raise RuntimeError(L.dugma_last_error().decode())
+        for k in range(npose):
+            rc = L.dugma_energy_grad_async(h.arr, pose[k].data_ptr(), 0, out[k].data_ptr(), None,
+                                           stream.cuda_stream)
+            if rc != 0:
+                raise RuntimeError(L.dugma_last_error().decode())
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -381,8 +393,16 @@ def main():
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-    value = world * pairs * args.steps / (ms * 1e-3)
-    res = out.cpu().numpy()
+    value = world * pairs * npose * args.steps / (ms * 1e-3)
+    res = out[0].cpu().numpy()
+
+    # the nearest-distance pass behind sigma (update_sig through the C ABI, host pose in, sigma out)
+    api.update_sig(h, R, t)
+    reps = 5
+    a0 = time.perf_counter()
+    for _ in range(reps):
+        api.update_sig(h, R, t)
+    upd_ms = 1e3 * (time.perf_counter() - a0) / reps
 
     # roofline of the adjoint kernel
     peak = ctypes.c_double(0)
@@ -406,7 +426,7 @@ def main():
         t1.record()
         torch.cuda.synchronize()
         fd_ms = t0.elapsed_time(t1) / reps
-        adj_ms = ms / args.steps
+        adj_ms = ms / (args.steps * npose)
         extra["plain_fd"] = {"ms_per_gradient": fd_ms, "evals_per_s": 1e3 / fd_ms,
                              "adjoint_evals_per_s": 1e3 / adj_ms, "adjoint_speedup": fd_ms / adj_ms,
                              "energy_evals_per_gradient": 13}
@@ -451,8 +471,10 @@ def main():
             "metric": "energy+grad pair-terms/s", "value": value, "unit": "pair-terms/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_for(P),
-            "details": {"sigma": sig, "kernel_shape": list(shape_key)},
+            "config": config_for(P, npose),
+            "details": {"sigma": sig, "kernel_shape": list(shape_key), "poses_per_step": npose,
+                        "update_sig_ms": upd_ms,
+                        "update_sig_pair_terms_per_s": pairs / (upd_ms * 1e-3)},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
                          "unit": "Tinstr/s (FP32 pipe, lane ops)", "frac": achieved / peak.value,
                          "traffic": profiled_traffic(shape_key) if (args.workload == 2 and not args.n) else None,
@@ -461,7 +483,7 @@ def main():
                                         "no FP32-pipe figure)",
                          "sfu_frac": sfu_frac, "kernel_ms": kernel_ms,
                          "instr_per_pair": FP32_INSTR_ADJOINT},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 3 * args.steps * npose,
             "result": {"E": float(res[0]), "g": [float(v) for v in res[1:7]]},
             "autotune": tune,
             "autotune_energy": tune_energy,

@@ -50,6 +50,7 @@ EXPORTS = {
     "dugma_version": (ctypes.c_char_p, []),
     "dugma_timing": (c_int, [PtrArray, c_int, dp, ip]),
     "dugma_shapes": (c_int, [c_int, ip, c_int]),
+    "dugma_knn_covariance": (c_int, [dp, c_int, c_int, c_int, c_double, c_double, dp]),
     "dugma_minimise_surrogate": (c_int, [c_int, dp, dp, dp, dp, ip]),
     "dugma_energy_grad_noalloc": (c_int, [c_void_p] * 6 + [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "dugma_set_shape": (c_int, [PtrArray, c_int, c_int, c_int, c_int, c_int]),

@@ -171,6 +171,15 @@ def autotune(h: Handles, what=0, model=_lib.MODEL_REF) -> str:
     return buf.value.decode()
 
 
+def knn_covariance(points, k=8, lo=1e-6, hi=1e-2):
+    """Per-point covariance from the k nearest other points (GPU), eigenvalues clamped to [lo, hi]."""
+    P = _d(points)
+    n, D = P.shape
+    out = np.zeros((n, D, D))
+    check(_lib.load().dugma_knn_covariance(_ptr(P), n, D, int(k), float(lo), float(hi), _ptr(out)))
+    return np.ascontiguousarray(np.transpose(out, (0, 2, 1)))
+
+
 def shapes(what=0):
     """Compiled kernel shapes for `what` (0 adjoint, 1 energy, 2 nearest neighbour): (ipt, nt, tj, pack)."""
     buf = (ctypes.c_int * 256)()

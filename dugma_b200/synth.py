@@ -257,13 +257,14 @@ def workload4(trial: int = 0, n: int = 300000) -> Problem:
     rng = rng_for(4, trial)
     boxes, spheres = [], []
     for _ in range(6):
-        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(1.0, 3.5)])
+        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(0.6, 3.0)])
         h = rng.uniform(0.1, 0.5, 3)
         boxes.append((c - h, c + h))
     for _ in range(4):
-        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(1.0, 3.5)])
+        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(0.6, 3.0)])
         spheres.append((c, rng.uniform(0.2, 0.6)))
-    boxes.append((np.array([-4.0, -3.0, 3.9]), np.array([4.0, 3.0, 4.0])))   # back wall
+    # a back wall wide and near enough that every pixel of both views hits something within 4 m
+    boxes.append((np.array([-10.0, -8.0, 3.5]), np.array([10.0, 8.0, 3.6])))
     Xc, XC = _range_view(rng, n, boxes, spheres, np.eye(3), np.zeros(3))
     Rv = random_rotation(rng, 15.0)
     tv = rng.uniform(-0.1, 0.1, 3)

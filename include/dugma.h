@@ -96,6 +96,11 @@ int dugma_energy_fd_grad(float* Ptr[6], const double* R, const double* t, double
  * fmaf(dz,dz, fmaf(dy,dy, dx*dx)) with y' = float(FP64(R y + t))). */
 int dugma_nn(float* Ptr[6], const double* R, const double* t, int k, int* idx, float* d2);
 
+/* Data preparation: per-point covariance from the k (1..15) nearest other points (brute-force
+ * self-join on the GPU): the sample covariance of the point and its neighbours (divided by k),
+ * eigenvalues clamped to [lo, hi].  points: n x D (MATLAB layout); cov: n blocks of D x D. */
+int dugma_knn_covariance(const double* points, int n, int D, int k, double lo, double hi, double* cov);
+
 /* sigma without quantisation (FP64 sum of the exact nearest squared distances / (D N)). */
 int dugma_sigma(float* Ptr[6], const double* R, const double* t, double* sig);
 

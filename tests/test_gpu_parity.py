@@ -333,3 +333,16 @@ def test_compi_coefficients(D):
         assert err <= 2e-6
     finally:
         api.fr_m(h)
+
+
+# ---------------------------------------------------------------- data preparation
+def test_knn_covariance_matches_cpu_estimator():
+    """GPU k-NN sample covariance (k = 8, eigenvalues clamped) against the seeded generators'
+    scipy-based estimator; neighbour sets can differ only on near-ties, so compare the bulk."""
+    rng = np.random.default_rng(9)
+    pts = synth.bumpy_sphere(rng, 3000)
+    ref = synth._knn_sample_cov(pts, 1e-6, 1e-2)
+    got = api.knn_covariance(pts, k=8, lo=1e-6, hi=1e-2)
+    err = np.abs(got - ref).reshape(len(pts), -1).max(axis=1) / np.abs(ref).reshape(len(pts), -1).max(axis=1)
+    assert np.mean(err < 1e-6) > 0.99, np.sort(err)[-10:]
+    assert np.all(np.linalg.eigvalsh(got) >= 1e-6 * (1 - 1e-9))
