@@ -42,6 +42,9 @@ sys.path.insert(0, ROOT)
 
 # algorithmic per-pair operation counts of the REF kernels, 3D (see the kernel sources)
 FP32_INSTR_ADJOINT = 44     # d 6, u = kC'd 9, exponent 3, d d^T 6, exponent 6, accumulations 14
+# CONV adjoint: d 6, S = Sx + C'y 6, adjugate 12, det 3, singularity test 3, h = adj d 9, d.h 3,
+# exponent and normalisation 5, energy 1, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
+FP32_INSTR_CONV_ADJOINT = 66
 FP32_INSTR_ENERGY = 26      # d 6, two Horner quadratic forms 9 + 9, accumulation 2
 SFU_PER_PAIR = 2            # two ex2
 
@@ -59,6 +62,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shape (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="override the cloud size (small profiling cases)")
     ap.add_argument("--shape", default="", help="pin the adjoint kernel shape ipt,nt,tj,pack (skips tuning)")
+    ap.add_argument("--model", type=int, default=0, choices=[0, 1],
+                    help="0: the reference's per-pair model (REF), 1: convolved GMM (CONV)")
     ap.add_argument("--poses", type=int, default=1,
                     help="multistart poses evaluated per step and GPU (the depth workload uses 64)")
     return ap.parse_args()
@@ -78,10 +83,11 @@ def workload(wl, n=0):
     return synth.WORKLOADS[wl](n=n) if n else synth.WORKLOADS[wl]()
 
 
-def config_for(P, poses=1):
+def config_for(P, poses=1, model=0):
     """The workload description, shared by both arms."""
     per = "one multistart pose" if poses == 1 else f"{poses} multistart poses"
-    return {"workload": f"{P.name}: N={P.N}, M={P.M}, REF model energy + pose gradient, {per} per step and GPU",
+    name = "REF" if model == 0 else "CONV"
+    return {"workload": f"{P.name}: N={P.N}, M={P.M}, {name} model energy + pose gradient, {per} per step and GPU",
             "l2": "flushed between steps (256 MiB write)"}
 
 
@@ -199,7 +205,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "energy+grad pair-terms/s", "value": val, "unit": "pair-terms/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_for(P, args.poses),
+            "config": config_for(P, args.poses, args.model),
             "cpu_baseline": {"value": val, "unit": "pair-terms/s", "cores": orc.num_threads(), "kind": "port",
                              "sample": f"{rows} source rows x {st.M} targets per step"},
             "e2e": {"value": val, "unit": "pair-terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -333,13 +339,13 @@ def main():
         api.set_shape(h, 0, shape_key)
         tune = f"pinned {args.shape}"
     else:
-        tune = "" if args.no_tune else api.autotune(h, 0)
+        tune = "" if (args.no_tune or args.model != 0) else api.autotune(h, 0)
         shape_key = api.shapes(0)[0]
         if tune:
             import re
             best = min(re.findall(r"\(ipt=(\d+),nt=(\d+),tj=(\d+),pack=(\d+)\):([0-9.]+)ms", tune), key=lambda m: float(m[4]))
             shape_key = tuple(int(v) for v in best[:4])
-    if not args.no_fd and not args.shape and not args.no_tune:
+    if not args.no_fd and not args.shape and not args.no_tune and args.model == 0:
         tune_energy = api.autotune(h, 1)     # the plain form's energy kernel gets the same treatment
     else:
         tune_energy = ""
@@ -360,7 +366,7 @@ def main():
 
     def step():
         for k in range(npose):
-            rc = L.dugma_energy_grad_async(h.arr, pose[k].data_ptr(), 0, out[k].data_ptr(), None,
+            rc = L.dugma_energy_grad_async(h.arr, pose[k].data_ptr(), args.model, out[k].data_ptr(), None,
                                            stream.cuda_stream)
             if rc != 0:
                 raise RuntimeError(L.dugma_last_error().decode())
@@ -410,7 +416,8 @@ def main():
     sfu = ctypes.c_double(0)
     L.dugma_calibrate(1, ctypes.byref(sfu), None)
     kernel_ms = kms.value / max(kl.value, 1)
-    achieved = FP32_INSTR_ADJOINT * pairs / (kernel_ms * 1e-3)
+    instr = FP32_INSTR_ADJOINT if args.model == 0 else FP32_INSTR_CONV_ADJOINT
+    achieved = instr * pairs / (kernel_ms * 1e-3)
     sfu_frac = SFU_PER_PAIR * pairs / (kernel_ms * 1e-3) / sfu.value if sfu.value else None
 
     extra = {}
@@ -418,11 +425,11 @@ def main():
         # plain form: energy + central FD over 6 pose coordinates (13 energy evaluations)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
-        api.energy_fd_grad(h, R, t, sig)
+        api.energy_fd_grad(h, R, t, sig, model=args.model)
         reps = max(2, args.steps // 4)
         t0.record()
         for _ in range(reps):
-            api.energy_fd_grad(h, R, t, sig)
+            api.energy_fd_grad(h, R, t, sig, model=args.model)
         t1.record()
         torch.cuda.synchronize()
         fd_ms = t0.elapsed_time(t1) / reps
@@ -430,6 +437,17 @@ def main():
         extra["plain_fd"] = {"ms_per_gradient": fd_ms, "evals_per_s": 1e3 / fd_ms,
                              "adjoint_evals_per_s": 1e3 / adj_ms, "adjoint_speedup": fd_ms / adj_ms,
                              "energy_evals_per_gradient": 13}
+        if args.model == 0:
+            # the same at the reference's per-pair precision (FP64 d, quadratic forms and exp)
+            api.energy_fd_grad(h, R, t, sig, model=2)
+            t0.record()
+            api.energy_fd_grad(h, R, t, sig, model=2)
+            t1.record()
+            torch.cuda.synchronize()
+            fd64_ms = t0.elapsed_time(t1)
+            extra["plain_fd"].update({"fp64_ms_per_gradient": fd64_ms,
+                                      "fp64_energy_pair_terms_per_s": 13 * pairs / (fd64_ms * 1e-3),
+                                      "adjoint_speedup_vs_fp64": fd64_ms / adj_ms})
 
     e2e = None
     if not args.no_e2e:
@@ -437,7 +455,7 @@ def main():
         h2d = 8 * (P.X.size + X_C.size + P.Y.size + Y_C.size)
         # warm-up of the end-to-end path
         _, h2 = api.init(P.X, X_C, P.Y, Y_C)
-        api.energy_grad(h2, R, t, sig)
+        api.energy_grad(h2, R, t, sig, model=args.model)
         api.fr_m(h2)
         ksteps = max(3, min(args.steps, 10))
         ph = [0.0, 0.0, 0.0]
@@ -446,7 +464,7 @@ def main():
             a = time.perf_counter()
             _, h2 = api.init(P.X, X_C, P.Y, Y_C)
             b = time.perf_counter()
-            api.energy_grad(h2, R, t, sig)
+            api.energy_grad(h2, R, t, sig, model=args.model)
             c = time.perf_counter()
             api.fr_m(h2)
             d = time.perf_counter()
@@ -471,18 +489,19 @@ def main():
             "metric": "energy+grad pair-terms/s", "value": value, "unit": "pair-terms/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_for(P, npose),
+            "config": config_for(P, npose, args.model),
             "details": {"sigma": sig, "kernel_shape": list(shape_key), "poses_per_step": npose,
                         "update_sig_ms": upd_ms,
                         "update_sig_pair_terms_per_s": pairs / (upd_ms * 1e-3)},
             "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
                          "unit": "Tinstr/s (FP32 pipe, lane ops)", "frac": achieved / peak.value,
-                         "traffic": profiled_traffic(shape_key) if (args.workload == 2 and not args.n) else None,
+                         "traffic": profiled_traffic(shape_key) if (args.workload == 2 and not args.n and args.model == 0)
+                         else None,
                          "algorithmic_bytes": 64 * (P.N + P.M),
                          "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json has "
                                         "no FP32-pipe figure)",
                          "sfu_frac": sfu_frac, "kernel_ms": kernel_ms,
-                         "instr_per_pair": FP32_INSTR_ADJOINT},
+                         "instr_per_pair": instr},
             "gpu_launches": 3 * args.steps * npose,
             "result": {"E": float(res[0]), "g": [float(v) for v in res[1:7]]},
             "autotune": tune,

@@ -21,7 +21,7 @@ PtrArray = c_void_p * 6
 
 # status codes (dugma.h)
 OK, ERR_ARG, ERR_CUDA, ERR_NONPD, ERR_TIMEOUT, ERR_NOMEM, ERR_NUMERIC, ERR_STATE = range(8)
-MODEL_REF, MODEL_CONV = 0, 1
+MODEL_REF, MODEL_CONV, MODEL_REF_F64 = 0, 1, 2
 DRIVE_REFERENCE, DRIVE_DIRECT = 0, 1
 
 EXPORTS = {

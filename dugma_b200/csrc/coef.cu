@@ -11,6 +11,9 @@
 // the P computation plus 10 multiply-adds in each pass instead of 637 atomics.
 #include <cmath>
 
+#include <mutex>
+#include <vector>
+
 #include "coef_map.h"
 #include "context.hpp"
 #include "pairs.cuh"
@@ -223,39 +226,62 @@ __global__ void __launch_bounds__(NT) coef_pass_kernel(PairArgs a)
 
 __constant__ signed char c_moment3[kNumMoments3D][4];
 __constant__ signed char c_moment2[kNumMoments2D][4];
+// per side, the indices of its moments in the table (kind 2: side 0, kind 1: side 1)
+__constant__ short c_side3[2][kNumMoments3D];
+__constant__ short c_side2[2][kNumMoments2D];
+__constant__ int c_side_n[2][2];   // [D == 3][side]
 
-// Moments from the per-point H: kind 2 over sources (side = 0), kind 1 over targets (side = 1).
-// Per-warp partial sums in shared memory, then per-block partials in fixed order.
+constexpr int kMomRows = 64;       // rows staged in shared memory per pass
+constexpr int kMomThreads = 256;   // >= moments of one side (168 in 3D)
+
+// Moments of one side from the per-point H: each pass stages kMomRows rows -- H summed over
+// the target chunks (one (row, feature) entry per thread, coalesced), the row's matrix and
+// monomials -- in shared memory; each thread then owns one moment of the side and sums its
+// products over the staged rows.  Per-block partials in fixed order (deterministic).
 template <int D>
-__global__ void moments_kernel(const double* __restrict__ hpart, int n_jc, int n, int side,
-                               const double* __restrict__ pose, const float* __restrict__ p,
-                               const float* __restrict__ cinv, double* __restrict__ block_out)
+__global__ void __launch_bounds__(kMomThreads) moments_kernel(const double* __restrict__ hpart, int n_jc, int n,
+                                                              int side, const double* __restrict__ pose,
+                                                              const float* __restrict__ p,
+                                                              const float* __restrict__ cinv,
+                                                              double* __restrict__ block_out)
 {
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     const signed char(*tab)[4] = D == 3 ? c_moment3 : c_moment2;
-    __shared__ double wsum[8][NM];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = threadIdx.x; k < 8 * NM; k += blockDim.x) (&wsum[0][0])[k] = 0.0;
-    __syncthreads();
+    const short* list = D == 3 ? c_side3[side] : c_side2[side];
+    const int nlist = c_side_n[D == 3][side];
+    __shared__ double sH[kMomRows][NF];
+    __shared__ double sM[kMomRows][NS];
+    __shared__ double sF[kMomRows][NF];
+    const int my = (int)threadIdx.x < nlist ? list[threadIdx.x] : -1;
+    int ia = 0, ib = 0, ic = 0;
+    if (my >= 0) {
+        ia = tab[my][1];
+        ib = tab[my][2];
+        ic = tab[my][3];
+    }
     double R[9], t[3];
     for (int k = 0; k < D * D; ++k) R[k] = pose[k];
     for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
     const double s = 1.0 / pose[kPoseSig];
-    const int kind = side == 0 ? 2 : 1;
     const int per_block = (n + gridDim.x - 1) / gridDim.x;
     const int b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
-    for (int base = b0; base < b1; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const bool ok = i < b1;
-        double H[NF], f[NF], mat[NS];
-        for (int q = 0; q < NF; ++q) H[q] = 0.0;
-        for (int q = 0; q < NS; ++q) mat[q] = 0.0;
-        for (int q = 0; q < NF; ++q) f[q] = 0.0;
-        if (ok) {
-            for (int c = 0; c < n_jc; ++c)
-                for (int q = 0; q < NF; ++q) H[q] += hpart[((size_t)c * n + i) * 16 + q];
-            double pt[3] = {0, 0, 0};
+    double acc = 0.0;
+    for (int base = b0; base < b1; base += kMomRows) {
+        const int nr = min(kMomRows, b1 - base);
+        for (int e = threadIdx.x; e < nr * 16; e += blockDim.x) {
+            const int r = e >> 4, q = e & 15;
+            if (q < NF) {
+                const double* h = hpart + (size_t)(base + r) * 16 + q;
+                double v = 0.0;
+#pragma unroll 8
+                for (int c = 0; c < n_jc; ++c) v += h[(size_t)c * n * 16];
+                sH[r][q] = v;
+            }
+        }
+        if ((int)threadIdx.x < nr) {
+            const int i = base + threadIdx.x;
+            double pt[3] = {0, 0, 0}, f[10];
             double A[3][3];
             for (int r0 = 0; r0 < D; ++r0)
                 for (int c0 = 0; c0 < D; ++c0)
@@ -263,7 +289,7 @@ __global__ void moments_kernel(const double* __restrict__ hpart, int n_jc, int n
                                            (double)cinv[(size_t)i * D * D + c0 + D * r0]);
             if (side == 0) {
                 for (int a = 0; a < D; ++a) pt[a] = (double)p[(size_t)i * D + a];
-                for (int k = 0; k < NS; ++k) mat[k] = A[Sym<D>::a(k)][Sym<D>::b(k)];
+                for (int k = 0; k < NS; ++k) sM[threadIdx.x][k] = A[Sym<D>::a(k)][Sym<D>::b(k)];
             } else {
                 for (int a = 0; a < D; ++a) {
                     double v = R[a] * (double)p[(size_t)i * D] + R[a + D] * (double)p[(size_t)i * D + 1];
@@ -273,42 +299,43 @@ __global__ void moments_kernel(const double* __restrict__ hpart, int n_jc, int n
                 double T[3][3];
                 for (int r0 = 0; r0 < D; ++r0)
                     for (int c0 = 0; c0 < D; ++c0) {
-                        double acc = 0;
-                        for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
-                        T[r0][c0] = acc;
+                        double a2 = 0;
+                        for (int k = 0; k < D; ++k) a2 += A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = a2;
                     }
                 for (int k = 0; k < NS; ++k) {
-                    double acc = 0;
-                    for (int q = 0; q < D; ++q) acc += R[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
-                    mat[k] = acc;
+                    double a2 = 0;
+                    for (int q = 0; q < D; ++q) a2 += R[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
+                    sM[threadIdx.x][k] = a2;
                 }
             }
             monomials<D>(pt, f);
+            for (int q = 0; q < NF; ++q) sF[threadIdx.x][q] = f[q];
         }
-        for (int mi = 0; mi < NM; ++mi) {
-            if (tab[mi][0] != kind) continue;
-            double v = mat[tab[mi][1]] * f[tab[mi][2]] * H[tab[mi][3]];
-            v = warp_sum(v);
-            if (lane == 0) wsum[warp][mi] += v;
-        }
+        __syncthreads();
+        if (my >= 0)
+            for (int r = 0; r < nr; ++r) acc += sM[r][ia] * sF[r][ib] * sH[r][ic];
+        __syncthreads();
     }
-    __syncthreads();
-    for (int mi = threadIdx.x; mi < NM; mi += blockDim.x) {
-        double v = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += wsum[w][mi];
-        block_out[(size_t)blockIdx.x * NM + mi] = v;
-    }
+    const int kind = side == 0 ? 2 : 1;
+    for (int mi = threadIdx.x; mi < NM; mi += blockDim.x)
+        if (tab[mi][0] != kind) block_out[(size_t)blockIdx.x * NM + mi] = 0.0;
+    if (my >= 0) block_out[(size_t)blockIdx.x * NM + my] = acc;
 }
 
+// out[mi] = sum over the na + nb block partials of moment mi; one warp per moment, lanes
+// strided over the blocks, fixed-order warp sum.
 __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, const double* __restrict__ b, int nb,
                                       int nm, double* __restrict__ out)
 {
-    for (int mi = threadIdx.x; mi < nm; mi += blockDim.x) {
-        double v = 0;
-        for (int k = 0; k < na; ++k) v += a[(size_t)k * nm + mi];
-        for (int k = 0; k < nb; ++k) v += b[(size_t)k * nm + mi];
-        out[mi] = v;
-    }
+    const int lane = threadIdx.x & 31;
+    const int mi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (mi >= nm) return;
+    double v = 0.0;
+    for (int k = lane; k < na; k += 32) v += a[(size_t)k * nm + mi];
+    for (int k = lane; k < nb; k += 32) v += b[(size_t)k * nm + mi];
+    v = warp_sum(v);
+    if (lane == 0) out[mi] = v;
 }
 
 using KernelFn = void (*)(PairArgs);
@@ -324,18 +351,43 @@ int Context::ensure_coef_records()
     if (yrec128) return DUGMA_OK;
     DUGMA_CK(cudaMalloc(&yrec128, sizeof(Rec128) * (size_t)M_pad));
     DUGMA_CK(cudaMalloc(&xrec128, sizeof(Rec128) * (size_t)N_pad));
+    // per-block moment partials of both sides: 2 x (2 blocks per SM) x the 3D moment count
+    DUGMA_CK(cudaMalloc(&mom_part, sizeof(double) * 2 * (size_t)(2 * num_sms) * kNumMoments3D));
+    return DUGMA_OK;
+}
+
+// The moment tables and per-side moment lists in constant memory, once per device.
+static int upload_moment_tables(int dev)
+{
+    static std::mutex mu;
+    static std::vector<char> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < (int)done.size() && done[dev]) return DUGMA_OK;
+    short side3[2][kNumMoments3D] = {}, side2[2][kNumMoments2D] = {};
+    int cnt[2][2] = {{0, 0}, {0, 0}};
+    for (int mi = 0; mi < kNumMoments3D; ++mi)
+        for (int sd = 0; sd < 2; ++sd)
+            if (kMoment3D[mi][0] == (sd == 0 ? 2 : 1)) side3[sd][cnt[1][sd]++] = (short)mi;
+    for (int mi = 0; mi < kNumMoments2D; ++mi)
+        for (int sd = 0; sd < 2; ++sd)
+            if (kMoment2D[mi][0] == (sd == 0 ? 2 : 1)) side2[sd][cnt[0][sd]++] = (short)mi;
+    for (int d = 0; d < 2; ++d)
+        for (int sd = 0; sd < 2; ++sd)
+            if (cnt[d][sd] > kMomThreads) return set_error(DUGMA_ERR_STATE, "moment table larger than a block");
+    DUGMA_CK(cudaMemcpyToSymbol(c_moment3, kMoment3D, sizeof(kMoment3D)));
+    DUGMA_CK(cudaMemcpyToSymbol(c_moment2, kMoment2D, sizeof(kMoment2D)));
+    DUGMA_CK(cudaMemcpyToSymbol(c_side3, side3, sizeof(side3)));
+    DUGMA_CK(cudaMemcpyToSymbol(c_side2, side2, sizeof(side2)));
+    DUGMA_CK(cudaMemcpyToSymbol(c_side_n, cnt, sizeof(cnt)));
+    if (dev >= (int)done.size()) done.resize(dev + 1, 0);
+    done[dev] = 1;
     return DUGMA_OK;
 }
 
 template <int D>
 static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
 {
-    static bool tables = false;
-    if (!tables) {
-        DUGMA_CK(cudaMemcpyToSymbol(c_moment3, kMoment3D, sizeof(kMoment3D)));
-        DUGMA_CK(cudaMemcpyToSymbol(c_moment2, kMoment2D, sizeof(kMoment2D)));
-        tables = true;
-    }
+    DUGMA_RET(upload_moment_tables(c.dev));
     DUGMA_RET(c.ensure_coef_records());
     const int n = std::max(c.M_pad, c.N_pad);
     coef_prologue_kernel<D><<<std::min((n + 255) / 256, c.num_sms * 4), 256, 0, s>>>(
@@ -344,11 +396,11 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     const KernelShape sh{2, 128, 32};
     KernelFn fn = coef_pass_kernel<CoefBody<D, 2>, 128, 32>;
-    const int nblk = std::min(c.num_sms, 64);
-    // the moment partials live in a dedicated device buffer (scratch is reused by each pass)
-    double* mom = nullptr;
-    DUGMA_CK(cudaMallocAsync(&mom, sizeof(double) * (size_t)2 * nblk * NM, s));
+    // blocks of the moments kernel: about 32 rows each, at most 2 per SM (the partial buffer's size)
+    const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
+    double* mom = c.mom_part;
     int rc = DUGMA_OK;
+    int nb_side[2] = {0, 0};
     for (int side = 0; side < 2 && rc == DUGMA_OK; ++side) {
         // side 0: sources stationary over streamed targets; side 1: the reverse
         double* hp = nullptr;
@@ -367,17 +419,20 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
                                  &n_jc, s);
         c.wx = wsave;
         if (rc != DUGMA_OK) break;
+        const int nb = std::min(nblk, rows);
+        nb_side[side] = nb;
         if (side == 0)
-            moments_kernel<D><<<nblk, 256, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x, c.xinv, mom);
+            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x, c.xinv, mom);
         else
-            moments_kernel<D><<<nblk, 256, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y, c.yinv, mom + (size_t)nblk * NM);
+            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y, c.yinv,
+                                                         mom + (size_t)nblk * NM);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moments kernel launch failed");
     }
     if (rc == DUGMA_OK) {
-        moments_reduce_kernel<<<1, 256, 0, s>>>(mom, nblk, mom + (size_t)nblk * NM, nblk, NM, moments_dev);
+        moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(mom, nb_side[0], mom + (size_t)nblk * NM, nb_side[1], NM,
+                                                           moments_dev);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moment reduction launch failed");
     }
-    cudaFreeAsync(mom, s);
     return rc;
 }
 

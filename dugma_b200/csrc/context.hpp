@@ -63,6 +63,7 @@ struct Context {
     int* counter = nullptr;                   // work-queue counters (8)
     double* dedx = nullptr;                   // dE/dx rows (allocated on first request)
     double* mom = nullptr;                    // surrogate moments (512 doubles)
+    double* mom_part = nullptr;               // per-block moment partials (with the 128-byte records)
     // scratch: a region of the arena, replaced by a separate allocation if a launch needs more
     void* arena = nullptr;                    // one allocation for every buffer above
     size_t arena_bytes = 0;
@@ -117,6 +118,8 @@ int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_
 // writes {E, g} to out_dev and, if dEdx_dev, dE/dx for rows [i0, i1) (relative index).
 int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1,
                  double* out_dev, double* dEdx_dev, cudaStream_t s, const KernelShape* force = nullptr);
+// REF energy at the reference's FP64 per-pair precision (ref64.cu), sums to out_dev[0].
+int ref64_launch(Context& c, const double* pose_dev, int i0, int i1, double* out_dev, cudaStream_t s);
 // Nearest neighbours: writes idx/d2 (device) and optionally the per-point minimum only.
 int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
               const KernelShape* force = nullptr);

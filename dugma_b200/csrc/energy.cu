@@ -221,6 +221,12 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
 {
     if (i0 < 0 || i1 > c.N || i0 >= i1) return set_error(DUGMA_ERR_ARG, "bad source row range [%d, %d)", i0, i1);
     if (model == DUGMA_MODEL_CONV) return conv_launch(c, pose_dev, grad, i0, i1, out_dev, dEdx_dev, s, force);
+    if (model == DUGMA_MODEL_REF_F64) {
+        if (grad)
+            return set_error(DUGMA_ERR_ARG, "the FP64 reference-precision model has no adjoint (use the "
+                                            "finite-difference gradient)");
+        return ref64_launch(c, pose_dev, i0, i1, out_dev, s);
+    }
     if (model != DUGMA_MODEL_REF) return set_error(DUGMA_ERR_ARG, "unknown model %d", model);
     const KernelShape want = force ? *force : (grad ? c.shape_adj : c.shape_energy);
     const std::vector<Variant>& vars =

@@ -209,11 +209,9 @@ def workload3(trial: int = 0, n_problems: int = 256, n_poses: int = 32,
     return probs
 
 
-def _range_view(rng, n_keep, boxes, spheres, view_R, view_t):
-    """Ray-cast a box-and-sphere scene from a pinhole camera (640x480, f=525)."""
-    H, W = 480, 640
-    fx = fy = 525.0
-    cx, cy = 319.5, 239.5
+def _range_view(rng, n_keep, boxes, spheres, view_R, view_t, camera=(640, 480, 525.0, 525.0, 319.5, 239.5)):
+    """Ray-cast a box-and-sphere scene from a pinhole camera (W, H, fx, fy, cx, cy)."""
+    W, H, fx, fy, cx, cy = camera
     u, v = np.meshgrid(np.arange(W), np.arange(H))
     dirs = np.stack([(u - cx) / fx, (v - cy) / fy, np.ones_like(u, dtype=np.float64)], axis=-1).reshape(-1, 3)
     z = np.full(dirs.shape[0], np.inf)
@@ -271,6 +269,41 @@ def workload4(trial: int = 0, n: int = 300000) -> Problem:
     Yc, YC = _range_view(rng, n, boxes, spheres, Rv, tv)
     # camera-frame points of view 2 map to the world (= view 1 frame) by y_w = Rv y + tv
     return Problem(Xc, Yc, XC, YC, Rv, tv, "depth300k")
+
+
+def _random_scene(rng, n_boxes=6, n_spheres=4, z=(0.6, 3.0), wall=None):
+    """Axis-aligned boxes and spheres in front of the camera, optionally a back wall at depth `wall`."""
+    boxes, spheres = [], []
+    for _ in range(n_boxes):
+        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(*z)])
+        h = rng.uniform(0.1, 0.5, 3)
+        boxes.append((c - h, c + h))
+    for _ in range(n_spheres):
+        c = np.array([rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0), rng.uniform(*z)])
+        spheres.append((c, rng.uniform(0.2, 0.6)))
+    if wall is not None:
+        boxes.append((np.array([-10.0, -8.0, wall]), np.array([10.0, 8.0, wall + 0.1])))
+    return boxes, spheres
+
+
+KINECT_V2 = (512, 424, 365.0, 365.0, 255.5, 211.5)
+
+
+def kinect_like(trial: int = 0) -> Problem:
+    """Stand-in for one two-camera depth scene: 12 boxes and 8 spheres (no background, so no
+    plane dominates) seen by two 512x424 depth cameras (f = 365 px) whose relative pose is a
+    rotation of up to 20 deg and a translation in [-0.2, 0.2]^3 m, subsampled to
+    N ~ U[3598, 5334] and M ~ U[463, 5159] points (the size ranges of two-sensor scenes),
+    depth-dependent sensor covariances."""
+    rng = rng_for(5, trial)
+    boxes, spheres = _random_scene(rng, n_boxes=12, n_spheres=8, z=(1.0, 3.5))
+    n = int(rng.integers(3598, 5335))
+    m = int(rng.integers(463, 5160))
+    X, XC = _range_view(rng, n, boxes, spheres, np.eye(3), np.zeros(3), KINECT_V2)
+    Rv = random_rotation(rng, 20.0)
+    tv = rng.uniform(-0.2, 0.2, 3)
+    Y, YC = _range_view(rng, m, boxes, spheres, Rv, tv, KINECT_V2)
+    return Problem(X, Y, XC, YC, Rv, tv, f"twoview{trial}")
 
 
 WORKLOADS = {0: workload0, 1: workload1, 2: workload2, 4: workload4}

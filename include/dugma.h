@@ -39,7 +39,10 @@ enum {
 /* Per-pair models. */
 enum {
     DUGMA_MODEL_REF = 0, /* the reference: w_i v_j [exp(-d'C'd/2) + exp(-d'Bd/2)] (compi.cu:753-772) */
-    DUGMA_MODEL_CONV = 1 /* convolved GMM: N(d; 0, sig (R Sy R' + Sx)) with its own 3x3 inverse */
+    DUGMA_MODEL_CONV = 1, /* convolved GMM: N(d; 0, sig (R Sy R' + Sx)) with its own 3x3 inverse */
+    DUGMA_MODEL_REF_F64 = 2 /* REF at the reference's per-pair precision (FP64 d, quadratic forms and exp,
+                               compi.cu:732-772); energy only: its gradient is the finite-difference
+                               plain form (dugma_energy_fd_grad) */
 };
 
 /* Largest supported cloud size (the reference stops at 3e6 points, compi.cu:535). */

@@ -269,6 +269,51 @@ def test_fd_grad_plain_form(w0):
     assert _rel(g, go) <= 1e-4
 
 
+@pytest.mark.parametrize("D", [3, 2])
+@pytest.mark.parametrize("n,m", [(1, 1), (700, 1111), (1025, 130)])
+def test_ref_precision_model_matches_oracle(D, n, m):
+    """The FP64 per-pair (reference precision) energy: FP64 sums in another order only, so
+    relative 1e-11; its gradient is the central-difference plain form, compared with the
+    oracle's central differences over the same perturbations (left rotation exp(h e_q) R,
+    then t + h e_q; relative 1e-7); asking it for an adjoint is an argument error."""
+    X, XC, Y, YC = _problem_small(D, n, m, seed=5 + n, bad=(2,) if n > 2 and m > 2 else ())
+    st = orc.State(X, XC, Y, YC)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D, seed=9)
+        for sig in (0.05, 0.4):
+            Eo, go, _ = st.energy(R, t, sig)
+            E = api.energy(h, R, t, sig, model=2)
+            assert abs(E - Eo) <= 1e-11 * abs(Eo) + 1e-300, (E, Eo)
+        hstep = 1e-4
+        Ef, gf = api.energy_fd_grad(h, R, t, 0.4, step=hstep, model=2)
+        Eo, go, _ = st.energy(R, t, 0.4)
+        assert abs(Ef - Eo) <= 1e-11 * abs(Eo) + 1e-300
+        nr = 3 if D == 3 else 1
+        gfd = []
+        for q in range(nr + D):
+            ev = []
+            for sgn in (1.0, -1.0):
+                R2, t2 = R.copy(), np.array(t, dtype=float)
+                if q < nr:
+                    w = np.zeros(3)
+                    w[q] = sgn * hstep
+                    R2 = (expmap(w) if D == 3 else rot2d(sgn * hstep)) @ R
+                else:
+                    t2[q - nr] += sgn * hstep
+                ev.append(st.energy(R2, t2, 0.4)[0])
+            gfd.append((ev[0] - ev[1]) / (2 * hstep))
+        assert _rel(gf, gfd) <= 1e-7, (gf, gfd)
+        assert _rel(gf, go) <= 1e-3   # central-difference truncation against the analytic gradient
+        with pytest.raises(api.DugmaError):
+            api.energy_grad(h, R, t, 0.4, model=2)
+    finally:
+        api.fr_m(h)
+
+
 def test_range_partials_sum_to_total(w0):
     P, st, h = w0
     R, t = _pose(3, 2)
