@@ -336,17 +336,19 @@ def main():
     sig = api.update_sig(h, R, t)
     if args.shape:
         shape_key = tuple(int(v) for v in args.shape.split(","))
-        api.set_shape(h, 0, shape_key)
+        api.set_shape(h, 0 if args.model == 0 else 3, shape_key)
         tune = f"pinned {args.shape}"
     else:
-        tune = "" if (args.no_tune or args.model != 0) else api.autotune(h, 0)
-        shape_key = api.shapes(0)[0]
+        kind = 0 if args.model == 0 else 3     # REF or CONV adjoint shapes
+        tune = "" if args.no_tune else api.autotune(h, kind)
+        shape_key = api.shapes(kind)[0]
         if tune:
             import re
             best = min(re.findall(r"\(ipt=(\d+),nt=(\d+),tj=(\d+),pack=(\d+)\):([0-9.]+)ms", tune), key=lambda m: float(m[4]))
             shape_key = tuple(int(v) for v in best[:4])
-    if not args.no_fd and not args.shape and not args.no_tune and args.model == 0:
-        tune_energy = api.autotune(h, 1)     # the plain form's energy kernel gets the same treatment
+    if not args.no_fd and not args.shape and not args.no_tune:
+        # the plain form's energy kernel gets the same treatment
+        tune_energy = api.autotune(h, 1 if args.model == 0 else 4)
     else:
         tune_energy = ""
     pairs = P.N * P.M

@@ -181,7 +181,8 @@ def knn_covariance(points, k=8, lo=1e-6, hi=1e-2):
 
 
 def shapes(what=0):
-    """Compiled kernel shapes for `what` (0 adjoint, 1 energy, 2 nearest neighbour): (ipt, nt, tj, pack)."""
+    """Compiled kernel shapes for `what` (0 adjoint, 1 energy, 2 nearest neighbour, 3 CONV adjoint,
+    4 CONV energy): (ipt, nt, tj, pack)."""
     buf = (ctypes.c_int * 256)()
     n = _lib.load().dugma_shapes(int(what), buf, 64)
     if n < 0:

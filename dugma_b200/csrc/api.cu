@@ -311,6 +311,8 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     c->shape_adj = {2, 128, 64, 2, 512};
     c->shape_energy = {4, 128, 32, 2};
     c->shape_nn = {4, 128, 128};
+    c->shape_conv_adj = {1, 64, 32, 2, 512};
+    c->shape_conv_energy = {1, 128, 32, 2};
     int rc = DUGMA_OK;
     auto fail = [&](int code) {
         destroy_context(c);
@@ -560,11 +562,35 @@ int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double*
 // ---------------------------------------------------------------------------
 // autotuner: time each candidate shape with CUDA events on the context stream
 // ---------------------------------------------------------------------------
+// kernel families that have tunable shapes: 0 adjoint, 1 energy, 2 nearest neighbour,
+// 3 CONV adjoint, 4 CONV energy
+static std::vector<KernelShape> shapes_of(int what)
+{
+    switch (what) {
+    case 0: return adjoint_shapes();
+    case 1: return energy_shapes();
+    case 2: return nn_shapes();
+    case 3: return conv_shapes(true);
+    default: return conv_shapes(false);
+    }
+}
+
+static KernelShape& shape_slot(Context& c, int what)
+{
+    switch (what) {
+    case 0: return c.shape_adj;
+    case 1: return c.shape_energy;
+    case 2: return c.shape_nn;
+    case 3: return c.shape_conv_adj;
+    default: return c.shape_conv_energy;
+    }
+}
+
 int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t report_len)
 {
     GET_CTX(c, Ptr);
-    if (what < 0 || what > 2) return set_error(DUGMA_ERR_ARG, "autotune: what must be 0, 1 or 2");
-    std::vector<KernelShape> cand = what == 0 ? adjoint_shapes() : (what == 1 ? energy_shapes() : nn_shapes());
+    if (what < 0 || what > 4) return set_error(DUGMA_ERR_ARG, "autotune: what must be 0 .. 4");
+    std::vector<KernelShape> cand = shapes_of(what);
     // use the pose of the last call if there was one, else the identity at sig = 0.01
     DUGMA_CK(cudaMemcpyAsync(c->host, c->pose, sizeof(double) * kPoseDoubles, cudaMemcpyDeviceToHost, c->stream));
     DUGMA_CK(cudaStreamSynchronize(c->stream));
@@ -588,6 +614,8 @@ int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t repo
     for (auto& sh : cand) {
         auto run = [&]() {
             if (what == 2) return launch_nn(*c, c->pose, 1, di, dd, c->stream, &sh);
+            if (what >= 3) return launch_pairs(*c, c->pose, DUGMA_MODEL_CONV, what == 3, 0, c->N, c->out, nullptr,
+                                               c->stream, &sh);
             return launch_pairs(*c, c->pose, model, what == 0, 0, c->N, c->out, nullptr, c->stream, &sh);
         };
         rc = run();   // warm-up (also sizes scratch)
@@ -615,17 +643,15 @@ int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t repo
     if (di) cudaFree(di);
     if (dd) cudaFree(dd);
     if (rc != DUGMA_OK) return rc;
-    if (what == 0) c->shape_adj = best_shape;
-    else if (what == 1) c->shape_energy = best_shape;
-    else c->shape_nn = best_shape;
+    shape_slot(*c, what) = best_shape;
     if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
     return DUGMA_OK;
 }
 
 int dugma_shapes(int what, int* shapes, int max)
 {
-    if (what < 0 || what > 2) return -set_error(DUGMA_ERR_ARG, "shapes: what must be 0, 1 or 2");
-    std::vector<KernelShape> cand = what == 0 ? adjoint_shapes() : (what == 1 ? energy_shapes() : nn_shapes());
+    if (what < 0 || what > 4) return -set_error(DUGMA_ERR_ARG, "shapes: what must be 0 .. 4");
+    std::vector<KernelShape> cand = shapes_of(what);
     const int n = (int)cand.size();
     for (int k = 0; k < n && k < max && shapes; ++k) {
         shapes[4 * k] = cand[k].ipt;
@@ -639,8 +665,8 @@ int dugma_shapes(int what, int* shapes, int max)
 int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack)
 {
     GET_CTX(c, Ptr);
-    if (what < 0 || what > 2) return set_error(DUGMA_ERR_ARG, "set_shape: what must be 0, 1 or 2");
-    std::vector<KernelShape> cand = what == 0 ? adjoint_shapes() : (what == 1 ? energy_shapes() : nn_shapes());
+    if (what < 0 || what > 4) return set_error(DUGMA_ERR_ARG, "set_shape: what must be 0 .. 4");
+    std::vector<KernelShape> cand = shapes_of(what);
     KernelShape want;
     want.ipt = ipt;
     want.nt = nt;
@@ -648,7 +674,7 @@ int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack)
     want.pack = pack;
     for (const KernelShape& s : cand)
         if (s.same(want)) {
-            (what == 0 ? c->shape_adj : what == 1 ? c->shape_energy : c->shape_nn) = s;
+            shape_slot(*c, what) = s;
             return DUGMA_OK;
         }
     return set_error(DUGMA_ERR_ARG, "set_shape: (%d, %d, %d, %d) is not a compiled shape", ipt, nt, tj, pack);

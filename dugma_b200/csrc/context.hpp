@@ -77,7 +77,7 @@ struct Context {
     double* host = nullptr;                   // kHostDoubles doubles
     cudaStream_t stream = nullptr;
     int num_sms = 148;
-    KernelShape shape_adj, shape_energy, shape_nn;
+    KernelShape shape_adj, shape_energy, shape_nn, shape_conv_adj, shape_conv_energy;
     std::mutex mu;                            // one host call at a time per context
     // optional timing of the main pairwise kernel (dugma_timing)
     bool timing = false;
@@ -137,5 +137,6 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
 std::vector<KernelShape> adjoint_shapes();
 std::vector<KernelShape> energy_shapes();
 std::vector<KernelShape> nn_shapes();
+std::vector<KernelShape> conv_shapes(bool grad);
 
 }  // namespace dugma

@@ -93,7 +93,7 @@ __global__ void conv_prologue_kernel(const double* __restrict__ pose, const floa
 // source covariance, and the difference d is formed from x and the y' split exactly.
 // Returns false (no contribution) when the combined covariance is not positive definite.
 template <int D>
-__device__ __noinline__ bool conv_pair_f64(const float* xi, const float* sxi, float4 v0, float4 v1,
+__device__ __forceinline__ bool conv_pair_f64(const float* xi, const float* sxi, float4 v0, float4 v1,
                                            const float* __restrict__ cy, const double* __restrict__ pose, double kl,
                                            float* adj, float* h, float* rd, float* Nt)
 {
@@ -149,6 +149,60 @@ __device__ __noinline__ bool conv_pair_f64(const float* xi, const float* sxi, fl
     for (int q = 0; q < D; ++q) h[q] = (float)hh[q];
     for (int k = 0; k < NS; ++k) adj[k] = (float)ad[k];
     return true;
+}
+
+// Per-source contraction of the CONV moments into the energy and the pose gradient (and
+// dE/dx when requested): E~ = sum N~, U = sum N~ u~, UU = sum N~ u~ u~^T, A = sum N~ St^-1
+// over the item's targets, with the source's own x and St_x.
+template <int D, int NV, bool GRAD>
+__device__ void conv_contract(const PairArgs& a, int jc, int row, const float* xv, const float* sxv, double E,
+                              const double* Ur, const double* UUr, const double* Ar, double lam, double c0,
+                              const double* t, double (&acc)[NV])
+{
+    constexpr int NS = Sym<D>::N, NR = Sym<D>::NR;
+    acc[0] += c0 * E;
+    if (!GRAD) return;
+    double S[3][3] = {}, UUm[3][3] = {}, Am[3][3] = {};
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        const int ra = Sym<D>::a(q), rb = Sym<D>::b(q);
+        S[ra][rb] = S[rb][ra] = (double)sxv[q];
+        UUm[ra][rb] = UUm[rb][ra] = UUr[q];
+        Am[ra][rb] = Am[rb][ra] = Ar[q];
+    }
+    double u[3], p[3];
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+        u[q] = Ur[q] / lam;        // sum N~ S^-1 d
+        p[q] = (double)xv[q] - t[q];
+    }
+    // B1 = S_x UU (for (S_x u) x u),  B2 = S_x A (for axial(S_x S^-1))
+    double B1[3][3] = {}, B2[3][3] = {};
+    for (int r0 = 0; r0 < D; ++r0)
+        for (int c1 = 0; c1 < D; ++c1)
+            for (int k = 0; k < D; ++k) {
+                B1[r0][c1] += S[r0][k] * UUm[k][c1];
+                B2[r0][c1] += S[r0][k] * Am[k][c1];
+            }
+    // (S_x u~) x u~ summed: component k = eps_kab (S_x UU)_ab ; / lam for the S scale
+    if (D == 3) {
+        const double q0 = (B1[1][2] - B1[2][1]) / lam, q1 = (B1[2][0] - B1[0][2]) / lam,
+                     q2 = (B1[0][1] - B1[1][0]) / lam;
+        const double x0 = B2[1][2] - B2[2][1], x1 = B2[2][0] - B2[0][2], x2 = B2[0][1] - B2[1][0];
+        acc[1] += c0 * (p[1] * u[2] - p[2] * u[1] - q0 + x0);
+        acc[2] += c0 * (p[2] * u[0] - p[0] * u[2] - q1 + x1);
+        acc[3] += c0 * (p[0] * u[1] - p[1] * u[0] - q2 + x2);
+    } else {
+        const double q0 = (B1[0][1] - B1[1][0]) / lam;
+        const double x0 = B2[0][1] - B2[1][0];
+        acc[1] += c0 * (p[0] * u[1] - p[1] * u[0] - q0 + x0);
+    }
+#pragma unroll
+    for (int q = 0; q < D; ++q) acc[1 + NR + q] += c0 * u[q];
+    if (a.dx_part) {
+        const int rows = a.i_end - a.i0;
+        for (int q = 0; q < D; ++q) a.dx_part[((size_t)jc * rows + (row - a.i0)) * D + q] = -c0 * u[q];
+    }
 }
 
 template <int D, int IPT_, bool GRAD>
@@ -299,88 +353,392 @@ struct ConvBody {
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
             if (row[ii] < 0) continue;
-            acc[0] += c0 * E64[ii];
-            if (!GRAD) continue;
-            double S[3][3] = {}, UUm[3][3] = {}, Am[3][3] = {};
-#pragma unroll
-            for (int q = 0; q < NS; ++q) {
-                const int ra = Sym<D>::a(q), rb = Sym<D>::b(q);
-                S[ra][rb] = S[rb][ra] = (double)sx[ii][q];
-                UUm[ra][rb] = UUm[rb][ra] = UUr[ii][q];
-                Am[ra][rb] = Am[rb][ra] = Ar[ii][q];
-            }
-            double u[3], p[3];
-#pragma unroll
-            for (int q = 0; q < D; ++q) {
-                u[q] = Ur[ii][q] / lam;        // sum N~ S^-1 d
-                p[q] = (double)x[ii][q] - t[q];
-            }
-            // B1 = S_x UU (for (S_x u) x u),  B2 = S_x A (for axial(S_x S^-1))
-            double B1[3][3] = {}, B2[3][3] = {};
-            for (int r0 = 0; r0 < D; ++r0)
-                for (int c1 = 0; c1 < D; ++c1)
-                    for (int k = 0; k < D; ++k) {
-                        B1[r0][c1] += S[r0][k] * UUm[k][c1];
-                        B2[r0][c1] += S[r0][k] * Am[k][c1];
-                    }
-            // (S_x u~) x u~ summed: component k = eps_kab (S_x UU)_ab ; / lam for the S scale
-            if (D == 3) {
-                const double q0 = (B1[1][2] - B1[2][1]) / lam, q1 = (B1[2][0] - B1[0][2]) / lam,
-                             q2 = (B1[0][1] - B1[1][0]) / lam;
-                const double x0 = B2[1][2] - B2[2][1], x1 = B2[2][0] - B2[0][2], x2 = B2[0][1] - B2[1][0];
-                acc[1] += c0 * (p[1] * u[2] - p[2] * u[1] - q0 + x0);
-                acc[2] += c0 * (p[2] * u[0] - p[0] * u[2] - q1 + x1);
-                acc[3] += c0 * (p[0] * u[1] - p[1] * u[0] - q2 + x2);
-            } else {
-                const double q0 = (B1[0][1] - B1[1][0]) / lam;
-                const double x0 = B2[0][1] - B2[1][0];
-                acc[1] += c0 * (p[0] * u[1] - p[1] * u[0] - q0 + x0);
-            }
-#pragma unroll
-            for (int q = 0; q < D; ++q) acc[1 + NR + q] += c0 * u[q];
-            if (a.dx_part) {
-                const int rows = a.i_end - a.i0;
-                for (int q = 0; q < D; ++q)
-                    a.dx_part[((size_t)jc * rows + (row[ii] - a.i0)) * D + q] = -c0 * u[q];
-            }
+            conv_contract<D, NV, GRAD>(a, jc, row[ii], x[ii], sx[ii], E64[ii], Ur[ii], UUr[ii], Ar[ii], lam, c0, t,
+                                       acc);
         }
     }
 };
 
-template <class Body, int NT, int TJ>
-__global__ void __launch_bounds__(NT) conv_kernel(PairArgs a)
+// ---------------------------------------------------------------------------
+// Packed CONV: two targets per f32x2 operation (YRec2 pair records).
+//   f0..f2 -y'hi, f3 lv (0, or -inf for padding), f4..f6 -y'lo, f7 + k  R St_y R^T packed
+//   entry k (Sym order), then the negated off-diagonal entries (3D: f13..f15, 2D: f10), so
+//   that every adjugate entry is one multiply and one fused multiply-add without negation.
+// Padding targets: y' = 0, St_y = I, lv = -inf (finite arithmetic, zero contribution).
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void conv_prologue2_kernel(const double* __restrict__ pose, const float* __restrict__ y,
+                                      const float* __restrict__ ycov, int M, int M_pad, YRec2* __restrict__ yrec)
+{
+    constexpr int NS = Sym<D>::N;
+    double R[9], t[3];
+    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
+    const int stride = gridDim.x * blockDim.x;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < M_pad / 2; p += stride) {
+        float f[2][16];
+        for (int h = 0; h < 2; ++h) {
+            const int j = 2 * p + h;
+            for (int q = 0; q < 16; ++q) f[h][q] = 0.f;
+            float hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, sp[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < D; ++k) sp[k] = 1.f;
+            float lv = -INFINITY;
+            if (j < M) {
+                lv = 0.f;
+                for (int a = 0; a < D; ++a) {
+                    double v = R[a] * (double)y[(size_t)j * D] + R[a + D] * (double)y[(size_t)j * D + 1];
+                    if (D == 3) v = v + R[a + 6] * (double)y[(size_t)j * D + 2];
+                    v = v + t[a];
+                    hi[a] = __double2float_rn(v);
+                    lo[a] = __double2float_rn(v - (double)hi[a]);
+                }
+                double A[3][3], T[3][3];
+                for (int k = 0; k < NS; ++k) {
+                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                    A[ra][rb] = A[rb][ra] = (double)ycov[(size_t)j * NS + k];
+                }
+                for (int r0 = 0; r0 < D; ++r0)
+                    for (int c0 = 0; c0 < D; ++c0) {
+                        double acc = 0;
+                        for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
+                        T[r0][c0] = acc;
+                    }
+                for (int k = 0; k < NS; ++k) {
+                    double acc = 0;
+                    for (int q = 0; q < D; ++q) acc += R[Sym<D>::a(k) + D * q] * T[q][Sym<D>::b(k)];
+                    sp[k] = __double2float_rn(acc);
+                }
+            }
+            for (int a = 0; a < D; ++a) {
+                f[h][a] = -hi[a];
+                f[h][4 + a] = -lo[a];
+            }
+            f[h][3] = lv;
+            for (int k = 0; k < NS; ++k) f[h][7 + k] = sp[k];
+            for (int k = D; k < NS; ++k) f[h][7 + NS + (k - D)] = -sp[k];
+        }
+        YRec2 r;
+        for (int q = 0; q < 8; ++q) r.q[q] = make_float4(f[0][2 * q], f[1][2 * q], f[0][2 * q + 1], f[1][2 * q + 1]);
+        yrec[p] = r;
+    }
+}
+
+__device__ __forceinline__ float2 fld2(const YRec2& r, int f)
+{
+    const float4 q = r.q[f >> 1];
+    return (f & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+}
+
+template <int D, int IPT_, bool GRAD>
+struct PackedConvBody {
+    using StreamRec = YRec2;
+    static constexpr int IPT = IPT_;
+    static constexpr int NS = Sym<D>::N, NR = Sym<D>::NR, NO = NS - D;
+    static constexpr int NV = GRAD ? 1 + NR + D : 1;
+    float2 X[IPT][D], SX[IPT][NS], OX[IPT][NO];  // duplicated in both halves; OX = -off-diagonals
+    float2 e[IPT];                               // energy, tile level
+    float2 U[IPT][GRAD ? D : 1], UU[IPT][GRAD ? NS : 1], A[IPT][GRAD ? NS : 1];   // item level
+    double E64[IPT];
+    int row[IPT];
+    float kl;
+    double c0, lam, t[3];
+    const float* ycov;
+    const double* pose;
+
+    __device__ void setup(const PairArgs& a)
+    {
+        lam = a.pose[kPoseSig] * a.Lmax;   // Lmax carries the covariance scale c for this body
+        kl = (float)(K_EXP2 / lam);
+        ycov = a.ycov;
+        pose = a.pose;
+        c0 = pow(2.0 * 3.14159265358979323846 * lam, -0.5 * D);
+        for (int q = 0; q < D; ++q) t[q] = a.pose[kPoseT + q];
+    }
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        row[ii] = i < a.i_end ? i : -1;
+        const XRec r = static_cast<const XRec*>(a.xrec)[i < a.i_end ? i : 0];
+        const bool ok = i < a.i_end;
+        const float xv[3] = {r.v0.x, r.v0.y, r.v0.z};
+        const float sv[6] = {r.v2.x, r.v2.y, r.v2.z, r.v2.w, r.v3.x, r.v3.y};
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            const float v = ok ? xv[q] : 0.f;
+            X[ii][q] = make_float2(v, v);
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            const float v = ok ? sv[q] : (q < D ? 1.f : 0.f);
+            SX[ii][q] = make_float2(v, v);
+            if (q >= D) OX[ii][q - D] = make_float2(-v, -v);
+        }
+    }
+    __device__ void zero_all()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            e[ii] = make_float2(0.f, 0.f);
+            E64[ii] = 0.0;
+            if (GRAD) {
+#pragma unroll
+                for (int q = 0; q < D; ++q) U[ii][q] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < NS; ++q) { UU[ii][q] = make_float2(0.f, 0.f); A[ii][q] = make_float2(0.f, 0.f); }
+            }
+        }
+    }
+    // One half of a pack the fast path cannot take (near-singular, not positive definite):
+    // the scalar rules of ConvBody, FP64 for near-singular pairs.
+    __device__ __forceinline__ void rare_half(int ii, const YRec2& r, int j, int h, const float* d, const float* sv,
+                                              const float* ad, float det, float& Nt, float& rd, float* hv, float* av)
+    {
+        Nt = 0.f;
+        rd = 0.f;
+        for (int q = 0; q < D; ++q) hv[q] = 0.f;
+        for (int k = 0; k < NS; ++k) av[k] = 0.f;
+        const float lvh = h ? fld2(r, 3).y : fld2(r, 3).x;
+        if (lvh == -INFINITY) return;   // padding target
+        float prod = sv[0] * sv[1];
+        if (D == 3) prod *= sv[2];
+        if (det < 1e-6f * prod) {
+            float yh[3] = {0, 0, 0}, yl[3] = {0, 0, 0};
+            for (int q = 0; q < D; ++q) {
+                const float2 a = fld2(r, q), b = fld2(r, 4 + q);
+                yh[q] = -(h ? a.y : a.x);
+                yl[q] = -(h ? b.y : b.x);
+            }
+            const float4 v0 = make_float4(yh[0], yh[1], yh[2], 1.f), v1 = make_float4(yl[0], yl[1], yl[2], 0.f);
+            float xs[3] = {0, 0, 0}, sxs[6] = {0, 0, 0, 0, 0, 0};
+            for (int q = 0; q < D; ++q) xs[q] = X[ii][q].x;
+            for (int k = 0; k < NS; ++k) sxs[k] = SX[ii][k].x;
+            if (!conv_pair_f64<D>(xs, sxs, v0, v1, ycov + (size_t)j * NS, pose, (double)kl, av, hv, &rd, &Nt)) {
+                Nt = 0.f;
+                rd = 0.f;
+                for (int q = 0; q < D; ++q) hv[q] = 0.f;
+                for (int k = 0; k < NS; ++k) av[k] = 0.f;
+            }
+            return;
+        }
+        if (!(det > 0.f)) return;   // not positive definite: no contribution
+        for (int k = 0; k < NS; ++k) av[k] = ad[k];
+        float m = 0.f;
+        for (int q = 0; q < D; ++q) {
+            float acc = 0.f;
+            for (int c = 0; c < D; ++c) {
+                const int k = q == c ? q : (D == 2 ? 2 : (q + c == 1 ? 3 : (q + c == 2 ? 4 : 5)));
+                acc = fmaf(ad[k], d[c], acc);
+            }
+            hv[q] = acc;
+            m = fmaf(d[q], acc, m);
+        }
+        const float rs = rsqrtf(det);
+        rd = rs * rs;
+        Nt = rs * ex2(m * (rd * kl));
+    }
+    __device__ __forceinline__ void consume(const YRec2& r, int jrec)
+    {
+        float2 ny[3], nl[3], cy[6], oy[3];
+#pragma unroll
+        for (int q = 0; q < D; ++q) { ny[q] = fld2(r, q); nl[q] = fld2(r, 4 + q); }
+        const float2 lv = fld2(r, 3);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) cy[k] = fld2(r, 7 + k);
+#pragma unroll
+        for (int k = 0; k < NO; ++k) oy[k] = fld2(r, 7 + NS + k);
+        const float2 KL = make_float2(kl, kl), EPS = make_float2(1e6f, 1e6f);
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            float2 d[3], sm[6], o[3], adj[6], det, h[3], rd, Nt;
+#pragma unroll
+            for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(X[ii][q], ny[q]), nl[q]);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) sm[k] = fadd2(SX[ii][k], cy[k]);
+#pragma unroll
+            for (int k = 0; k < NO; ++k) o[k] = fadd2(OX[ii][k], oy[k]);
+            float2 prod;
+            if (D == 3) {
+                adj[0] = ffma2(o[2], sm[5], fmul2(sm[1], sm[2]));
+                adj[1] = ffma2(o[1], sm[4], fmul2(sm[0], sm[2]));
+                adj[2] = ffma2(o[0], sm[3], fmul2(sm[0], sm[1]));
+                adj[3] = ffma2(sm[4], sm[5], fmul2(o[0], sm[2]));
+                adj[4] = ffma2(sm[3], sm[5], fmul2(o[1], sm[1]));
+                adj[5] = ffma2(sm[3], sm[4], fmul2(o[2], sm[0]));
+                det = ffma2(sm[4], adj[4], ffma2(sm[3], adj[3], fmul2(sm[0], adj[0])));
+                prod = fmul2(fmul2(sm[0], sm[1]), sm[2]);
+            } else {
+                adj[0] = sm[1];
+                adj[1] = sm[0];
+                adj[2] = o[0];
+                det = ffma2(o[0], sm[2], fmul2(sm[0], sm[1]));
+                prod = fmul2(sm[0], sm[1]);
+            }
+            // fast path: both halves positive definite and well conditioned (NaN fails too)
+            const float2 dd = fmul2(det, EPS);
+            const bool fast = (dd.x >= prod.x) & (dd.y >= prod.y) & (det.x > 0.f) & (det.y > 0.f);
+            if (fast) {
+                if (D == 3) {
+                    h[0] = ffma2(adj[4], d[2], ffma2(adj[3], d[1], fmul2(adj[0], d[0])));
+                    h[1] = ffma2(adj[5], d[2], ffma2(adj[1], d[1], fmul2(adj[3], d[0])));
+                    h[2] = ffma2(adj[2], d[2], ffma2(adj[5], d[1], fmul2(adj[4], d[0])));
+                } else {
+                    h[0] = ffma2(adj[2], d[1], fmul2(adj[0], d[0]));
+                    h[1] = ffma2(adj[1], d[1], fmul2(adj[2], d[0]));
+                }
+                float2 m = fmul2(d[0], h[0]);
+#pragma unroll
+                for (int q = 1; q < D; ++q) m = ffma2(d[q], h[q], m);
+                const float2 rs = make_float2(rsqrtf(det.x), rsqrtf(det.y));
+                rd = fmul2(rs, rs);
+                const float2 arg = ffma2(m, fmul2(rd, KL), lv);
+                Nt = fmul2(rs, make_float2(ex2(arg.x), ex2(arg.y)));
+            } else {
+                float dv[2][3], sv[2][6], av[2][6], hv[2][3], nt[2], rdv[2];
+                for (int hh = 0; hh < 2; ++hh) {
+                    for (int q = 0; q < D; ++q) dv[hh][q] = hh ? d[q].y : d[q].x;
+                    for (int k = 0; k < NS; ++k) {
+                        sv[hh][k] = hh ? sm[k].y : sm[k].x;
+                        av[hh][k] = hh ? adj[k].y : adj[k].x;
+                    }
+                }
+                float ao[2][6];
+                rare_half(ii, r, 2 * jrec, 0, dv[0], sv[0], av[0], det.x, nt[0], rdv[0], hv[0], ao[0]);
+                rare_half(ii, r, 2 * jrec + 1, 1, dv[1], sv[1], av[1], det.y, nt[1], rdv[1], hv[1], ao[1]);
+                Nt = make_float2(nt[0], nt[1]);
+                rd = make_float2(rdv[0], rdv[1]);
+                for (int q = 0; q < D; ++q) h[q] = make_float2(hv[0][q], hv[1][q]);
+                for (int k = 0; k < NS; ++k) adj[k] = make_float2(ao[0][k], ao[1][k]);
+            }
+            e[ii] = fadd2(e[ii], Nt);
+            if (GRAD) {
+                const float2 nr = fmul2(Nt, rd), nr2 = fmul2(nr, rd);
+                float2 w[3];
+#pragma unroll
+                for (int q = 0; q < D; ++q) {
+                    U[ii][q] = ffma2(nr, h[q], U[ii][q]);
+                    w[q] = fmul2(nr2, h[q]);
+                }
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    UU[ii][k] = ffma2(w[Sym<D>::a(k)], h[Sym<D>::b(k)], UU[ii][k]);
+                    A[ii][k] = ffma2(nr, adj[k], A[ii][k]);
+                }
+            }
+        }
+    }
+    __device__ void fold()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            E64[ii] += (double)e[ii].x + (double)e[ii].y;
+            e[ii] = make_float2(0.f, 0.f);
+        }
+    }
+    __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            double ur[3] = {0, 0, 0}, uur[6] = {0, 0, 0, 0, 0, 0}, ar[6] = {0, 0, 0, 0, 0, 0};
+            if (GRAD) {
+#pragma unroll
+                for (int q = 0; q < D; ++q) ur[q] = (double)U[ii][q].x + (double)U[ii][q].y;
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    uur[k] = (double)UU[ii][k].x + (double)UU[ii][k].y;
+                    ar[k] = (double)A[ii][k].x + (double)A[ii][k].y;
+                }
+            }
+            float xs[3] = {0, 0, 0}, sxs[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < D; ++q) xs[q] = X[ii][q].x;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) sxs[k] = SX[ii][k].x;
+            conv_contract<D, NV, GRAD>(a, jc, row[ii], xs, sxs, E64[ii], ur, uur, ar, lam, c0, t, acc);
+        }
+    }
+};
+
+template <class Body, int NT, int TJ, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) conv_kernel(PairArgs a)
 {
     Body body;
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
 using KernelFn = void (*)(PairArgs);
+
+struct ConvVariant {
+    KernelShape shape;
+    KernelFn fn;
+};
+
+// compiled CONV shapes; the first of each list is the default
+template <int D>
+static const std::vector<ConvVariant>& conv_variants(bool grad)
+{
+    static const std::vector<ConvVariant> g = {
+        {{1, 64, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 64, 32, 6>},
+        {{1, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 128, 32, 3>},
+        {{1, 128, 64, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 128, 64, 2>},
+        {{1, 128, 64}, conv_kernel<ConvBody<D, 1, true>, 128, 64>},
+        {{2, 128, 64}, conv_kernel<ConvBody<D, 2, true>, 128, 64>},
+        {{1, 256, 32}, conv_kernel<ConvBody<D, 1, true>, 256, 32>},
+        {{1, 64, 64}, conv_kernel<ConvBody<D, 1, true>, 64, 64>},
+    };
+    static const std::vector<ConvVariant> e = {
+        {{1, 128, 32, 2}, conv_kernel<PackedConvBody<D, 1, false>, 128, 32, 4>},
+        {{2, 128, 32, 2}, conv_kernel<PackedConvBody<D, 2, false>, 128, 32, 3>},
+        {{2, 128, 64}, conv_kernel<ConvBody<D, 2, false>, 128, 64>},
+        {{1, 128, 64}, conv_kernel<ConvBody<D, 1, false>, 128, 64>},
+        {{4, 128, 64}, conv_kernel<ConvBody<D, 4, false>, 128, 64>},
+        {{2, 256, 32}, conv_kernel<ConvBody<D, 2, false>, 256, 32>},
+    };
+    return grad ? g : e;
+}
+
+std::vector<KernelShape> conv_shapes(bool grad)
+{
+    std::vector<KernelShape> s;
+    for (auto& v : conv_variants<3>(grad)) s.push_back(v.shape);
+    return s;
+}
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
                         cudaStream_t s);
 
 int conv_launch(Context& c, const double* pose_dev, bool grad, int i0, int i1, double* out_dev, double* dEdx_dev,
-                cudaStream_t s, const KernelShape*)
+                cudaStream_t s, const KernelShape* force)
 {
+    const KernelShape want = force ? *force : (grad ? c.shape_conv_adj : c.shape_conv_energy);
+    const std::vector<ConvVariant>& vars = c.D == 3 ? conv_variants<3>(grad) : conv_variants<2>(grad);
+    const ConvVariant* v = &vars[0];
+    for (auto& cand : vars)
+        if (cand.shape.same(want)) v = &cand;
+    const bool packed = v->shape.pack == 2;
+    // source records always; target records scalar (YRec) or paired (YRec2, same bytes)
     const int n = std::max(c.M_pad, c.N_pad);
     const int g = std::min((n + 255) / 256, c.num_sms * 4);
+    const int my = packed ? 0 : c.M, myp = packed ? 0 : c.M_pad;
     if (c.D == 3)
-        conv_prologue_kernel<3><<<g, 256, 0, s>>>(pose_dev, c.y, c.ycov, c.M, c.M_pad, c.yrec, c.x, c.xcov, c.N,
-                                                  c.N_pad, c.xrec);
+        conv_prologue_kernel<3><<<g, 256, 0, s>>>(pose_dev, c.y, c.ycov, my, myp, c.yrec, c.x, c.xcov, c.N, c.N_pad,
+                                                  c.xrec);
     else
-        conv_prologue_kernel<2><<<g, 256, 0, s>>>(pose_dev, c.y, c.ycov, c.M, c.M_pad, c.yrec, c.x, c.xcov, c.N,
-                                                  c.N_pad, c.xrec);
+        conv_prologue_kernel<2><<<g, 256, 0, s>>>(pose_dev, c.y, c.ycov, my, myp, c.yrec, c.x, c.xcov, c.N, c.N_pad,
+                                                  c.xrec);
     DUGMA_CK(cudaGetLastError());
-    const KernelShape sh{grad ? 1 : 2, 128, 64};
-    KernelFn fn;
-    if (c.D == 3)
-        fn = grad ? conv_kernel<ConvBody<3, 1, true>, 128, 64> : conv_kernel<ConvBody<3, 2, false>, 128, 64>;
-    else
-        fn = grad ? conv_kernel<ConvBody<2, 1, true>, 128, 64> : conv_kernel<ConvBody<2, 2, false>, 128, 64>;
+    if (packed) {
+        YRec2* y2 = reinterpret_cast<YRec2*>(c.yrec);
+        const int g2 = std::min((c.M_pad / 2 + 255) / 256, c.num_sms * 4);
+        if (c.D == 3)
+            conv_prologue2_kernel<3><<<g2, 256, 0, s>>>(pose_dev, c.y, c.ycov, c.M, c.M_pad, y2);
+        else
+            conv_prologue2_kernel<2><<<g2, 256, 0, s>>>(pose_dev, c.y, c.ycov, c.M, c.M_pad, y2);
+        DUGMA_CK(cudaGetLastError());
+    }
     const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
-    return launch_pair_variant(c, fn, sh, c.xrec, c.yrec, (size_t)c.M_pad, nv, c.cscale, pose_dev, i0, i1, out_dev,
-                               grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
+    return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad / v->shape.pack, nv, c.cscale,
+                               pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
 }
 
 }  // namespace dugma

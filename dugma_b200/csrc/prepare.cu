@@ -5,82 +5,10 @@
 // FP32 rounding of y' match the CPU oracle bit for bit.
 #include <cmath>
 #include <cstdio>
-#include <cstring>
-#include <map>
-#include <mutex>
-#include <thread>
-#include <vector>
 
 #include "context.hpp"
 
 namespace dugma {
-
-// ---------------------------------------------------------------------------
-// Host -> device upload of pageable caller arrays through a pinned staging ring: the
-// host copies chunk k into a pinned buffer (split over a few threads when large) while
-// the copy engine moves chunk k - 1, so the upload runs at host-copy speed instead of
-// the driver's pageable path.  One ring per device, shared by every init of the
-// process (serialised by a mutex).
-// ---------------------------------------------------------------------------
-constexpr size_t kStageChunk = (size_t)4 << 20;
-constexpr int kStageBufs = 3;
-
-struct StageRing {
-    char* buf[kStageBufs] = {};
-    cudaEvent_t done[kStageBufs] = {};
-    bool ok = false;
-};
-
-static std::mutex g_stage_mu;
-static std::map<int, StageRing> g_stage;
-
-static void par_memcpy(char* dst, const char* src, size_t n)
-{
-    constexpr size_t kPart = (size_t)1 << 20;
-    const int parts = (int)std::min<size_t>(4, n / kPart);
-    if (parts < 2) {
-        memcpy(dst, src, n);
-        return;
-    }
-    const size_t per = (n + parts - 1) / parts;
-    std::vector<std::thread> th;
-    for (int k = 1; k < parts; ++k) {
-        const size_t o = k * per, len = std::min(per, n - o);
-        th.emplace_back([=] { memcpy(dst + o, src + o, len); });
-    }
-    memcpy(dst, src, std::min(per, n));
-    for (auto& t : th) t.join();
-}
-
-// Copies `bytes` from pageable `src` to device `dst` on stream s (ordered with the
-// stream's later work); returns a CUDA error or cudaSuccess.  The caller's array may be
-// reused when this returns: the last chunk is still in flight only from pinned memory.
-static cudaError_t staged_upload(int dev, cudaStream_t s, void* dst, const void* src, size_t bytes)
-{
-    std::lock_guard<std::mutex> lock(g_stage_mu);
-    StageRing& r = g_stage[dev];
-    if (!r.ok) {
-        for (int k = 0; k < kStageBufs; ++k) {
-            cudaError_t e = cudaHostAlloc((void**)&r.buf[k], kStageChunk, cudaHostAllocPortable);
-            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.done[k], cudaEventDisableTiming);
-            if (e != cudaSuccess) return e;
-        }
-        r.ok = true;
-    }
-    static int slot = 0;
-    for (size_t off = 0; off < bytes; off += kStageChunk) {
-        const size_t len = std::min(kStageChunk, bytes - off);
-        const int k = slot;
-        slot = (slot + 1) % kStageBufs;
-        cudaError_t e = cudaEventSynchronize(r.done[k]);   // the buffer's previous copy has finished
-        if (e != cudaSuccess) return e;
-        par_memcpy(r.buf[k], static_cast<const char*>(src) + off, len);
-        e = cudaMemcpyAsync(static_cast<char*>(dst) + off, r.buf[k], len, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaEventRecord(r.done[k], s);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
 
 // ---------------------------------------------------------------------------
 // init: FP64 -> FP32 conversion (init.cu:192-234) fused with the per-point inverse
@@ -185,10 +113,12 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
         if (e != cudaSuccess && rc == DUGMA_OK)
             rc = set_error(DUGMA_ERR_CUDA, "init: %s failed: %s", what, cudaGetErrorString(e));
     };
-    ck(staged_upload(c.dev, s, tX, X, sizeof(double) * nd), "copy X");
-    ck(staged_upload(c.dev, s, tXC, XC, sizeof(double) * nd * D), "copy X_C");
-    ck(staged_upload(c.dev, s, tY, Y, sizeof(double) * md), "copy Y");
-    ck(staged_upload(c.dev, s, tYC, YC, sizeof(double) * md * D), "copy Y_C");
+    // pageable sources: the driver pipelines these through its own pinned buffers (a
+    // host-side copy into a pinned ring of ours measured slower on the B200 host)
+    ck(cudaMemcpyAsync(tX, X, sizeof(double) * nd, cudaMemcpyHostToDevice, s), "copy X");
+    ck(cudaMemcpyAsync(tXC, XC, sizeof(double) * nd * D, cudaMemcpyHostToDevice, s), "copy X_C");
+    ck(cudaMemcpyAsync(tY, Y, sizeof(double) * md, cudaMemcpyHostToDevice, s), "copy Y");
+    ck(cudaMemcpyAsync(tYC, YC, sizeof(double) * md * D, cudaMemcpyHostToDevice, s), "copy Y_C");
     ck(cudaMemsetAsync(c.counter, 0, sizeof(int) * 8, s), "memset");
     const int bs = 256;
     const int gx = std::min((N + bs - 1) / bs, c.num_sms * 8), gy = std::min((M + bs - 1) / bs, c.num_sms * 8);

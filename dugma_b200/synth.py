@@ -290,19 +290,42 @@ KINECT_V2 = (512, 424, 365.0, 365.0, 255.5, 211.5)
 
 
 def kinect_like(trial: int = 0) -> Problem:
-    """Stand-in for one two-camera depth scene: 12 boxes and 8 spheres (no background, so no
-    plane dominates) seen by two 512x424 depth cameras (f = 365 px) whose relative pose is a
-    rotation of up to 20 deg and a translation in [-0.2, 0.2]^3 m, subsampled to
-    N ~ U[3598, 5334] and M ~ U[463, 5159] points (the size ranges of two-sensor scenes),
-    depth-dependent sensor covariances."""
+    """Stand-in for one two-sensor depth scene (the shape of the reference's 30 Kinect scenes:
+    clouds cropped to the shared ~1.2 m working volume, N ~ U[3598, 5334] and M ~ U[463, 5159]
+    points, isotropic "uncertainty" covariances c_i I with c_i in [1.3, 7.9]).
+
+    12 boxes and 8 spheres fill a 1.2 m volume centred 1.8 m in front of camera 1 (the world
+    frame).  Camera 2 orbits the volume's centre by a rotation of up to 30 deg about a random
+    axis, plus a translation in [-0.1, 0.1]^3 m, so it sees the scene from another side.  Both
+    are 512x424 depth cameras (f = 365 px).  Each view keeps its points inside the working
+    volume, is subsampled, and expressed in its own camera frame; c_i grows geometrically
+    with the point's depth from 1.3 at 0.5 m to 7.9 at 4 m.  Ground truth: R_G y + t_G is the
+    world position of camera-2 point y."""
     rng = rng_for(5, trial)
-    boxes, spheres = _random_scene(rng, n_boxes=12, n_spheres=8, z=(1.0, 3.5))
+    centre = np.array([0.0, 0.0, 1.8])
+    boxes, spheres = [], []
+    for _ in range(12):
+        c = centre + rng.uniform(-0.45, 0.45, 3)
+        h = rng.uniform(0.05, 0.2, 3)
+        boxes.append((c - h, c + h))
+    for _ in range(8):
+        spheres.append((centre + rng.uniform(-0.45, 0.45, 3), rng.uniform(0.08, 0.25)))
     n = int(rng.integers(3598, 5335))
     m = int(rng.integers(463, 5160))
-    X, XC = _range_view(rng, n, boxes, spheres, np.eye(3), np.zeros(3), KINECT_V2)
-    Rv = random_rotation(rng, 20.0)
-    tv = rng.uniform(-0.2, 0.2, 3)
-    Y, YC = _range_view(rng, m, boxes, spheres, Rv, tv, KINECT_V2)
+    Rv = random_rotation(rng, 30.0)
+    tv = centre - Rv @ centre + rng.uniform(-0.1, 0.1, 3)
+
+    def view(R, t, k):
+        P, _ = _range_view(rng, 10 ** 9, boxes, spheres, R, t, KINECT_V2)
+        world = P @ R.T + t
+        keep = np.flatnonzero(np.all(np.abs(world - centre) <= 0.6, axis=1))
+        keep = rng.choice(keep, size=min(k, keep.size), replace=False)
+        P = P[keep]
+        c = 1.3 * (7.9 / 1.3) ** np.clip((P[:, 2] - 0.5) / 3.5, 0.0, 1.0)
+        return P, c[:, None, None] * np.eye(3)
+
+    X, XC = view(np.eye(3), np.zeros(3), n)
+    Y, YC = view(Rv, tv, m)
     return Problem(X, Y, XC, YC, Rv, tv, f"twoview{trial}")
 
 

@@ -139,11 +139,13 @@ int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv, const floa
 
 /* ---------------- tuning and graphs ---------------- */
 
-/* Times the kernel shapes of `what` (0 = adjoint, 1 = energy, 2 = nearest neighbour) on this
- * context and keeps the fastest; writes a one-line report into `report` (may be NULL). */
+/* Times the kernel shapes of `what` (0 = adjoint, 1 = energy, 2 = nearest neighbour, 3 = CONV
+ * adjoint, 4 = CONV energy) on this context and keeps the fastest; writes a one-line report
+ * into `report` (may be NULL).  `model` selects REF or CONV for what = 0 and 1. */
 int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t report_len);
 
-/* Kernel shapes available for `what` (0 adjoint, 1 energy, 2 nearest neighbour): writes up to
+/* Kernel shapes available for `what` (0 adjoint, 1 energy, 2 nearest neighbour, 3 CONV adjoint,
+ * 4 CONV energy): writes up to
  * `max` tuples {source points per thread, threads per block, records per tile, targets per
  * record} into shapes[4 * k] and returns the count (negative status on error). */
 int dugma_shapes(int what, int* shapes, int max);

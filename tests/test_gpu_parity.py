@@ -165,10 +165,11 @@ def test_energy_adjoint_ragged_sizes(D, n, m):
         api.fr_m(h)
 
 
-@pytest.mark.parametrize("what", [0, 1])
+@pytest.mark.parametrize("what", [0, 1, 3, 4])
 @pytest.mark.parametrize("D", [3, 2])
 def test_every_kernel_shape_matches_oracle(what, D):
-    """Each compiled shape (scalar and packed f32x2 pair kernels) against the oracle."""
+    """Each compiled shape (REF scalar and packed f32x2 pair kernels: what 0 adjoint, 1 energy;
+    CONV: 3 adjoint, 4 energy) against the oracle."""
     X, XC, Y, YC = _problem_small(D, 700, 1111, seed=21, bad=(3,))
     st = orc.State(X, XC, Y, YC)
     import warnings
@@ -177,15 +178,17 @@ def test_every_kernel_shape_matches_oracle(what, D):
         _, h = api.init(X, XC, Y, YC)
     try:
         R, t = _pose(D, seed=8)
-        Eo, go, dxo = st.energy(R, t, 0.2, with_dx=True)
+        model = 1 if what >= 3 else 0
+        ref = st.energy_conv if model else st.energy
+        Eo, go, dxo = ref(R, t, 0.2, with_dx=True)
         for shape in api.shapes(what):
             api.set_shape(h, what, shape)
-            if what == 0:
-                E, g, dx = api.energy_grad(h, R, t, 0.2, with_dx=True)
+            if what in (0, 3):
+                E, g, dx = api.energy_grad(h, R, t, 0.2, model=model, with_dx=True)
                 assert _rel(g, go) <= 1e-5, shape
                 assert _rel(dx, dxo) <= 1e-4, shape
             else:
-                E = api.energy(h, R, t, 0.2)
+                E = api.energy(h, R, t, 0.2, model=model)
             assert abs(E - Eo) <= 1e-6 * Eo, (shape, E, Eo)
     finally:
         api.fr_m(h)
