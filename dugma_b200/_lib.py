@@ -28,6 +28,7 @@ EXPORTS = {
     "dugma_init": (c_int, [dp, dp, dp, dp, dp, c_int, c_int, c_int, PtrArray]),
     "dugma_update_sig": (c_int, [PtrArray, dp, dp, dp, dp, dp, fp]),
     "dugma_compi": (c_int, [PtrArray, dp, dp, dp, dp, dp, dp, dp]),
+    "dugma_compi_range": (c_int, [PtrArray, dp, dp, c_double, c_int, c_int, c_int, c_int, dp]),
     "dugma_fr_m": (c_int, [PtrArray]),
     "dugma_last_error": (ctypes.c_char_p, []),
     "dugma_energy": (c_int, [PtrArray, dp, dp, c_double, c_int, dp]),

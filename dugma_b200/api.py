@@ -105,6 +105,15 @@ def compi(h: Handles, R, t, N=None, M=None, D=None, sig=None) -> np.ndarray:
     return out[: 637 if h.D == 3 else 45].copy()
 
 
+def compi_range(h: Handles, R, t, sig, i0, i1, j0, j1) -> np.ndarray:
+    """Partial coefficients: source-side terms of source rows [i0, i1) plus target-side terms of
+    target rows [j0, j1); partials over partitions of both ranges sum to compi's."""
+    out = np.zeros(640)
+    check(_lib.load().dugma_compi_range(h.arr, _ptr(_cm(R)), _ptr(_d(t)), float(sig), int(i0), int(i1), int(j0),
+                                        int(j1), _ptr(out)))
+    return out[: 637 if h.D == 3 else 45].copy()
+
+
 def fr_m(h: Handles) -> float:
     check(_lib.load().dugma_fr_m(h.arr))
     h.alive = False

@@ -432,6 +432,25 @@ int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N
     return coef_from_moments(c->D, mom, coefficient);
 }
 
+int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double sig, int i_begin, int i_end,
+                      int j_begin, int j_end, double coefficient[640])
+{
+    if (!R || !t || !coefficient) return set_error(DUGMA_ERR_ARG, "compi_range: null argument");
+    if (!(sig > 0)) return set_error(DUGMA_ERR_ARG, "compi_range: sig must be positive");
+    GET_CTX(c, Ptr);
+    if (i_begin < 0 || i_end > c->N || i_begin > i_end || j_begin < 0 || j_end > c->M || j_begin > j_end)
+        return set_error(DUGMA_ERR_ARG, "compi_range: bad row ranges [%d, %d) x [%d, %d)", i_begin, i_end, j_begin,
+                         j_end);
+    DUGMA_RET(upload_pose(*c, R, t, sig));
+    const int nm = num_moments(c->D);
+    DUGMA_CK(cudaMemsetAsync(c->mom, 0, sizeof(double) * nm, c->stream));
+    DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream, i_begin, i_end, j_begin, j_end));
+    double mom[512];
+    DUGMA_CK(cudaMemcpyAsync(mom, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
+    DUGMA_RET(fetch(*c, c->out, 0, nullptr));
+    return coef_from_moments(c->D, mom, coefficient);
+}
+
 int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, int model, double* E)
 {
     if (!R || !t || !E) return set_error(DUGMA_ERR_ARG, "energy: null argument");

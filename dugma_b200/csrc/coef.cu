@@ -385,7 +385,8 @@ static int upload_moment_tables(int dev)
 }
 
 template <int D>
-static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0,
+                     int j1)
 {
     DUGMA_RET(upload_moment_tables(c.dev));
     DUGMA_RET(c.ensure_coef_records());
@@ -394,10 +395,21 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128);
     DUGMA_CK(cudaGetLastError());
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
-    const KernelShape sh{2, 128, 32};
-    KernelFn fn = coef_pass_kernel<CoefBody<D, 2>, 128, 32>;
+    // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
+    // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
+    // streamed records (128 .. 512), which bounds the per-chunk H partials the moments
+    // kernel has to sum to about 8 copies of the rows' H
+    auto pass_shape = [&](int rows, KernelFn* fn) {
+        const int min_chunk = std::max(128, std::min(512, rows / 8));
+        if (rows >= 2 * 256 * c.num_sms) {
+            *fn = coef_pass_kernel<CoefBody<D, 2>, 128, 32>;
+            return KernelShape{2, 128, 32, 1, 0, min_chunk};
+        }
+        *fn = coef_pass_kernel<CoefBody<D, 1>, 64, 32>;
+        return KernelShape{1, 64, 32, 1, 0, min_chunk};
+    };
     // blocks of the moments kernel: about 32 rows each, at most 2 per SM (the partial buffer's size)
-    const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
+    const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(i1 - i0, j1 - j0) + 31) / 32));
     double* mom = c.mom_part;
     int rc = DUGMA_OK;
     int nb_side[2] = {0, 0};
@@ -405,26 +417,28 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         // side 0: sources stationary over streamed targets; side 1: the reverse
         double* hp = nullptr;
         int n_jc = 0;
-        PairArgs dummy{};
-        (void)dummy;
         const Rec128* src = side == 0 ? c.xrec128 : c.yrec128;
         const Rec128* str = side == 0 ? c.yrec128 : c.xrec128;
-        const int rows = side == 0 ? c.N : c.M;
+        const int r0 = side == 0 ? i0 : j0, r1 = side == 0 ? i1 : j1, rows = r1 - r0;
+        if (rows <= 0) continue;   // an empty range contributes nothing
         const size_t nstr = side == 0 ? (size_t)c.M_pad : (size_t)c.N_pad;
         const double Lmax = side == 0 ? c.Lmax_y : c.Lmax_x;
         // launch_pair_variant reads the stationary weights from c.wx; swap for the target pass
         float* wsave = c.wx;
         if (side == 1) c.wx = c.wy;
-        rc = launch_pair_variant(c, fn, sh, src, str, nstr, 1, Lmax, pose_dev, 0, rows, nullptr, nullptr, &hp, 16,
+        KernelFn fn;
+        const KernelShape sh = pass_shape(rows, &fn);
+        rc = launch_pair_variant(c, fn, sh, src, str, nstr, 1, Lmax, pose_dev, r0, r1, nullptr, nullptr, &hp, 16,
                                  &n_jc, s);
         c.wx = wsave;
         if (rc != DUGMA_OK) break;
         const int nb = std::min(nblk, rows);
         nb_side[side] = nb;
+        const size_t o1 = (size_t)r0 * c.D, o2 = (size_t)r0 * c.D * c.D;
         if (side == 0)
-            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x, c.xinv, mom);
+            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x + o1, c.xinv + o2, mom);
         else
-            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y, c.yinv,
+            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y + o1, c.yinv + o2,
                                                          mom + (size_t)nblk * NM);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moments kernel launch failed");
     }
@@ -436,9 +450,12 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     return rc;
 }
 
-int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0, int j1)
 {
-    return c.D == 3 ? coef_impl<3>(c, pose_dev, moments_dev, s) : coef_impl<2>(c, pose_dev, moments_dev, s);
+    if (i1 < 0) i1 = c.N;
+    if (j1 < 0) j1 = c.M;
+    return c.D == 3 ? coef_impl<3>(c, pose_dev, moments_dev, s, i0, i1, j0, j1)
+                    : coef_impl<2>(c, pose_dev, moments_dev, s, i0, i1, j0, j1);
 }
 
 int coef_from_moments(int D, const double* mom, double* out640)

@@ -35,6 +35,8 @@ struct KernelShape {
     int tj = 0;       // streamed records per shared-memory tile
     int pack = 1;     // targets per streamed record (2: packed f32x2 kernels on pair records)
     int max_chunk = 0;   // most streamed records one work item may cover (0: no limit)
+    int min_chunk = 0;   // fewest streamed records per work item (0: no limit); bounds the
+                         // per-chunk partial buffers of the coefficient passes
     bool valid() const { return ipt > 0; }
     bool same(const KernelShape& o) const { return ipt == o.ipt && nt == o.nt && tj == o.tj && pack == o.pack; }
 };
@@ -126,7 +128,10 @@ int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2
 // sigma: out_dev[0] = exact FP64 sigma, out_dev[1] = quantised (reference) sigma.
 int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s);
 // Surrogate coefficient moments: out_dev receives kNumMoments doubles.
-int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s);
+// Source rows [i0, i1) carry the source-side (B) terms, target rows [j0, j1) the target-side
+// (C') terms; -1 for i1 / j1 means all rows.  Sums over partitions of both add up to the whole.
+int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0 = 0, int i1 = -1,
+                int j0 = 0, int j1 = -1);
 int coef_from_moments(int D, const double* moments, double* coef640);
 int num_moments(int D);
 

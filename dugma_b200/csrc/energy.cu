@@ -153,6 +153,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     const int target = 4 * resident;
     int n_jc = std::max(1, std::min(total_tiles, (target + n_ib - 1) / n_ib));
     if (sh.max_chunk > 0) n_jc = std::max(n_jc, (total_tiles * sh.tj + sh.max_chunk - 1) / sh.max_chunk);
+    if (sh.min_chunk > 0) n_jc = std::min(n_jc, std::max(1, total_tiles * sh.tj / sh.min_chunk));
     n_jc = std::min(n_jc, total_tiles);
     const int jc_tiles = (total_tiles + n_jc - 1) / n_jc;
     n_jc = (total_tiles + jc_tiles - 1) / jc_tiles;

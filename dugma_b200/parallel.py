@@ -5,8 +5,10 @@ Two ways the path divides (no collective is on the data path of either):
     rank, nothing exchanged (bench.py --gpus N);
   * one large problem split by source rows: each rank evaluates its rows
     (dugma_energy_grad_range) and the partial energies and pose gradients (7 doubles in
-    3D) are summed with one all-reduce.  The sum over rows is exactly the full sum up to
-    FP64 rounding of the final additions.
+    3D) are summed with one all-reduce; the surrogate coefficients likewise split by
+    source and target rows (dugma_compi_range) and are summed with one all-reduce of 637
+    (45 in 2D) doubles.  Sums over rows are exactly the full sums up to FP64 rounding of
+    the final additions.
 """
 from __future__ import annotations
 
@@ -56,3 +58,30 @@ def energy_grad_sharded(n_rows: int, rank: int, world: int,
         t = t.cpu()
     out = t.numpy()
     return float(out[0]), out[1:].copy()
+
+
+def _all_reduce_sum(vec: np.ndarray, world: int, group=None) -> np.ndarray:
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(np.ascontiguousarray(vec, dtype=np.float64))
+    if world > 1:
+        if dist.get_backend(group) == "nccl":
+            t = t.cuda()
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        t = t.cpu()
+    return t.numpy().copy()
+
+
+def compi_sharded(n_rows: int, m_rows: int, rank: int, world: int,
+                  compute: Callable[[int, int, int, int], np.ndarray], n_coef: int, group=None) -> np.ndarray:
+    """Surrogate coefficients summed over the ranks' source-row and target-row ranges.
+
+    `compute(i0, i1, j0, j1)` is the per-rank evaluation, normally
+    lambda i0, i1, j0, j1: dugma_b200.api.compi_range(handles, R, t, sig, i0, i1, j0, j1);
+    every rank returns the full n_coef-vector."""
+    i0, i1 = row_ranges(n_rows, world)[rank]
+    j0, j1 = row_ranges(m_rows, world)[rank]
+    part = np.zeros(n_coef)
+    if i1 > i0 or j1 > j0:
+        part = np.asarray(compute(i0, i1, j0, j1), dtype=np.float64).reshape(-1)[:n_coef]
+    return _all_reduce_sum(part, world, group)

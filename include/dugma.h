@@ -89,6 +89,13 @@ int dugma_energy_grad(float* Ptr[6], const double* R, const double* t, double si
 int dugma_energy_grad_range(float* Ptr[6], const double* R, const double* t, double sig, int model,
                             int i_begin, int i_end, double* E, double* g);
 
+/* Partial surrogate coefficients for sharding compi across GPUs: the source-side terms of
+ * source rows [i_begin, i_end) plus the target-side terms of target rows [j_begin, j_end).
+ * The coefficients are sums over rows, so the partials of any partition of both ranges add
+ * up to dugma_compi's (one all-reduce of 640 doubles).  No counterpart in the reference. */
+int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double sig, int i_begin, int i_end,
+                      int j_begin, int j_end, double coefficient[640]);
+
 /* The plain form: E plus central finite differences of step h over the NR + D pose
  * coordinates (1 + 2 (NR + D) energy evaluations). */
 int dugma_energy_fd_grad(float* Ptr[6], const double* R, const double* t, double sig, int model,

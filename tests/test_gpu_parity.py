@@ -379,6 +379,17 @@ def test_compi_coefficients(D):
         err = np.abs(A - Ao).max() / np.abs(Ao).max()
         print(f"{D}D coefficients: max |dA| / max |A| = {err:.3e}")
         assert err <= 2e-6
+        # partial coefficients over a 3-way partition of the source rows and an uneven
+        # 2-way partition of the target rows add up to the whole (sharding across GPUs)
+        n, m = X.shape[0], Y.shape[0]
+        parts = [api.compi_range(h, R, t, sig, 0, n // 3, 0, m // 4),
+                 api.compi_range(h, R, t, sig, n // 3, n // 2, m // 4, m),
+                 api.compi_range(h, R, t, sig, n // 2, n, m, m)]
+        S = np.sum(parts, axis=0)
+        assert np.abs(S - A).max() <= 1e-6 * np.abs(A).max()
+        assert np.abs(api.compi_range(h, R, t, sig, 0, n, 0, m) - A).max() <= 1e-12 * np.abs(A).max()
+        with pytest.raises(api.DugmaError):
+            api.compi_range(h, R, t, sig, 0, n + 1, 0, m)
     finally:
         api.fr_m(h)
 

@@ -68,3 +68,39 @@ def test_sharded_sum_matches_unsharded():
         assert abs(res[0] - E) <= 1e-12 * abs(E)
         assert np.allclose(res[1:], g, rtol=1e-12, atol=1e-12 * np.abs(g).max())
     assert np.array_equal(np.asarray(out[0]), np.asarray(out[1]))
+
+
+def _compi_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from oracle import oracle as orc
+    from dugma_b200 import synth
+    from dugma_b200.parallel import compi_sharded
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    P = synth.workload0(n=200)
+
+    def compute(i0, i1, j0, j1):
+        # the oracle's coefficients of this rank's source rows against all targets
+        # (a partition by source rows; the GPU path also splits the target side by rows)
+        st = orc.State(P.X[i0:i1], P.X_C[i0:i1], P.Y, P.Y_C)
+        return st.coef(P.R_G, P.t_G, 0.05)
+
+    out[rank] = list(compi_sharded(P.N, P.M, rank, world, compute, 637))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_compi_sharded_sum_matches_unsharded():
+    from oracle import oracle as orc
+    from dugma_b200 import synth
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_compi_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
+    P = synth.workload0(n=200)
+    A = np.asarray(orc.State(P.X, P.X_C, P.Y, P.Y_C).coef(P.R_G, P.t_G, 0.05))[:637]
+    for r in range(world):
+        got = np.asarray(out[r])
+        assert np.max(np.abs(got - A)) <= 1e-12 * np.max(np.abs(A))
+    assert np.array_equal(np.asarray(out[0]), np.asarray(out[1]))
