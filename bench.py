@@ -10,9 +10,9 @@ pose.  Inputs are seeded synthetic clouds of the named workload (no dataset).
 value       whole-job pair-terms/s with the clouds resident on the device (CUDA events
             around each step on the launching stream; the L2 is flushed between steps
             by writing 256 MiB, outside the timed events).
-e2e         the same metric through the C ABI with host buffers: dugma_init (FP64 host
-            clouds and covariances copied in), dugma_energy_grad (E and g copied out)
-            and dugma_fr_m per step, wall clock.
+e2e         the same metric through the C ABI with host buffers: dugma_init (FP64 clouds
+            and covariances copied in from pinned host memory), dugma_energy_grad (E and g
+            copied out) and dugma_fr_m per step, wall clock (max over ranks).
 roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instructions per
             pair x pairs per launch / launch time from CUDA events inside the library)
             against the FP32 fused-multiply-add rate measured in this run.
@@ -453,10 +453,17 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        X_C, Y_C = P.X_C, P.Y_C
-        h2d = 8 * (P.X.size + X_C.size + P.Y.size + Y_C.size)
+        # the step's inputs in pinned host memory, laid out as the C ABI takes them (the
+        # covariance arrays are views whose transpose is the contiguous MATLAB block order)
+        def pinned(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+        Xh, Yh = pinned(P.X), pinned(P.Y)
+        X_C = pinned(np.transpose(P.X_C, (0, 2, 1))).transpose(0, 2, 1)
+        Y_C = pinned(np.transpose(P.Y_C, (0, 2, 1))).transpose(0, 2, 1)
+        h2d = 8 * (Xh.size + X_C.size + Yh.size + Y_C.size)
         # warm-up of the end-to-end path
-        _, h2 = api.init(P.X, X_C, P.Y, Y_C)
+        _, h2 = api.init(Xh, X_C, Yh, Y_C)
         api.energy_grad(h2, R, t, sig, model=args.model)
         api.fr_m(h2)
         ksteps = max(3, min(args.steps, 10))
@@ -464,7 +471,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(ksteps):
             a = time.perf_counter()
-            _, h2 = api.init(P.X, X_C, P.Y, Y_C)
+            _, h2 = api.init(Xh, X_C, Yh, Y_C)
             b = time.perf_counter()
             api.energy_grad(h2, R, t, sig, model=args.model)
             c = time.perf_counter()
@@ -474,7 +481,12 @@ def main():
             ph[1] += c - b
             ph[2] += d - c
         el = time.perf_counter() - t0
-        e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "h2d_bytes_per_step": int(h2d),
+        if world > 1:
+            te = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+            el = float(te.item())
+        e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "host_memory": "pinned",
+               "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps,
                "ms_per_step": {"init": 1e3 * ph[0] / ksteps, "energy_grad": 1e3 * ph[1] / ksteps,
                                "fr_m": 1e3 * ph[2] / ksteps}}
