@@ -179,7 +179,7 @@ static void destroy_context(Context* c)
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     arena_release(c->dev, c->arena, c->arena_bytes);
-    void* bufs[] = {c->scratch_extra, c->yrec128, c->xrec128, c->mom_part, c->dedx};
+    void* bufs[] = {c->scratch_extra, c->yrec128, c->xrec128, c->yrec256, c->xrec256, c->mom_part, c->dedx};
     for (void* b : bufs)
         if (b) cudaFree(b);
     pinned_release(c->host);

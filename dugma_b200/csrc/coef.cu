@@ -120,33 +120,83 @@ __global__ void coef_prologue_kernel(const double* __restrict__ pose, const floa
     }
 }
 
-// Horner quadratic form of a packed (k-scaled, off-diagonal-doubled) matrix plus an offset
-template <int D>
-__device__ __forceinline__ float qform(const float* m, float d0, float d1, float d2, float off)
+// ---------------------------------------------------------------------------
+// Packed form: the streamed side as pair records (256 B, two points per f32x2 operation).
+// Field f (0..31) of a Rec256 is the float2 (field f of point 2p, field f of point 2p+1) of
+// the Rec128 layout read as 32 floats, with the coordinates (fields 0-2 hi, 4-6 lo) negated
+// so that d = (hi_s + f0) + (lo_s + f4) needs only packed adds; field 3 is the log2 weight,
+// 8..13 the matrix, 16.. the monomials.
+// ---------------------------------------------------------------------------
+struct __align__(16) Rec256 {
+    float4 q[16];   // q[k] = (field 2k even, field 2k odd, field 2k+1 even, field 2k+1 odd)
+};
+
+// pairs the records of both sides in one launch: pairs [0, n_pairs_a) of `in_a`, then those of `in_b`
+__global__ void pair_rec128_kernel(const Rec128* __restrict__ in_a, int n_pairs_a, Rec256* __restrict__ out_a,
+                                   const Rec128* __restrict__ in_b, int n_pairs_b, Rec256* __restrict__ out_b)
 {
-    if (D == 3) {
-        const float g0 = fmaf(m[4], d2, fmaf(m[3], d1, m[0] * d0));
-        const float g1 = fmaf(m[5], d2, m[1] * d1);
-        const float g2 = m[2] * d2;
-        return fmaf(d0, g0, fmaf(d1, g1, fmaf(d2, g2, off)));
-    } else {
-        const float g0 = fmaf(m[2], d1, m[0] * d0);
-        const float g1 = m[1] * d1;
-        return fmaf(d0, g0, fmaf(d1, g1, off));
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_pairs_a + n_pairs_b; k += gridDim.x * blockDim.x) {
+        const bool first = k < n_pairs_a;
+        const int p = first ? k : k - n_pairs_a;
+        const Rec128* in = first ? in_a : in_b;
+        Rec256* out = first ? out_a : out_b;
+        const float* a = reinterpret_cast<const float*>(in + 2 * p);
+        const float* b = reinterpret_cast<const float*>(in + 2 * p + 1);
+        Rec256 r;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            float v[4] = {a[2 * k], b[2 * k], a[2 * k + 1], b[2 * k + 1]};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int f = 2 * k + h;
+                if (f <= 2 || (f >= 4 && f <= 6)) {
+                    v[2 * h] = -v[2 * h];
+                    v[2 * h + 1] = -v[2 * h + 1];
+                }
+            }
+            r.q[k] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+        out[p] = r;
     }
 }
 
-// One body for both passes.  The stationary side keeps (pos hi, pos lo, matrix) in registers;
-// the streamed side supplies (pos hi, pos lo, matrix, log2 weight, monomials).  d = p_x - p_y' up
-// to sign (the quadratic forms do not see the sign).  H accumulates P * streamed monomials.
-template <int D, int IPT_>
-struct CoefBody {
-    using StreamRec = Rec128;
+__device__ __forceinline__ float2 fld256(const Rec256& r, int f)
+{
+    const float4 q = r.q[f >> 1];
+    return (f & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+}
+
+// packed Horner quadratic form (k-scaled, off-diagonals doubled) plus an offset
+template <int D>
+__device__ __forceinline__ float2 qform2(const float2* m, const float2* d, float2 off)
+{
+    if (D == 3) {
+        const float2 g0 = ffma2(m[4], d[2], ffma2(m[3], d[1], fmul2(m[0], d[0])));
+        const float2 g1 = ffma2(m[5], d[2], fmul2(m[1], d[1]));
+        const float2 g2 = fmul2(m[2], d[2]);
+        return ffma2(d[0], g0, ffma2(d[1], g1, ffma2(d[2], g2, off)));
+    } else {
+        const float2 g0 = ffma2(m[2], d[1], fmul2(m[0], d[0]));
+        const float2 g1 = fmul2(m[1], d[1]);
+        return ffma2(d[0], g0, ffma2(d[1], g1, off));
+    }
+}
+
+// One body for both passes.  The stationary side keeps (position hi, lo, matrix) in registers,
+// duplicated in both halves; the streamed pair record supplies two points' positions,
+// matrices, log2 weights and monomials.  H accumulates P * (streamed monomials); the sign of
+// d does not matter to the quadratic forms.
+// STREAM_LO: the streamed side carries the y' low parts (targets streamed, sources stationary);
+// otherwise the stationary side does.  The other side's low part is zero (x is FP32), so d
+// needs two packed adds per coordinate instead of three.
+template <int D, int IPT_, bool STREAM_LO>
+struct PackedCoefBody {
+    using StreamRec = Rec256;
     static constexpr int IPT = IPT_;
     static constexpr int NV = 1;
     static constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
-    float ph[IPT][D], pl[IPT][D], m[IPT][NS];
-    float h[IPT][NF];
+    float2 PH[IPT][D], PL[IPT][D], Mx[IPT][NS];   // stationary point, duplicated in both halves
+    float2 h[IPT][NF];
     double H[IPT][NF];
     int row[IPT];
     double G;
@@ -165,35 +215,45 @@ struct CoefBody {
         const float hv[3] = {r.v0.x, r.v0.y, r.v0.z}, lv[3] = {r.v1.x, r.v1.y, r.v1.z};
         const float mv[6] = {r.v2.x, r.v2.y, r.v2.z, r.v2.w, r.v3.x, r.v3.y};
 #pragma unroll
-        for (int q = 0; q < D; ++q) { ph[ii][q] = ok ? hv[q] : 0.f; pl[ii][q] = ok ? lv[q] : 0.f; }
+        for (int q = 0; q < D; ++q) {
+            const float a0 = ok ? hv[q] : 0.f, a1 = ok ? lv[q] : 0.f;
+            PH[ii][q] = make_float2(a0, a0);
+            PL[ii][q] = make_float2(a1, a1);
+        }
 #pragma unroll
-        for (int q = 0; q < NS; ++q) m[ii][q] = ok ? mv[q] : 0.f;
+        for (int q = 0; q < NS; ++q) {
+            const float v = ok ? mv[q] : 0.f;
+            Mx[ii][q] = make_float2(v, v);
+        }
     }
     __device__ void zero_all()
     {
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii)
 #pragma unroll
-            for (int q = 0; q < NF; ++q) { h[ii][q] = 0.f; H[ii][q] = 0.0; }
+            for (int q = 0; q < NF; ++q) { h[ii][q] = make_float2(0.f, 0.f); H[ii][q] = 0.0; }
     }
-    __device__ __forceinline__ void consume(const Rec128& r, int)
+    __device__ __forceinline__ void consume(const Rec256& r, int)
     {
-        const float4 v0 = r.v0, v1 = r.v1, v2 = r.v2, v3 = r.v3;
-        const float ms[6] = {v2.x, v2.y, v2.z, v2.w, v3.x, v3.y};
-        float g[NF];
+        float2 nh[3], nl[3], ms[6], g[NF];
 #pragma unroll
-        for (int q = 0; q < NF; ++q) g[q] = r.g[q];
+        for (int q = 0; q < D; ++q) { nh[q] = fld256(r, q); nl[q] = fld256(r, 4 + q); }
+        const float2 lv = fld256(r, 3);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) ms[k] = fld256(r, 8 + k);
+#pragma unroll
+        for (int q = 0; q < NF; ++q) g[q] = fld256(r, 16 + q);
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
-            // (hi_s + lo_s) - (hi_t + lo_t); hi_s - hi_t is exact for near pairs
-            const float d0 = (ph[ii][0] - v0.x) + (pl[ii][0] - v1.x);
-            const float d1 = (ph[ii][1] - v0.y) + (pl[ii][1] - v1.y);
-            const float d2 = D == 3 ? (ph[ii][2] - v0.z) + (pl[ii][2] - v1.z) : 0.f;
-            const float t1 = qform<D>(m[ii], d0, d1, d2, v0.w);
-            const float t2 = qform<D>(ms, d0, d1, d2, v0.w);
-            const float p = ex2(t1) + ex2(t2);
+            // (hi_s - hi_t) + (lo_s - lo_t); hi_s - hi_t is exact for near pairs
+            float2 d[3];
 #pragma unroll
-            for (int q = 0; q < NF; ++q) h[ii][q] = fmaf(p, g[q], h[ii][q]);
+            for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), STREAM_LO ? nl[q] : PL[ii][q]);
+            const float2 t1 = qform2<D>(Mx[ii], d, lv);
+            const float2 t2 = qform2<D>(ms, d, lv);
+            const float2 p = fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+#pragma unroll
+            for (int q = 0; q < NF; ++q) h[ii][q] = ffma2(p, g[q], h[ii][q]);
         }
     }
     __device__ void fold()
@@ -201,7 +261,10 @@ struct CoefBody {
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii)
 #pragma unroll
-            for (int q = 0; q < NF; ++q) { H[ii][q] += (double)h[ii][q]; h[ii][q] = 0.f; }
+            for (int q = 0; q < NF; ++q) {
+                H[ii][q] += (double)h[ii][q].x + (double)h[ii][q].y;
+                h[ii][q] = make_float2(0.f, 0.f);
+            }
     }
     __device__ void finish(const PairArgs& a, int jc, double (&)[NV])
     {
@@ -217,8 +280,8 @@ struct CoefBody {
     }
 };
 
-template <class Body, int NT, int TJ>
-__global__ void __launch_bounds__(NT) coef_pass_kernel(PairArgs a)
+template <class Body, int NT, int TJ, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) coef_pass_kernel(PairArgs a)
 {
     Body body;
     run_pairs<Body, NT, TJ, 4>(a, body);
@@ -351,6 +414,9 @@ int Context::ensure_coef_records()
     if (yrec128) return DUGMA_OK;
     DUGMA_CK(cudaMalloc(&yrec128, sizeof(Rec128) * (size_t)M_pad));
     DUGMA_CK(cudaMalloc(&xrec128, sizeof(Rec128) * (size_t)N_pad));
+    // the same records paired for the packed passes (Rec256: two points, same bytes)
+    DUGMA_CK(cudaMalloc(&yrec256, sizeof(Rec128) * (size_t)M_pad));
+    DUGMA_CK(cudaMalloc(&xrec256, sizeof(Rec128) * (size_t)N_pad));
     // per-block moment partials of both sides: 2 x (2 blocks per SM) x the 3D moment count
     DUGMA_CK(cudaMalloc(&mom_part, sizeof(double) * 2 * (size_t)(2 * num_sms) * kNumMoments3D));
     return DUGMA_OK;
@@ -399,15 +465,25 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
     // streamed records (128 .. 512), which bounds the per-chunk H partials the moments
     // kernel has to sum to about 8 copies of the rows' H
-    auto pass_shape = [&](int rows, KernelFn* fn) {
-        const int min_chunk = std::max(128, std::min(512, rows / 8));
-        if (rows >= 2 * 256 * c.num_sms) {
-            *fn = coef_pass_kernel<CoefBody<D, 2>, 128, 32>;
-            return KernelShape{2, 128, 32, 1, 0, min_chunk};
-        }
-        *fn = coef_pass_kernel<CoefBody<D, 1>, 64, 32>;
-        return KernelShape{1, 64, 32, 1, 0, min_chunk};
+    // (the packed passes stream pair records: min_chunk counts records of two points)
+    auto pass_shape = [&](int rows, int side, KernelFn* fn) {
+        const int min_chunk = std::max(64, std::min(256, rows / 16));
+        const bool big = rows >= 2 * 256 * c.num_sms;
+        if (big)
+            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 128, 16, 2>
+                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 128, 16, 2>;
+        else
+            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 64, 16, 4>
+                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 64, 16, 4>;
+        return big ? KernelShape{2, 128, 16, 2, 0, min_chunk} : KernelShape{2, 64, 16, 2, 0, min_chunk};
     };
+    {
+        const int np = (c.M_pad + c.N_pad) / 2;
+        const int g = std::min((np + 255) / 256, c.num_sms * 4);
+        pair_rec128_kernel<<<g, 256, 0, s>>>(c.yrec128, c.M_pad / 2, static_cast<Rec256*>(c.yrec256), c.xrec128,
+                                             c.N_pad / 2, static_cast<Rec256*>(c.xrec256));
+        DUGMA_CK(cudaGetLastError());
+    }
     // blocks of the moments kernel: about 32 rows each, at most 2 per SM (the partial buffer's size)
     const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(i1 - i0, j1 - j0) + 31) / 32));
     double* mom = c.mom_part;
@@ -418,16 +494,16 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         double* hp = nullptr;
         int n_jc = 0;
         const Rec128* src = side == 0 ? c.xrec128 : c.yrec128;
-        const Rec128* str = side == 0 ? c.yrec128 : c.xrec128;
+        const void* str = side == 0 ? c.yrec256 : c.xrec256;
         const int r0 = side == 0 ? i0 : j0, r1 = side == 0 ? i1 : j1, rows = r1 - r0;
         if (rows <= 0) continue;   // an empty range contributes nothing
-        const size_t nstr = side == 0 ? (size_t)c.M_pad : (size_t)c.N_pad;
+        const size_t nstr = (side == 0 ? (size_t)c.M_pad : (size_t)c.N_pad) / 2;
         const double Lmax = side == 0 ? c.Lmax_y : c.Lmax_x;
         // launch_pair_variant reads the stationary weights from c.wx; swap for the target pass
         float* wsave = c.wx;
         if (side == 1) c.wx = c.wy;
         KernelFn fn;
-        const KernelShape sh = pass_shape(rows, &fn);
+        const KernelShape sh = pass_shape(rows, side, &fn);
         rc = launch_pair_variant(c, fn, sh, src, str, nstr, 1, Lmax, pose_dev, r0, r1, nullptr, nullptr, &hp, 16,
                                  &n_jc, s);
         c.wx = wsave;

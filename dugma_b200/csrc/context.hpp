@@ -57,6 +57,8 @@ struct Context {
     XRec* xrec = nullptr;
     Rec128* yrec128 = nullptr;
     Rec128* xrec128 = nullptr;
+    void* yrec256 = nullptr;                  // the 128-byte records paired (coefficient passes)
+    void* xrec256 = nullptr;
     float4* yp32 = nullptr;                   // float(y') for nearest neighbours
     float* dmin = nullptr;                    // nearest squared distance per source (sigma)
     double* pose = nullptr;                   // kPoseDoubles

@@ -91,6 +91,7 @@ static const std::vector<Variant>& adjoint_variants()
         {{1, 256, 32, 2, 512}, pair_kernel<PackedBody<D, 1, true>, 256, 32>},
         {{2, 96, 32, 2, 512}, pair_kernel_occ<PackedBody<D, 2, true>, 96, 32, 5>},
         {{2, 128, 64, 2, 512}, pair_kernel_occ<PackedBody<D, 2, true>, 128, 64, 4>},
+        {{4, 64, 64, 2, 512}, pair_kernel_occ<PackedBody<D, 4, true>, 64, 64, 4>},
     };
     return v;
 }
