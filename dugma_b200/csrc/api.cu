@@ -308,7 +308,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     c->N_pad = (N + kPadI - 1) / kPadI * kPadI;
     c->M_pad = (M + kPadJ - 1) / kPadJ * kPadJ;
     // packed f32x2 pair kernels by default (fastest on B200 in every tuning run so far)
-    c->shape_adj = {2, 128, 64, 2, 512};
+    c->shape_adj = {4, 64, 64, 2, 512};
     c->shape_energy = {4, 128, 32, 2};
     c->shape_nn = {4, 128, 128};
     c->shape_conv_adj = {1, 64, 32, 2, 512};
