@@ -341,7 +341,7 @@ def main():
     else:
         kind = 0 if args.model == 0 else 3     # REF or CONV adjoint shapes
         tune = "" if args.no_tune else api.autotune(h, kind)
-        shape_key = api.shapes(kind)[0]
+        shape_key = api.get_shape(h, kind)
         if tune:
             import re
             best = min(re.findall(r"\(ipt=(\d+),nt=(\d+),tj=(\d+),pack=(\d+)\):([0-9.]+)ms", tune), key=lambda m: float(m[4]))

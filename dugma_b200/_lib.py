@@ -55,6 +55,7 @@ EXPORTS = {
     "dugma_minimise_surrogate": (c_int, [c_int, dp, dp, dp, dp, ip]),
     "dugma_energy_grad_noalloc": (c_int, [c_void_p] * 6 + [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "dugma_set_shape": (c_int, [PtrArray, c_int, c_int, c_int, c_int, c_int]),
+    "dugma_get_shape": (c_int, [PtrArray, c_int, ip]),
     "dugma_calibrate": (c_int, [c_int, dp, dp]),
 }
 

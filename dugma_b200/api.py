@@ -199,6 +199,13 @@ def shapes(what=0):
     return [tuple(buf[4 * k:4 * k + 4]) for k in range(n)]
 
 
+def get_shape(h: Handles, what) -> tuple:
+    """The kernel shape (ipt, nt, tj, pack) this context uses for `what`."""
+    buf = (ctypes.c_int * 4)()
+    check(_lib.load().dugma_get_shape(h.arr, int(what), buf))
+    return tuple(buf)
+
+
 def set_shape(h: Handles, what, shape):
     check(_lib.load().dugma_set_shape(h.arr, int(what), *[int(v) for v in shape]))
 

@@ -310,7 +310,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     // packed f32x2 pair kernels by default (fastest on B200 in every tuning run so far)
     c->shape_adj = {4, 64, 64, 2, 512};
     c->shape_energy = {4, 128, 32, 2};
-    c->shape_nn = {4, 128, 128};
+    c->shape_nn = {4, 128, 64};
     c->shape_conv_adj = {1, 64, 32, 2, 512};
     c->shape_conv_energy = {1, 128, 32, 2};
     int rc = DUGMA_OK;
@@ -679,6 +679,18 @@ int dugma_shapes(int what, int* shapes, int max)
         shapes[4 * k + 3] = cand[k].pack;
     }
     return n;
+}
+
+int dugma_get_shape(float* Ptr[6], int what, int shape[4])
+{
+    GET_CTX(c, Ptr);
+    if (what < 0 || what > 4 || !shape) return set_error(DUGMA_ERR_ARG, "get_shape: what must be 0 .. 4");
+    const KernelShape& k = shape_slot(*c, what);
+    shape[0] = k.ipt;
+    shape[1] = k.nt;
+    shape[2] = k.tj;
+    shape[3] = k.pack;
+    return DUGMA_OK;
 }
 
 int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack)

@@ -59,7 +59,7 @@ struct Context {
     Rec128* xrec128 = nullptr;
     void* yrec256 = nullptr;                  // the 128-byte records paired (coefficient passes)
     void* xrec256 = nullptr;
-    float4* yp32 = nullptr;                   // float(y') for nearest neighbours
+    float4* yp32 = nullptr;                   // -float(y') for nearest neighbours, pair-interleaved
     float* dmin = nullptr;                    // nearest squared distance per source (sigma)
     double* pose = nullptr;                   // kPoseDoubles
     double* out = nullptr;                    // 64 doubles of results

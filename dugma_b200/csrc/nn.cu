@@ -5,6 +5,8 @@
 // (update_sig.cu:181-269, 272-315, 384-385).  Here:
 //   y'_j = float(FP64(R y_j + t))               (update_sig.cu:247-252, written by the prologue)
 //   d    = x_i - y'_j in FP32,  d2 = fmaf(dz,dz, fmaf(dy,dy, dx*dx))
+// Target records hold two targets each, coordinates negated (d = x + (-y') is the same FP32
+// value), interleaved so that the sigma kernel evaluates both with f32x2 operations.
 //   the k smallest (d2, j) in lexicographic order are kept in registers (ties -> lowest j)
 // Targets are streamed by bulk copy like the energy kernels; target chunks are merged in
 // index order afterwards, so the result is exact and deterministic.  sigma is then
@@ -17,9 +19,14 @@
 
 namespace dugma {
 
+// two nearest-neighbour targets (see the prologue): a = (-y0, -y0', -y1, -y1'), b = (-y2, -y2', 0, 0)
+struct __align__(16) NNRec2 {
+    float4 a, b;
+};
+
 template <int D, int IPT_, int K>
 struct NNBody {
-    using StreamRec = float4;
+    using StreamRec = NNRec2;
     static constexpr int IPT = IPT_;
     static constexpr int NV = 1;
     float x[IPT][D];
@@ -42,14 +49,19 @@ struct NNBody {
 #pragma unroll
             for (int q = 0; q < K; ++q) { bd[ii][q] = INFINITY; bi[ii][q] = 0x7fffffff; }
     }
-    __device__ __forceinline__ void consume(const float4& y, int j)
+    __device__ __forceinline__ void consume(const NNRec2& r, int jp)
+    {
+        one(r.a.x, r.a.z, r.b.x, 2 * jp);       // targets in index order: ties keep the lower j
+        one(r.a.y, r.a.w, r.b.y, 2 * jp + 1);
+    }
+    __device__ __forceinline__ void one(float n0, float n1, float n2, int j)
     {
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
-            const float d0 = x[ii][0] - y.x, d1 = x[ii][1] - y.y;
+            const float d0 = x[ii][0] + n0, d1 = x[ii][1] + n1;
             float dd;
             if (D == 3) {
-                const float d2 = x[ii][2] - y.z;
+                const float d2 = x[ii][2] + n2;
                 dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
             } else {
                 dd = fmaf(d1, d1, d0 * d0);
@@ -81,6 +93,63 @@ struct NNBody {
             float2* o = out + ((size_t)jc * rows + (row[ii] - a.i0)) * K;
 #pragma unroll
             for (int q = 0; q < K; ++q) o[q] = make_float2(bd[ii][q], __int_as_float(bi[ii][q]));
+        }
+    }
+};
+
+// Nearest squared distance only (sigma): both targets of a record in one f32x2 sequence, the
+// same FP32 operations as NNBody, a running minimum per half.
+template <int D, int IPT_>
+struct NNMinBody {
+    using StreamRec = NNRec2;
+    static constexpr int IPT = IPT_;
+    static constexpr int NV = 1;
+    float2 X[IPT][D];
+    float2 bd[IPT];
+    int row[IPT];
+
+    __device__ void setup(const PairArgs&) {}
+    __device__ void load_src(const PairArgs& a, int ii, int i)
+    {
+        const float* xs = static_cast<const float*>(a.xrec);
+        row[ii] = i < a.i_end ? i : -1;
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            const float v = i < a.i_end ? xs[(size_t)i * D + q] : 0.f;
+            X[ii][q] = make_float2(v, v);
+        }
+    }
+    __device__ void zero_all()
+    {
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) bd[ii] = make_float2(INFINITY, INFINITY);
+    }
+    __device__ __forceinline__ void consume(const NNRec2& r, int)
+    {
+        const float2 n0 = make_float2(r.a.x, r.a.y), n1 = make_float2(r.a.z, r.a.w), n2 = make_float2(r.b.x, r.b.y);
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            const float2 d0 = fadd2(X[ii][0], n0), d1 = fadd2(X[ii][1], n1);
+            float2 dd;
+            if (D == 3) {
+                const float2 d2 = fadd2(X[ii][2], n2);
+                dd = ffma2(d2, d2, ffma2(d1, d1, fmul2(d0, d0)));
+            } else {
+                dd = ffma2(d1, d1, fmul2(d0, d0));
+            }
+            bd[ii].x = fminf(bd[ii].x, dd.x);
+            bd[ii].y = fminf(bd[ii].y, dd.y);
+        }
+    }
+    __device__ void fold() {}
+    __device__ void finish(const PairArgs& a, int jc, double (&)[NV])
+    {
+        const int rows = a.i_end - a.i0;
+        float2* out = reinterpret_cast<float2*>(a.h_part);
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            out[(size_t)jc * rows + (row[ii] - a.i0)] = make_float2(fminf(bd[ii].x, bd[ii].y), __int_as_float(0));
         }
     }
 };
@@ -120,18 +189,49 @@ __global__ void nn_merge_kernel(const float2* __restrict__ part, int n_jc, int r
     }
 }
 
-// sigma sums over the nearest squared distances (single block, fixed order)
-__global__ void sigma_kernel(const float* __restrict__ dmin, int n, int D, double* __restrict__ out)
+// sigma sums over the nearest squared distances: per-block partials over contiguous slices
+// (fixed order), then one block over the partials (fixed order), so the result is deterministic
+__global__ void sigma_partial_kernel(const float* __restrict__ dmin, int n, int D, double* __restrict__ pe,
+                                     unsigned long long* __restrict__ pq)
+{
+    __shared__ double s_exact[256];
+    __shared__ unsigned long long s_q[256];
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    double se = 0;
+    unsigned long long sq = 0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const float v = dmin[i];
+        se += (double)v;
+        const float sv = __fmul_rn(__fdiv_rn(v, (float)D), 1000000.0f);
+        sq += (unsigned long long)__float2uint_rn(sv);
+    }
+    s_exact[threadIdx.x] = se;
+    s_q[threadIdx.x] = sq;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            s_exact[threadIdx.x] += s_exact[threadIdx.x + h];
+            s_q[threadIdx.x] += s_q[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        pe[blockIdx.x] = s_exact[0];
+        pq[blockIdx.x] = s_q[0];
+    }
+}
+
+__global__ void sigma_final_kernel(const double* __restrict__ pe, const unsigned long long* __restrict__ pq, int nb,
+                                   int n, int D, double* __restrict__ out)
 {
     __shared__ double s_exact[256];
     __shared__ unsigned long long s_q[256];
     double se = 0;
     unsigned long long sq = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const float v = dmin[i];
-        se += (double)v;
-        const float sv = __fmul_rn(__fdiv_rn(v, (float)D), 1000000.0f);
-        sq += (unsigned long long)__float2uint_rn(sv);
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        se += pe[i];
+        sq += pq[i];
     }
     s_exact[threadIdx.x] = se;
     s_q[threadIdx.x] = sq;
@@ -163,20 +263,20 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
                         cudaStream_t s);
 
 struct NNVariant {
-    KernelShape shape;
-    KernelFn k1, k8, k16;
+    KernelShape shape;           // tj counts records of two targets
+    KernelFn k1, k8, k16, kmin;  // kmin: nearest distance only (sigma)
 };
 
 template <int D>
 static const std::vector<NNVariant>& nn_variants()
 {
     static const std::vector<NNVariant> v = {
-        {{4, 128, 128}, nn_kernel<NNBody<D, 4, 1>, 128, 128>, nn_kernel<NNBody<D, 4, 8>, 128, 128>,
-         nn_kernel<NNBody<D, 2, 16>, 128, 128>},
-        {{8, 128, 128}, nn_kernel<NNBody<D, 8, 1>, 128, 128>, nn_kernel<NNBody<D, 4, 8>, 128, 128>,
-         nn_kernel<NNBody<D, 2, 16>, 128, 128>},
-        {{4, 256, 128}, nn_kernel<NNBody<D, 4, 1>, 256, 128>, nn_kernel<NNBody<D, 2, 8>, 256, 128>,
-         nn_kernel<NNBody<D, 1, 16>, 256, 128>},
+        {{4, 128, 64}, nn_kernel<NNBody<D, 4, 1>, 128, 64>, nn_kernel<NNBody<D, 4, 8>, 128, 64>,
+         nn_kernel<NNBody<D, 2, 16>, 128, 64>, nn_kernel<NNMinBody<D, 4>, 128, 64>},
+        {{8, 128, 64}, nn_kernel<NNBody<D, 8, 1>, 128, 64>, nn_kernel<NNBody<D, 4, 8>, 128, 64>,
+         nn_kernel<NNBody<D, 2, 16>, 128, 64>, nn_kernel<NNMinBody<D, 8>, 128, 64>},
+        {{4, 256, 64}, nn_kernel<NNBody<D, 4, 1>, 256, 64>, nn_kernel<NNBody<D, 2, 8>, 256, 64>,
+         nn_kernel<NNBody<D, 1, 16>, 256, 64>, nn_kernel<NNMinBody<D, 4>, 256, 64>},
     };
     return v;
 }
@@ -199,14 +299,16 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     for (auto& cand : vars)
         if (cand.shape.ipt == want.ipt && cand.shape.nt == want.nt && cand.shape.tj == want.tj) v = &cand;
     const int K = k <= 1 ? 1 : (k <= 8 ? 8 : 16);
-    KernelFn fn = K == 1 ? v->k1 : (K == 8 ? v->k8 : v->k16);
+    // only the nearest distance wanted (sigma): the packed distance-only kernel
+    const bool min_only = K == 1 && !idx_dev && !d2_dev;
+    KernelFn fn = min_only ? v->kmin : (K == 1 ? v->k1 : (K == 8 ? v->k8 : v->k16));
     KernelShape sh = v->shape;
     // the k = 8 / 16 kernels keep fewer sources per thread (see the variant table)
     if (K == 8) sh.ipt = sh.nt == 128 ? 4 : 2;
     if (K == 16) sh.ipt = sh.nt == 128 ? 2 : 1;
     double* hp = nullptr;
     int n_jc = 0;
-    DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad, 1, 0.0, pose_dev, 0, c.N, nullptr,
+    DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad / 2, 1, 0.0, pose_dev, 0, c.N, nullptr,
                                   nullptr, &hp, K, &n_jc, s));
     const int g = std::min((c.N + 255) / 256, c.num_sms * 8);
     const float2* part = reinterpret_cast<const float2*>(hp);
@@ -230,7 +332,13 @@ int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2
 int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s)
 {
     DUGMA_RET(nn_run(c, pose_dev, 1, nullptr, nullptr, c.dmin, s, nullptr));
-    sigma_kernel<<<1, 256, 0, s>>>(c.dmin, c.N, c.D, out_dev);
+    // partials in the scratch region (the search's chunk lists there are merged by now, in stream order)
+    const int nb = std::max(1, std::min(2 * c.num_sms, (c.N + 1023) / 1024));
+    DUGMA_RET(c.ensure_scratch(sizeof(double) * 2 * (size_t)nb));
+    double* pe = c.scratch;
+    unsigned long long* pq = reinterpret_cast<unsigned long long*>(c.scratch + nb);
+    sigma_partial_kernel<<<nb, 256, 0, s>>>(c.dmin, c.N, c.D, pe, pq);
+    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, c.N, c.D, out_dev);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }

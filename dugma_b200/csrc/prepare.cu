@@ -258,10 +258,15 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
             }
             yrec[j] = r;
         }
-        // padding targets sit at +inf so that no source ever picks them as a neighbour
-        if (yp32)
-            yp32[j] = j < M ? make_float4(hi[0], hi[1], hi[2], 0.f)
-                            : make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        // nearest-neighbour records, two targets per 32 bytes with negated coordinates:
+        // (-y0 2p, -y0 2p+1, -y1 2p, -y1 2p+1), (-y2 2p, -y2 2p+1, 0, 0); padding targets sit
+        // at +inf so that no source ever picks them as a neighbour
+        if (yp32) {
+            float* pr = reinterpret_cast<float*>(yp32 + 2 * (j / 2));
+            const int h = j & 1;
+            for (int q = 0; q < 3; ++q) pr[2 * q + h] = j < M ? (q < D ? -hi[q] : 0.f) : -INFINITY;
+            pr[6 + h] = 0.f;
+        }
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
         XRec r;

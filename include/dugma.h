@@ -160,6 +160,9 @@ int dugma_shapes(int what, int* shapes, int max);
 /* Pins the kernel shape used for `what` on this context (one of dugma_shapes' tuples). */
 int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack);
 
+/* The kernel shape this context uses for `what`: shape[0..4) = {ipt, nt, tj, pack}. */
+int dugma_get_shape(float* Ptr[6], int what, int shape[4]);
+
 /* Captures one energy+gradient evaluation (prologue, pair kernel, reduction) as a CUDA graph
  * reading its pose from the context's pose buffer; dugma_graph_eval replays it for a new
  * pose and returns E and g. */
