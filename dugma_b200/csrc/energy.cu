@@ -377,6 +377,3 @@ extern "C" int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv,
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
-
-namespace dugma {
-}  // namespace dugma
