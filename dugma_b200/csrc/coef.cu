@@ -401,11 +401,6 @@ __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, cons
     if (lane == 0) out[mi] = v;
 }
 
-using KernelFn = void (*)(PairArgs);
-int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
-                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
-                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s);
 
 int num_moments(int D) { return D == 3 ? kNumMoments3D : kNumMoments2D; }
 
@@ -499,14 +494,11 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         if (rows <= 0) continue;   // an empty range contributes nothing
         const size_t nstr = (side == 0 ? (size_t)c.M_pad : (size_t)c.N_pad) / 2;
         const double Lmax = side == 0 ? c.Lmax_y : c.Lmax_x;
-        // launch_pair_variant reads the stationary weights from c.wx; swap for the target pass
-        float* wsave = c.wx;
-        if (side == 1) c.wx = c.wy;
         KernelFn fn;
         const KernelShape sh = pass_shape(rows, side, &fn);
+        // the stationary weights: sources in pass A, targets in pass B
         rc = launch_pair_variant(c, fn, sh, src, str, nstr, 1, Lmax, pose_dev, r0, r1, nullptr, nullptr, &hp, 16,
-                                 &n_jc, s);
-        c.wx = wsave;
+                                 &n_jc, s, side == 1 ? c.wy : nullptr);
         if (rc != DUGMA_OK) break;
         const int nb = std::min(nblk, rows);
         nb_side[side] = nb;

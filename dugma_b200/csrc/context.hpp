@@ -116,6 +116,18 @@ const char* last_error();
     } while (0)
 
 // ---- kernel launchers (energy.cu, nn.cu, coef.cu) ----
+struct PairArgs;
+using KernelFn = void (*)(PairArgs);
+// One persistent all-pairs launch of `fn` (a run_pairs kernel of shape `sh`): source rows
+// [i0, i1) of the stationary records `xrec` against `yrec_size` streamed records `yrec`,
+// then, if out_dev, the fixed-order sum of the nv per-item partials into out_dev, and, if
+// dEdx_dev, the per-row sums over target chunks.  h_part (nullable) receives the per-chunk
+// row buffer of h_width doubles per row, n_jc_out the chunk count.  The stationary side's
+// weights are c.wx unless w_stationary is given (the coefficient pass over targets).
+int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
+                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
+                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
+                        cudaStream_t s, const float* w_stationary = nullptr);
 // Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy), x records.
 int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s);
 // Pairwise energy (grad = false) or fused adjoint (grad = true) over source rows [i0, i1);

@@ -665,7 +665,6 @@ __global__ void __launch_bounds__(NT, MINB) conv_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
-using KernelFn = void (*)(PairArgs);
 
 struct ConvVariant {
     KernelShape shape;
@@ -702,10 +701,6 @@ std::vector<KernelShape> conv_shapes(bool grad)
     for (auto& v : conv_variants<3>(grad)) s.push_back(v.shape);
     return s;
 }
-int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
-                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
-                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s);
 
 int conv_launch(Context& c, const double* pose_dev, bool grad, int i0, int i1, double* out_dev, double* dEdx_dev,
                 cudaStream_t s, const KernelShape* force)

@@ -69,7 +69,6 @@ __global__ void reduce_chunks_kernel(const double* __restrict__ part, int n_jc, 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-using KernelFn = void (*)(PairArgs);
 
 struct Variant {
     KernelShape shape;
@@ -144,7 +143,7 @@ static int occupancy_blocks(KernelFn fn, int nt)
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s)
+                        cudaStream_t s, const float* w_stationary)
 {
     const int rows = i1 - i0;
     const int BI = sh.ipt * sh.nt;
@@ -168,7 +167,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     PairArgs a{};
     a.xrec = xrec;
     a.yrec = yrec;
-    a.wx = c.wx;
+    a.wx = w_stationary ? w_stationary : c.wx;
     a.wy = c.wy;
     a.xcov = c.xcov;
     a.ycov = c.ycov;

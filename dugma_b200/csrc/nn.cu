@@ -256,11 +256,6 @@ __global__ void __launch_bounds__(NT) nn_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
-using KernelFn = void (*)(PairArgs);
-int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
-                        size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
-                        double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s);
 
 struct NNVariant {
     KernelShape shape;           // tj counts records of two targets
