@@ -344,6 +344,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
         {(void**)&c->yrec, sizeof(YRec) * c->M_pad},    {(void**)&c->xrec, sizeof(XRec) * c->N_pad},
         {(void**)&c->yp32, sizeof(float4) * c->M_pad},  {(void**)&c->dmin, sizeof(float) * N},
         {(void**)&c->pose, sizeof(double) * kPoseDoubles * 2}, {(void**)&c->out, sizeof(double) * 64},
+        {(void**)&c->poses, sizeof(double) * kPoseDoubles * kMaxPoses},
         {(void**)&c->err, sizeof(int) * 4},             {(void**)&c->counter, sizeof(int) * 8},
         {(void**)&c->mom, sizeof(double) * 512},        {(void**)&c->arena_scratch, scratch_bytes},
     };
@@ -522,8 +523,7 @@ int dugma_energy_fd_grad(float* Ptr[6], const double* R, const double* t, double
         }
         pack_pose(*c, R2, t2, sig, hp + 16 * k);
     }
-    double* poses = nullptr;
-    DUGMA_CK(cudaMallocAsync(&poses, sizeof(double) * 16 * nev, c->stream));
+    double* poses = c->poses;   // nev <= 13 <= kMaxPoses
     DUGMA_CK(cudaMemcpyAsync(poses, hp, sizeof(double) * 16 * nev, cudaMemcpyHostToDevice, c->stream));
     DUGMA_CK(cudaMemsetAsync(c->err, 0, sizeof(int), c->stream));
     int rc = DUGMA_OK;
@@ -531,7 +531,6 @@ int dugma_energy_fd_grad(float* Ptr[6], const double* R, const double* t, double
         rc = launch_pairs(*c, poses + 16 * k, model, false, 0, c->N, c->out + k, nullptr, c->stream);
     double ev[16];
     if (rc == DUGMA_OK) rc = fetch(*c, c->out, nev, ev);
-    cudaFreeAsync(poses, c->stream);
     cudaStreamSynchronize(c->stream);
     if (rc != DUGMA_OK) return rc;
     *E = ev[0];

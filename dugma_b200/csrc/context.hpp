@@ -22,6 +22,7 @@ namespace dugma {
 
 // Pose block on the device: R (D x D col-major, zero padded to 9), t (3), sig, pad.
 constexpr int kPoseDoubles = 16;
+constexpr int kMaxPoses = 16;     // device pose slots of a context (the finite-difference stencil)
 constexpr int kPoseT = 9;
 constexpr int kPoseSig = 12;
 
@@ -62,6 +63,7 @@ struct Context {
     float4* yp32 = nullptr;                   // -float(y') for nearest neighbours, pair-interleaved
     float* dmin = nullptr;                    // nearest squared distance per source (sigma)
     double* pose = nullptr;                   // kPoseDoubles
+    double* poses = nullptr;                  // kMaxPoses x kPoseDoubles
     double* out = nullptr;                    // 64 doubles of results
     int* err = nullptr;                       // device error word
     int* counter = nullptr;                   // work-queue counters (8)
