@@ -382,8 +382,8 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                else f"/tmp/clocks_rank{rank}.csv", local) as clk:
+    import tempfile
+    with Clocks(os.path.join(tempfile.gettempdir(), f"dugma_clocks_rank{rank}.csv"), local) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
