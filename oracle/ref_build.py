@@ -1,11 +1,12 @@
-"""Build the reference's CUDA plugins from their sources into oracle/_ref (checker only).
+"""Build the reference's CUDA plugins from their sources into oracle/_ref (test infrastructure only).
 
 Each of init.cu, update_sig.cu, compi.cu is compiled unmodified from the reference
 tree, with the flags of its compile.m (-use_fast_math -maxrregcount=50 -O3) but for
 sm_100a, into its own shared object (they define the same helper symbols):
     oracle/_ref/libref_init.so, libref_update_sig.so, libref_compi.so
-The outputs travel to the GPU box with the repository snapshot; this recipe only runs
-where the reference sources exist.  Nothing here is part of the product library.
+The built objects are kept with the repository's other build outputs, so that machines
+without the reference sources can still load them; this recipe only runs where the
+reference sources exist.  Nothing here is part of the product library.
 """
 from __future__ import annotations
 
