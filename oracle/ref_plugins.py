@@ -1,7 +1,7 @@
 """ctypes harness for the reference's own CUDA plugins built by oracle/ref_build.py.
 
-CHECKER ONLY: used by tests/golden/make_golden.py (run on a GPU) to record the
-reference's outputs, and by bench.py to time the reference kernels on the same box.
+Test infrastructure only: used by tests/golden/make_golden.py (run on a GPU) to record the
+reference's outputs, and by bench.py to time the reference kernels on the same GPU.
 It calls the reference's C++ entry points by their mangled names, exactly as the MEX
 gateways do (init.cpp:65, update_sig.cpp:45, compi.cpp:45).  fr_m is never called:
 it ends with cudaDeviceReset (fr_m.cu:27), which would tear down the caller's context.
