@@ -13,7 +13,8 @@
 // gradient of Q (from the monomial exponents) and a Hessian by central differences of
 // that gradient, with backtracking.
 // Direct mode (DUGMA_DRIVE_DIRECT): maximise E(R, t) at the current sig with BFGS on the
-// left-perturbation coordinates using the fused adjoint's gradient, then update sig.
+// left-perturbation coordinates using the fused adjoint's gradient, then update sig; every
+// evaluation replays one captured CUDA graph (pose prologue, adjoint, reduction).
 // Both modes normalise the clouds first (normalize.m:3-26) and denormalise the
 // translation at the end (DUGMA.m:122).
 #include <algorithm>
@@ -354,6 +355,15 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
     int evals = 0;
     rc = dugma_update_sig(Ptr, R, t, &Nd, &Md, &Dd, &sigf);
     double sig = sigf;
+    // direct mode: one captured CUDA graph (pose prologue, fused adjoint, reduction) replayed
+    // for every evaluation; without it (capture refused) the eager launches run instead
+    void* graph = nullptr;
+    if (rc == DUGMA_OK && mode == DUGMA_DRIVE_DIRECT && dugma_graph_create(Ptr, DUGMA_MODEL_REF, &graph) != DUGMA_OK)
+        graph = nullptr;
+    auto eval = [&](const double* Rx, const double* tx, double* Ex, double* gx) {
+        return graph ? dugma_graph_eval(graph, Rx, tx, sig, Ex, gx)
+                     : dugma_energy_grad(Ptr, Rx, tx, sig, DUGMA_MODEL_REF, Ex, gx, nullptr);
+    };
     const int NR = D == 3 ? 3 : 1;
     double angle[3] = {1e4, 1e4, 1e4}, angle0[3];
     double tprev[3] = {t[0], t[1], t[2]};
@@ -393,7 +403,7 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
             // BFGS ascent of E on the left-perturbation coordinates at fixed sig
             const int n = NR + D;
             double g[6];
-            rc = dugma_energy_grad(Ptr, R, t, sig, DUGMA_MODEL_REF, &E, g, nullptr);
+            rc = eval(R, t, &E, g);
             ++evals;
             if (rc != DUGMA_OK) break;
             std::vector<double> Hi(n * n, 0.0);
@@ -428,7 +438,7 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
                         Rn[3] = sn * Rc[2] + c * Rc[3];
                     }
                     for (int a = 0; a < D; ++a) tn[a] = tc[a] + alpha * s[NR + a];
-                    rc = dugma_energy_grad(Ptr, Rn, tn, sig, DUGMA_MODEL_REF, &En, gnew, nullptr);
+                    rc = eval(Rn, tn, &En, gnew);
                     ++evals;
                     if (rc != DUGMA_OK) break;
                     double dir = 0;
@@ -516,6 +526,7 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
         double gtmp[6];
         dugma_energy_grad(Ptr, R, t, sig, DUGMA_MODEL_REF, &E, gtmp, nullptr);
     }
+    if (graph) dugma_graph_destroy(graph);
     dugma_fr_m(Ptr);
     if (rc != DUGMA_OK) return rc;
     if (exitflag < 0) {   // DUGMA.m:116-118: an unsolvable surrogate returns the identity
