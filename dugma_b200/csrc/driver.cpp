@@ -84,35 +84,60 @@ void rotm2eul(const Mat3& R, double e[3])
     }
 }
 
-// Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq and its gradient in v.
+// The surrogate's monomials as lists of at most 4 variable indices (a variable appears once
+// per unit of its exponent; -1 pads), built once per dimension from the exponent tables.
+struct Mono {
+    signed char f[4];
+};
+
+const std::vector<Mono>& mono_table(int D)
+{
+    auto build = [](const unsigned char* E, int K, int nv) {
+        std::vector<Mono> t(K);
+        for (int k = 0; k < K; ++k) {
+            int n = 0;
+            for (int q = 0; q < 4; ++q) t[k].f[q] = -1;
+            for (int q = 0; q < nv; ++q)
+                for (int e = 0; e < E[k * nv + q] && n < 4; ++e) t[k].f[n++] = (signed char)q;
+        }
+        return t;
+    };
+    static const std::vector<Mono> t3 = build(&dugma::kMonoExp3D[0][0], 637, 12);
+    static const std::vector<Mono> t2 = build(&dugma::kMonoExp2D[0][0], 45, 4);
+    return D == 3 ? t3 : t2;
+}
+
+// Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq and its gradient in v (product rule over the
+// factor list: a factor repeated e times contributes e v^(e-1) times the rest).
 struct Surrogate {
     int D, K, nv;
     const double* A;
     const unsigned char* E;
     double value(const double* v) const
     {
+        const std::vector<Mono>& T = mono_table(D);
         double s = 0;
         for (int k = 0; k < K; ++k) {
             double m = A[k];
-            for (int q = 0; q < nv; ++q)
-                for (int e = 0; e < E[k * nv + q]; ++e) m *= v[q];
+            for (int j = 0; j < 4 && T[k].f[j] >= 0; ++j) m *= v[T[k].f[j]];
             s += m;
         }
         return s;
     }
     void grad(const double* v, double* g) const
     {
+        const std::vector<Mono>& T = mono_table(D);
         for (int q = 0; q < nv; ++q) g[q] = 0;
         for (int k = 0; k < K; ++k) {
-            for (int q = 0; q < nv; ++q) {
-                const int eq = E[k * nv + q];
-                if (!eq) continue;
-                double m = A[k] * eq;
-                for (int p = 0; p < nv; ++p) {
-                    const int ep = E[k * nv + p] - (p == q ? 1 : 0);
-                    for (int e = 0; e < ep; ++e) m *= v[p];
-                }
-                g[q] += m;
+            const signed char* f = T[k].f;
+            int n = 0;
+            double x[4];
+            for (; n < 4 && f[n] >= 0; ++n) x[n] = v[f[n]];
+            for (int j = 0; j < n; ++j) {
+                double m = A[k];
+                for (int l = 0; l < n; ++l)
+                    if (l != j) m *= x[l];
+                g[f[j]] += m;
             }
         }
     }
