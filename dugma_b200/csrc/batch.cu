@@ -21,7 +21,7 @@
 
 namespace dugma {
 
-constexpr int kBatchNT = 128, kBatchTJ = 32, kBatchIPT = 2, kBatchChunk = 512;   // chunk in pair records
+constexpr int kBatchNT = 64, kBatchTJ = 64, kBatchIPT = 4, kBatchChunk = 512;   // chunk in pair records
 
 struct PQDesc {
     const float *x, *xinv, *lwx, *y, *yinv, *lwy, *wx;
