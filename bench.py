@@ -78,6 +78,36 @@ def dist_setup(n):
     return rank, world, local
 
 
+def dist_init(world, local):
+    """This rank's device (local rank, wrapped over the visible devices) and, for world > 1, the
+    process group: NCCL, or the backend named by DUGMA_DIST_BACKEND (gloo runs several ranks'
+    host-side plumbing on fewer GPUs; each rank's kernels are independent)."""
+    import datetime
+    import torch
+    dev = local % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = os.environ.get("DUGMA_DIST_BACKEND", "nccl")
+        kw = {"device_id": torch.device("cuda", dev)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+    return dev
+
+
+def all_reduce(values, op):
+    """All-reduce a few host floats over the ranks (op "sum" or "max"); identity when alone."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64)
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def workload(wl, n=0):
     from dugma_b200 import synth
     return synth.WORKLOADS[wl](n=n) if n else synth.WORKLOADS[wl]()
@@ -167,6 +197,7 @@ class Clocks:
 def cpu_rate(P, R, t, sig, budget_s=8.0):
     """Oracle (FP64, OpenMP, all host threads) pair-terms/s on a bounded sample of source rows."""
     from oracle import oracle as orc
+    orc.use_all_cores()
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
     rows = 64
     done = 0
@@ -188,18 +219,20 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from oracle import oracle as orc
+    orc.use_all_cores()
     P = workload(args.workload, args.n)
     R, t = eval_pose(P, 0)
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
     _, d2 = st.nn(R, t, 1)
     sig = float(np.mean(d2) / 3.0)
-    rows = 256
+    rows = min(2048, st.N)
+    fn = st.energy_conv if args.model == 1 else st.energy
     for _ in range(args.warmup):
-        st.energy(R, t, sig, i0=0, i1=rows)
+        fn(R, t, sig, i0=0, i1=rows)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        i0 = (k * rows) % (st.N - rows)
-        st.energy(R, t, sig, i0=i0, i1=i0 + rows)
+        i0 = (k * rows) % (st.N - rows + 1)
+        fn(R, t, sig, i0=i0, i1=i0 + rows)
     el = time.perf_counter() - t0
     val = args.steps * rows * st.M / el
     line = {"impl": "reference", "metric": "energy+grad pair-terms/s", "value": val, "unit": "pair-terms/s",
@@ -280,13 +313,7 @@ def run_batch(args, rank, world):
         E, g = b.energy_grad(R, t, sig)
     el = time.perf_counter() - t0
     b.close()
-    tot = torch.tensor([pairs, el], dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        tt = tot.cuda()
-        dist.all_reduce(tt[:1], op=dist.ReduceOp.SUM)
-        dist.all_reduce(tt[1:], op=dist.ReduceOp.MAX)
-        tot = tt.cpu()
+    tot = all_reduce([pairs], "sum") + all_reduce([el], "max")
     if rank == 0:
         line = {"metric": "energy+grad pair-terms/s", "value": float(tot[0]) * steps / float(tot[1]),
                 "unit": "pair-terms/s", "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup),
@@ -308,13 +335,7 @@ def main():
         run_reference_gpu(args, rank)
         return
     if args.workload == 3:
-        import torch
-        torch.cuda.set_device(local)
-        if world > 1:
-            import datetime
-            import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", local))
+        dist_init(world, local)
         run_batch(args, rank, world)
         if world > 1:
             import torch.distributed as dist
@@ -322,11 +343,7 @@ def main():
         return
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    if world > 1:
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = dist_init(world, local)
     from dugma_b200 import _lib, api
     L = _lib.load(build_if_missing=False)
 
@@ -383,7 +400,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     import tempfile
-    with Clocks(os.path.join(tempfile.gettempdir(), f"dugma_clocks_rank{rank}.csv"), local) as clk:
+    with Clocks(os.path.join(tempfile.gettempdir(), f"dugma_clocks_rank{rank}.csv"), dev) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
@@ -397,10 +414,7 @@ def main():
     kl = ctypes.c_int(0)
     L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
     L.dugma_timing(h.arr, 0, None, None)
-    if world > 1:
-        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = all_reduce([ms], "max")[0]
     value = world * pairs * npose * args.steps / (ms * 1e-3)
     res = out[0].cpu().numpy()
 
@@ -484,10 +498,7 @@ def main():
             ph[1] += c - b
             ph[2] += d - c
         el = time.perf_counter() - t0
-        if world > 1:
-            te = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-            el = float(te.item())
+        el = all_reduce([el], "max")[0]
         e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "host_memory": "pinned",
                "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps,
@@ -495,7 +506,7 @@ def main():
                                "fr_m": 1e3 * ph[2] / ksteps}}
 
     cpu = None
-    if not args.no_cpu and rank == 0:
+    if not args.no_cpu and world == 1:
         rate, done, el, cores = cpu_rate(P, R, t, sig)
         cpu = {"value": rate, "unit": "pair-terms/s", "cores": cores, "kind": "port",
                "sample": f"{done // P.M} source rows x {P.M} targets ({el:.1f} s, FP64 oracle, OpenMP)"}

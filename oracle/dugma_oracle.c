@@ -511,6 +511,19 @@ double dugma_oracle_surrogate(int D, const double* A, const double* v, const uns
     return s;
 }
 
+/* Use n OpenMP threads from now on (n < 1: leave the setting alone); returns the count in use.
+ * Launchers such as torchrun pin OMP_NUM_THREADS to 1; timing code sets all host cores back. */
+int dugma_oracle_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n >= 1) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
 int dugma_oracle_num_threads(void)
 {
 #ifdef _OPENMP

@@ -47,6 +47,8 @@ def lib():
         L.dugma_oracle_sigma.restype = ctypes.c_double
         L.dugma_oracle_coef.argtypes = [ctypes.c_int] * 3 + [_f32p] * 6 + [_f64p, _f64p, ctypes.c_double, _f64p]
         L.dugma_oracle_num_threads.restype = ctypes.c_int
+        L.dugma_oracle_set_threads.restype = ctypes.c_int
+        L.dugma_oracle_set_threads.argtypes = [ctypes.c_int]
         _LIB = L
     return _LIB
 
@@ -141,6 +143,13 @@ class State:
 
 def num_threads() -> int:
     return lib().dugma_oracle_num_threads()
+
+
+def use_all_cores() -> int:
+    """Run the oracle on every host core (launchers may have set OMP_NUM_THREADS=1)."""
+    import os
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    return lib().dugma_oracle_set_threads(n)
 
 
 # ---------------------------------------------------------------------------
