@@ -37,6 +37,7 @@ EXPORTS = {
     "dugma_energy_fd_grad": (c_int, [PtrArray, dp, dp, c_double, c_int, c_double, dp, dp]),
     "dugma_nn": (c_int, [PtrArray, dp, dp, c_int, ip, fp]),
     "dugma_sigma": (c_int, [PtrArray, dp, dp, dp]),
+    "dugma_sigma_range": (c_int, [PtrArray, dp, dp, c_int, c_int, dp]),
     "dugma_energy_grad_async": (c_int, [PtrArray, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "dugma_energy_async": (c_int, [PtrArray, c_void_p, c_int, c_void_p, c_void_p]),
     "dugma_autotune": (c_int, [PtrArray, c_int, c_int, ctypes.c_char_p, c_size_t]),

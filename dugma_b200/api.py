@@ -174,6 +174,13 @@ def sigma(h: Handles, R, t) -> float:
     return s.value
 
 
+def sigma_range(h: Handles, R, t, i0, i1) -> np.ndarray:
+    """Partial sums behind sigma over source rows [i0, i1): (sum d2min, sum of quantised terms)."""
+    out = np.zeros(2)
+    check(_lib.load().dugma_sigma_range(h.arr, _ptr(_cm(R)), _ptr(_d(t)), int(i0), int(i1), _ptr(out)))
+    return out
+
+
 def autotune(h: Handles, what=0, model=_lib.MODEL_REF) -> str:
     buf = ctypes.create_string_buffer(1024)
     check(_lib.load().dugma_autotune(h.arr, int(what), int(model), buf, 1024))

@@ -417,6 +417,21 @@ int dugma_sigma(float* Ptr[6], const double* R, const double* t, double* sig)
     return DUGMA_OK;
 }
 
+int dugma_sigma_range(float* Ptr[6], const double* R, const double* t, int i_begin, int i_end, double sums[2])
+{
+    if (!R || !t || !sums) return set_error(DUGMA_ERR_ARG, "sigma_range: null argument");
+    GET_CTX(c, Ptr);
+    if (i_begin < 0 || i_end > c->N || i_begin > i_end)
+        return set_error(DUGMA_ERR_ARG, "sigma_range: bad source row range [%d, %d)", i_begin, i_end);
+    if (i_begin == i_end) {
+        sums[0] = sums[1] = 0.0;
+        return DUGMA_OK;
+    }
+    DUGMA_RET(upload_pose(*c, R, t, 1.0));
+    DUGMA_RET(launch_sigma(*c, c->pose, c->out, c->stream, i_begin, i_end));
+    return fetch(*c, c->out, 2, sums);
+}
+
 int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N, const double* M, const double* D,
                 const double* sig, double coefficient[640])
 {

@@ -141,8 +141,10 @@ int ref64_launch(Context& c, const double* pose_dev, int i0, int i1, double* out
 // Nearest neighbours: writes idx/d2 (device) and optionally the per-point minimum only.
 int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
               const KernelShape* force = nullptr);
-// sigma: out_dev[0] = exact FP64 sigma, out_dev[1] = quantised (reference) sigma.
-int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s);
+// sigma: out_dev[0] = exact FP64 sigma, out_dev[1] = quantised (reference) sigma.  For a source
+// row range [i0, i1) (i1 >= 0) the partial sums instead: out_dev[0] = sum of the nearest squared
+// distances, out_dev[1] = sum of the reference's quantised terms (an integer below 2^53).
+int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s, int i0 = 0, int i1 = -1);
 // Surrogate coefficient moments: out_dev receives kNumMoments doubles.
 // Source rows [i0, i1) carry the source-side (B) terms, target rows [j0, j1) the target-side
 // (C') terms; -1 for i1 / j1 means all rows.  Sums over partitions of both add up to the whole.

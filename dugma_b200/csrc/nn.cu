@@ -244,8 +244,13 @@ __global__ void sigma_final_kernel(const double* __restrict__ pe, const unsigned
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        out[0] = s_exact[0] / ((double)D * n);
-        out[1] = (double)__double2float_rn((double)s_q[0] / 1e6 / (double)n);
+        if (n > 0) {
+            out[0] = s_exact[0] / ((double)D * n);
+            out[1] = (double)__double2float_rn((double)s_q[0] / 1e6 / (double)n);
+        } else {   // the partial sums of a row range: sum d2min, and the sum of the quantised terms
+            out[0] = s_exact[0];
+            out[1] = (double)s_q[0];
+        }
     }
 }
 
@@ -284,9 +289,12 @@ std::vector<KernelShape> nn_shapes()
 }
 
 // Runs the brute-force search; dmin_dev (nullable) receives the nearest squared distance per source.
+// Source rows [i0, i1) (i1 < 0: all); idx/d2 rows are relative to i0, dmin is indexed absolutely.
 static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, float* dmin_dev,
-                  cudaStream_t s, const KernelShape* force)
+                  cudaStream_t s, const KernelShape* force, int i0 = 0, int i1 = -1)
 {
+    if (i1 < 0) i1 = c.N;
+    const int rows = i1 - i0;
     DUGMA_RET(launch_prologue(c, pose_dev, 0, s));
     const KernelShape want = force ? *force : c.shape_nn;
     const auto& vars = c.D == 3 ? nn_variants<3>() : nn_variants<2>();
@@ -303,16 +311,17 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     if (K == 16) sh.ipt = sh.nt == 128 ? 2 : 1;
     double* hp = nullptr;
     int n_jc = 0;
-    DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad / 2, 1, 0.0, pose_dev, 0, c.N, nullptr,
+    DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad / 2, 1, 0.0, pose_dev, i0, i1, nullptr,
                                   nullptr, &hp, K, &n_jc, s));
-    const int g = std::min((c.N + 255) / 256, c.num_sms * 8);
+    const int g = std::min((rows + 255) / 256, c.num_sms * 8);
     const float2* part = reinterpret_cast<const float2*>(hp);
+    float* dm = dmin_dev ? dmin_dev + i0 : nullptr;
     if (K == 1)
-        nn_merge_kernel<1><<<g, 256, 0, s>>>(part, n_jc, c.N, k, idx_dev, d2_dev, dmin_dev);
+        nn_merge_kernel<1><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
     else if (K == 8)
-        nn_merge_kernel<8><<<g, 256, 0, s>>>(part, n_jc, c.N, k, idx_dev, d2_dev, dmin_dev);
+        nn_merge_kernel<8><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
     else
-        nn_merge_kernel<16><<<g, 256, 0, s>>>(part, n_jc, c.N, k, idx_dev, d2_dev, dmin_dev);
+        nn_merge_kernel<16><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
@@ -324,16 +333,19 @@ int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2
     return nn_run(c, pose_dev, k, idx_dev, d2_dev, nullptr, s, force);
 }
 
-int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s)
+int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s, int i0, int i1)
 {
-    DUGMA_RET(nn_run(c, pose_dev, 1, nullptr, nullptr, c.dmin, s, nullptr));
+    const bool whole = i1 < 0;
+    if (whole) i1 = c.N;
+    const int rows = i1 - i0;
+    DUGMA_RET(nn_run(c, pose_dev, 1, nullptr, nullptr, c.dmin, s, nullptr, i0, i1));
     // partials in the scratch region (the search's chunk lists there are merged by now, in stream order)
-    const int nb = std::max(1, std::min(2 * c.num_sms, (c.N + 1023) / 1024));
+    const int nb = std::max(1, std::min(2 * c.num_sms, (rows + 1023) / 1024));
     DUGMA_RET(c.ensure_scratch(sizeof(double) * 2 * (size_t)nb));
     double* pe = c.scratch;
     unsigned long long* pq = reinterpret_cast<unsigned long long*>(c.scratch + nb);
-    sigma_partial_kernel<<<nb, 256, 0, s>>>(c.dmin, c.N, c.D, pe, pq);
-    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, c.N, c.D, out_dev);
+    sigma_partial_kernel<<<nb, 256, 0, s>>>(c.dmin + i0, rows, c.D, pe, pq);
+    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, whole ? c.N : 0, c.D, out_dev);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }

@@ -7,7 +7,7 @@ Two ways the path divides (no collective is on the data path of either):
     (dugma_energy_grad_range) and the partial energies and pose gradients (7 doubles in
     3D) are summed with one all-reduce; the surrogate coefficients likewise split by
     source and target rows (dugma_compi_range) and are summed with one all-reduce of 637
-    (45 in 2D) doubles.  Sums over rows are exactly the full sums up to FP64 rounding of
+    (45 in 2D) doubles, and sigma's two partial sums (dugma_sigma_range) with one of 2.  Sums over rows are exactly the full sums up to FP64 rounding of
     the final additions.
 """
 from __future__ import annotations
@@ -85,3 +85,16 @@ def compi_sharded(n_rows: int, m_rows: int, rank: int, world: int,
     if i1 > i0 or j1 > j0:
         part = np.asarray(compute(i0, i1, j0, j1), dtype=np.float64).reshape(-1)[:n_coef]
     return _all_reduce_sum(part, world, group)
+
+
+def sigma_sharded(n_rows: int, D: int, rank: int, world: int,
+                  compute: Callable[[int, int], Sequence[float]], group=None) -> tuple[float, float]:
+    """update_sig's sigma over source rows split across ranks: (quantised sigma as the reference
+    returns it, unquantised sigma).  `compute(i0, i1)` returns the two partial sums of a row
+    range, normally lambda i0, i1: dugma_b200.api.sigma_range(handles, R, t, i0, i1)."""
+    i0, i1 = row_ranges(n_rows, world)[rank]
+    part = np.zeros(2)
+    if i1 > i0:
+        part = np.asarray(compute(i0, i1), dtype=np.float64).reshape(-1)[:2]
+    s0, s1 = _all_reduce_sum(part, world, group)
+    return float(np.float32(s1 / 1e6 / n_rows)), float(s0 / (D * n_rows))

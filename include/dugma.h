@@ -111,6 +111,13 @@ int dugma_nn(float* Ptr[6], const double* R, const double* t, int k, int* idx, f
  * eigenvalues clamped to [lo, hi].  points: n x D (MATLAB layout); cov: n blocks of D x D. */
 int dugma_knn_covariance(const double* points, int n, int D, int k, double lo, double hi, double* cov);
 
+/* Partial sums behind sigma for source rows [i_begin, i_end), for sharding update_sig across
+ * GPUs: sums[0] = sum of the nearest squared distances (FP64), sums[1] = sum of the reference's
+ * quantised terms round(d2 / D * 1e6) (an exact integer).  Over a partition of the rows,
+ * sigma = float(S1 / 1e6 / N) as update_sig returns it, and S0 / (D N) unquantised.
+ * No counterpart in the reference. */
+int dugma_sigma_range(float* Ptr[6], const double* R, const double* t, int i_begin, int i_end, double sums[2]);
+
 /* sigma without quantisation (FP64 sum of the exact nearest squared distances / (D N)). */
 int dugma_sigma(float* Ptr[6], const double* R, const double* t, double* sig);
 

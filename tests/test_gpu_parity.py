@@ -125,6 +125,15 @@ def test_sigma_matches_oracle(w0):
         s_ref = api.update_sig(h, R, t)
         assert s_ref == np.float32(st.sigma(R, t, quantised=True))
         assert api.sigma(h, R, t) == st.sigma(R, t, quantised=False)
+        # partial sums over an uneven partition of the rows (sharding update_sig): the quantised
+        # terms add up exactly, the FP64 sums to rounding
+        n = P.N
+        parts = [api.sigma_range(h, R, t, a, b) for (a, b) in [(0, 1), (1, n // 3), (n // 3, n // 3), (n // 3, n)]]
+        S = np.sum(parts, axis=0)
+        assert np.float32(S[1] / 1e6 / n) == s_ref
+        assert abs(S[0] / (3 * n) - st.sigma(R, t, quantised=False)) <= 1e-14 * S[0] / (3 * n)
+    with pytest.raises(api.DugmaError):
+        api.sigma_range(h, np.eye(3), np.zeros(3), 0, P.N + 1)
 
 
 # ---------------------------------------------------------------- energy and adjoint

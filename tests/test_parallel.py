@@ -104,3 +104,43 @@ def test_compi_sharded_sum_matches_unsharded():
         got = np.asarray(out[r])
         assert np.max(np.abs(got - A)) <= 1e-12 * np.max(np.abs(A))
     assert np.array_equal(np.asarray(out[0]), np.asarray(out[1]))
+
+
+def _sigma_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from oracle import oracle as orc
+    from dugma_b200 import synth
+    from dugma_b200.parallel import sigma_sharded
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    P = synth.workload0(n=300)
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    _, d2 = st.nn(P.R_G, P.t_G, 1)
+    d2 = d2[:, 0]
+
+    def compute(i0, i1):
+        # partial sums of the oracle's nearest squared distances over this rank's rows, with
+        # the reference's quantisation of each term (the library's dugma_sigma_range contract)
+        q = np.rint((d2[i0:i1] / np.float32(3)).astype(np.float32) * np.float32(1e6)).astype(np.float64)
+        return [float(np.sum(d2[i0:i1].astype(np.float64))), float(q.sum())]
+
+    out[rank] = list(sigma_sharded(P.N, 3, rank, world, compute))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sigma_sharded_matches_unsharded():
+    from oracle import oracle as orc
+    from dugma_b200 import synth
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_sigma_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
+    P = synth.workload0(n=300)
+    st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    sq, se = st.sigma(P.R_G, P.t_G, quantised=True), st.sigma(P.R_G, P.t_G, quantised=False)
+    for r in range(world):
+        got = out[r]
+        assert got[0] == np.float32(sq)
+        assert abs(got[1] - se) <= 1e-14 * se
