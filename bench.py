@@ -43,8 +43,8 @@ sys.path.insert(0, ROOT)
 # algorithmic per-pair operation counts of the REF kernels, 3D (see the kernel sources)
 FP32_INSTR_ADJOINT = 44     # d 6, u = kC'd 9, exponent 3, d d^T 6, exponent 6, accumulations 14
 # CONV adjoint: d 6, S = Sx + C'y 6, adjugate 12, det 3, singularity test 3, h = adj d 9, d.h 3,
-# exponent and normalisation 5, energy 1, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
-FP32_INSTR_CONV_ADJOINT = 66
+# exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
+FP32_INSTR_CONV_ADJOINT = 68
 FP32_INSTR_ENERGY = 26      # d 6, two Horner quadratic forms 9 + 9, accumulation 2
 SFU_PER_PAIR = 2            # two ex2
 
