@@ -44,6 +44,16 @@ def cov_to_matlab(C) -> np.ndarray:
     return C.transpose(1, 0, 2).reshape(D, n * D).copy()
 
 
+def load_cloud(path: str, var: str = "X") -> np.ndarray:
+    """Read one D x N cloud (single or double) from a .mat file -> (N, D) float64 (the
+    dataset's shape-model files hold a single model cloud X)."""
+    from scipy.io import loadmat
+    m = loadmat(path)
+    if var not in m:
+        raise KeyError(f"{path}: no variable {var!r}")
+    return cloud_from_matlab(m[var])
+
+
 def load_problem(path: str, x: str = "X", y: str = "Y", x_cov: str = "X_C", y_cov: str = "Y_C",
                  r_gt: str = "R_G", t_gt: str = "t_G") -> Problem:
     """Read a registration problem from a .mat file in the reference's layout.  The ground

@@ -47,3 +47,13 @@ def test_mat_errors(tmp_path):
     savemat(path, {"X": np.zeros((3, 4))})
     with pytest.raises(KeyError):
         matio.load_problem(path)
+
+
+def test_load_single_precision_model_cloud(tmp_path):
+    from scipy.io import savemat
+    X = np.random.default_rng(0).standard_normal((3, 17)).astype(np.float32)
+    path = str(tmp_path / "model.mat")
+    savemat(path, {"X": X})
+    got = matio.load_cloud(path)
+    assert got.shape == (17, 3) and got.dtype == np.float64
+    assert np.array_equal(got, X.T.astype(np.float64))
