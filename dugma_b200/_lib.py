@@ -58,6 +58,7 @@ EXPORTS = {
     "dugma_set_shape": (c_int, [PtrArray, c_int, c_int, c_int, c_int, c_int]),
     "dugma_get_shape": (c_int, [PtrArray, c_int, ip]),
     "dugma_calibrate": (c_int, [c_int, dp, dp]),
+    "dugma_wait_selftest": (c_int, [c_int, ip]),
 }
 
 

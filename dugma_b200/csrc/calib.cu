@@ -54,6 +54,21 @@ __global__ void __launch_bounds__(256) ex2_chains_kernel(float* out, int iters)
     if (s == 12345.678f) out[blockIdx.x] = s;
 }
 
+// The bounded-wait path of the pair kernels, exercised on purpose: one mbarrier whose phase
+// nothing completes (no arrival, no copy in flight), polled by every thread of one warp
+// through mbar_wait_bounded with `polls` polls.  The wait runs out, the error word gets the
+// timeout bit and the kernel returns; nothing is left pending on the device.
+__global__ void wait_selftest_kernel(uint32_t polls, int* err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    mbar_wait_bounded(&bar, 0u, err, polls);
+}
+
 }  // namespace dugma
 
 extern "C" int dugma_calibrate(int what, double* lane_ops_per_s, double* ms)
@@ -96,4 +111,23 @@ extern "C" int dugma_calibrate(int what, double* lane_ops_per_s, double* ms)
     *lane_ops_per_s = best;
     if (ms) *ms = best_ms;
     return DUGMA_OK;
+}
+
+extern "C" int dugma_wait_selftest(int polls, int* timed_out)
+{
+    using namespace dugma;
+    if (!timed_out || polls < 1 || polls > (1 << 20))
+        return set_error(DUGMA_ERR_ARG, "wait_selftest: need timed_out and 1 <= polls <= 2^20");
+    int* err = nullptr;
+    DUGMA_CK(cudaMalloc(&err, sizeof(int)));
+    int rc = DUGMA_OK, h = 0;
+    if (cudaMemset(err, 0, sizeof(int)) != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "wait_selftest: memset");
+    if (rc == DUGMA_OK) {
+        wait_selftest_kernel<<<1, 32>>>((uint32_t)polls, err);
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = set_error(DUGMA_ERR_CUDA, "wait_selftest: kernel failed");
+    }
+    cudaFree(err);
+    *timed_out = (h >> DUGMA_ERR_TIMEOUT) & 1;
+    return rc;
 }

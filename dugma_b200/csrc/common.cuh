@@ -166,9 +166,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 // Bounded wait: gives up after `limit` polls (each poll may suspend the thread for a
 // hardware-chosen interval), records DUGMA_ERR_TIMEOUT in *err and returns false.
 constexpr uint32_t kWaitPolls = 1u << 24;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err,
+                                                  uint32_t limit = kWaitPolls)
 {
-    for (uint32_t it = 0; it < kWaitPolls; ++it)
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     if (err) atomicOr(err, 1 << DUGMA_ERR_TIMEOUT);
     return false;

@@ -217,6 +217,14 @@ int dugma_timing(float* Ptr[6], int mode, double* total_ms, int* launches);
  * kernel time in ms). */
 int dugma_calibrate(int what, double* lane_ops_per_s, double* ms);
 
+/* Diagnostic of the failure path: every wait of the pair kernels on a shared-memory tile is
+ * bounded; when it runs out the kernel sets DUGMA_ERR_TIMEOUT in the context's error word,
+ * drains its copies and returns, and the host call reports DUGMA_ERR_TIMEOUT.  This runs one
+ * such wait on an mbarrier that nothing completes, with `polls` (1 .. 2^20) polls, and sets
+ * *timed_out = 1 when the wait gave up as designed; the device stays usable.  No counterpart
+ * in the reference. */
+int dugma_wait_selftest(int polls, int* timed_out);
+
 /* The solver the driver uses in place of fmincon (DUGMA.m:73 with energy3D.m / fcontr3D.m;
  * 2D: DUGMA.m:65 with energy2D.m / fcontr2D.m): minimises Q(dR, dt) = sum_k A_k b_k(dR, dt) over
  * dR in SO(D) (dR = exp([w]x), 2D a rotation by theta) and dt, from dR = I, dt = 0.

@@ -333,6 +333,24 @@ def test_ref_precision_model_matches_oracle(D, n, m):
         api.fr_m(h)
 
 
+def test_bounded_wait_gives_up_and_device_stays_usable(w0):
+    """The failure path of every tile wait, made to happen: a wait on an mbarrier that nothing
+    completes gives up after its poll limit and reports a timeout instead of hanging; the
+    device and an existing context keep working afterwards."""
+    import ctypes
+    from dugma_b200 import _lib
+    L = _lib.load()
+    flag = ctypes.c_int(0)
+    assert L.dugma_wait_selftest(1000, ctypes.byref(flag)) == 0
+    assert flag.value == 1
+    assert L.dugma_wait_selftest(0, ctypes.byref(flag)) == _lib.ERR_ARG
+    P, st, h = w0
+    R, t = _pose(3, 31)
+    E, g, _ = api.energy_grad(h, R, t, 0.05)
+    Eo, go, _ = st.energy(R, t, 0.05)
+    assert abs(E - Eo) <= 1e-6 * Eo and _rel(g, go) <= 1e-5
+
+
 def test_range_partials_sum_to_total(w0):
     P, st, h = w0
     R, t = _pose(3, 2)
