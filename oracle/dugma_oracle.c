@@ -329,7 +329,7 @@ int dugma_oracle_energy_conv(int D, int N, int M, const float* x, const float* x
         for (int i = ib; i < ie; ++i) {
             double dxi[3] = {0};
             for (int j = 0; j < M; ++j) {
-                double S[6], Si[6], det, d[3], u[3], r[3], Su[3], m = 0;
+                double S[6], Si[6], det, d[3] = {0, 0, 0}, u[3] = {0, 0, 0}, r[3] = {0, 0, 0}, Su[3] = {0, 0, 0}, m = 0;
                 for (int k = 0; k < ns; ++k) S[k] = Sy[(size_t)j * ns + k] + Sx[(size_t)i * ns + k];
                 sym_inv_det(D, S, Si, &det);
                 if (!(det > 0)) continue;
