@@ -30,12 +30,13 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
-// the same with a register budget that keeps MINB blocks resident per SM
-template <class Body, int NT, int TJ, int MINB>
+// the same with a register budget that keeps MINB blocks resident per SM, and the record loop
+// unrolled UNROLL times
+template <class Body, int NT, int TJ, int MINB, int UNROLL = 4>
 __global__ void __launch_bounds__(NT, MINB) pair_kernel_occ(PairArgs a)
 {
     Body body;
-    run_pairs<Body, NT, TJ, 4>(a, body);
+    run_pairs<Body, NT, TJ, 4, UNROLL>(a, body);
 }
 
 // deterministic reduction of per-item partials: out[v] = sum_items partials[item][v];

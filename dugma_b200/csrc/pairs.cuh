@@ -32,7 +32,7 @@ struct PairArgs {
     int* err;
 };
 
-template <class Body, int NT, int TJ, int STAGES>
+template <class Body, int NT, int TJ, int STAGES, int UNROLL = 4>
 __device__ __forceinline__ void run_pairs(const PairArgs& a, Body& body)
 {
     using Rec = typename Body::StreamRec;
@@ -81,7 +81,7 @@ __device__ __forceinline__ void run_pairs(const PairArgs& a, Body& body)
             const int st = u % STAGES;
             const bool ok = mbar_wait_bounded(&bars[st], (u / STAGES) & 1u, a.err);
             const Rec* yb = ybuf[st];
-#pragma unroll 4
+#pragma unroll UNROLL
             for (int jj = 0; jj < TJ; ++jj) body.consume(yb[jj], (tile0 + k) * TJ + jj);
             body.fold();
             if (__syncthreads_or(!ok)) {
