@@ -5,7 +5,8 @@ Tolerances (written per assertion):
   * nearest-neighbour indices and squared distances: bit-exact (same FP32 sequence);
   * sigma: bit-exact against the oracle's quantised and exact forms;
   * energy: relative 1e-6; pose gradient: relative 1e-5 (norm-wise) on
-    well-conditioned covariances (1K sphere, 64K harmonic surface); the 6K
+    well-conditioned covariances (1K sphere here; the 64K harmonic surface and the 300K
+    depth views in test_gpu_fullsize.py); the 6K
     workload's noise-free source has covariances of condition up to ~7e3,
     where FP32 per-pair arithmetic is good to ~3e-4 (its own assertion);
   * surrogate coefficients: |A - A_oracle| <= 2e-6 max|A_oracle|.
