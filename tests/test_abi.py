@@ -63,3 +63,20 @@ def test_errors_are_returned_not_fatal():
     coef = ctypes.c_double(5)
     rc = L.dugma_init(None, None, None, None, ctypes.byref(coef), 10, 10, 3, ptrs)
     assert rc == _lib.ERR_ARG and coef.value == 0
+
+
+def build_mex_harness(out_dir):
+    """Compile tests/abi/mex_harness.cpp against include/dugma_mex.hpp and link it to the
+    library: the reference's C++ signatures resolve against the exported symbols."""
+    lib = build.build()
+    exe = os.path.join(str(out_dir), "mex_harness")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "abi", "mex_harness.cpp"), "-o", exe,
+                    "-L", os.path.dirname(lib), "-ldugma_b200", "-Wl,-rpath," + os.path.dirname(lib)],
+                   check=True, capture_output=True)
+    return exe
+
+
+def test_reference_gateway_calls_link(tmp_path):
+    exe = build_mex_harness(tmp_path)
+    assert os.access(exe, os.X_OK)

@@ -440,3 +440,31 @@ def test_knn_covariance_matches_cpu_estimator():
     err = np.abs(got - ref).reshape(len(pts), -1).max(axis=1) / np.abs(ref).reshape(len(pts), -1).max(axis=1)
     assert np.mean(err < 1e-6) > 0.99, np.sort(err)[-10:]
     assert np.all(np.linalg.eigvalsh(got) >= 1e-6 * (1 - 1e-9))
+
+
+# ---------------------------------------------------------------- the reference's C++ entry points
+def test_reference_cpp_entry_points_match_python_mirror(tmp_path):
+    """A C++ program calls init / cpd (update_sig) / cpd (compi) / fr_m by the reference's own
+    signatures, as its MEX gateways do; the results equal the C-ABI path's (same kernels)."""
+    import subprocess
+    from tests.test_abi import build_mex_harness
+    exe = build_mex_harness(tmp_path)
+    P = synth.workload0(n=700)
+    R, t = P.R_G @ expmap([0.05, 0.02, -0.03]), P.t_G
+    inp, out = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(inp, "wb") as f:
+        np.array([P.N, P.M, 3], np.int32).tofile(f)
+        for a in (P.X, np.transpose(P.X_C, (0, 2, 1)), P.Y, np.transpose(P.Y_C, (0, 2, 1)), np.asarray(R).T,
+                  np.asarray(t)):
+            np.ascontiguousarray(a, np.float64).tofile(f)
+    subprocess.run([exe, inp, out], check=True, timeout=300)
+    res = np.fromfile(out, np.float64)
+    assert res[0] == 1.0
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    try:
+        sig = api.update_sig(h, R, t)
+        A = api.compi(h, R, t, sig=sig)
+    finally:
+        api.fr_m(h)
+    assert res[1] == sig
+    assert np.array_equal(res[2:2 + 637], A)
