@@ -5,6 +5,7 @@
 // FP32 rounding of y' match the CPU oracle bit for bit.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "context.hpp"
 
@@ -20,9 +21,11 @@ namespace dugma {
 template <int D>
 __global__ void init_points_kernel(const double* __restrict__ P, const double* __restrict__ C, int n,
                                    float* __restrict__ p32, float* __restrict__ cinv,
-                                   float* __restrict__ w, float* __restrict__ cpack, double inv_scale, int* nonpd)
+                                   float* __restrict__ w, float* __restrict__ cpack, const double* __restrict__ scale,
+                                   int* nonpd)
 {
     constexpr int NS = Sym<D>::N;
+    const double inv_scale = scale[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 #pragma unroll
         for (int a = 0; a < D; ++a) p32[(size_t)i * D + a] = __double2float_rn(P[(size_t)i * D + a]);
@@ -99,6 +102,32 @@ __global__ void norm_log2_kernel(const float* __restrict__ w, int n, const doubl
         lw[i] = w[i] > 0.0f ? __double2float_rn(log2((double)w[i]) - L) : -INFINITY;
 }
 
+// CONV covariance scale: the mean of trace / D over both clouds' covariances (the FP64 staged
+// inputs), rounded to a power of two so that dividing by it is exact in FP32.  One block,
+// fixed order.  scale[0] = the scale, scale[1] = its inverse.
+__global__ void cov_scale_kernel(const double* __restrict__ XC, int n, const double* __restrict__ YC, int m, int D,
+                                 double* __restrict__ scale)
+{
+    __shared__ double red[1024];
+    double s = 0;
+    for (int i = threadIdx.x; i < n + m; i += blockDim.x) {
+        const double* C = i < n ? XC + (size_t)i * D * D : YC + (size_t)(i - n) * D * D;
+        for (int a = 0; a < D; ++a) s += C[a * (D + 1)];
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double tr = red[0] / ((double)D * (n + m));
+        const double c = (isfinite(tr) && tr > 0) ? exp2(round(log2(tr))) : 1.0;
+        scale[0] = c;
+        scale[1] = 1.0 / c;
+    }
+}
+
 int launch_init(Context& c, const double* X, const double* XC, const double* Y, const double* YC)
 {
     const int D = c.D, N = c.N, M = c.M;
@@ -122,37 +151,30 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     ck(cudaMemsetAsync(c.counter, 0, sizeof(int) * 8, s), "memset");
     const int bs = 256;
     const int gx = std::min((N + bs - 1) / bs, c.num_sms * 8), gy = std::min((M + bs - 1) / bs, c.num_sms * 8);
-    double* Lm = c.out;   // scratch: out[0], out[1]
+    double* Lm = c.out;   // scratch: out[0], out[1] max log2 weights; out[2], out[3] the covariance scale
     // CONV covariances are kept divided by the mean of trace / D over both clouds
-    double tr = 0;
-    for (size_t i = 0; i < (size_t)N; ++i)
-        for (int a = 0; a < D; ++a) tr += XC[i * D * D + a * (D + 1)];
-    for (size_t i = 0; i < (size_t)M; ++i)
-        for (int a = 0; a < D; ++a) tr += YC[i * D * D + a * (D + 1)];
-    tr /= (double)D * (N + M);
-    // a power of two, so that dividing by it is exact in FP32
-    c.cscale = (std::isfinite(tr) && tr > 0) ? std::exp2(std::round(std::log2(tr))) : 1.0;
-    const double inv = 1.0 / c.cscale;
+    cov_scale_kernel<<<1, 1024, 0, s>>>(tXC, N, tYC, M, D, Lm + 2);
     if (D == 3) {
-        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, inv, c.counter);
-        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, inv, c.counter);
+        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
+        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
     } else {
-        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, inv, c.counter);
-        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, inv, c.counter);
+        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
+        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
     }
     max_log2_kernel<<<1, 1024, 0, s>>>(c.wx, N, Lm);
     max_log2_kernel<<<1, 1024, 0, s>>>(c.wy, M, Lm + 1);
     norm_log2_kernel<<<gx, bs, 0, s>>>(c.wx, N, Lm, c.lwx);
     norm_log2_kernel<<<gy, bs, 0, s>>>(c.wy, M, Lm + 1, c.lwy);
     ck(cudaGetLastError(), "init kernels");
-    ck(cudaMemcpyAsync(c.host, Lm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax");
-    ck(cudaMemcpyAsync(c.host + 2, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
+    ck(cudaMemcpyAsync(c.host, Lm, 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax, scale");
+    ck(cudaMemcpyAsync(c.host + 3, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
     ck(cudaStreamSynchronize(s), "sync");
     if (rc != DUGMA_OK) return rc;
     c.Lmax_x = std::isfinite(c.host[0]) ? c.host[0] : 0.0;
     c.Lmax_y = std::isfinite(c.host[1]) ? c.host[1] : 0.0;
+    c.cscale = c.host[2];
     int nonpd = 0;
-    memcpy(&nonpd, c.host + 2, sizeof(int));
+    memcpy(&nonpd, c.host + 3, sizeof(int));
     c.nonpd = nonpd;
     return DUGMA_OK;
 }
