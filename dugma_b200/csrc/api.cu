@@ -174,6 +174,37 @@ static void arena_release(int dev, void* p, size_t bytes)
     cudaFree(p);
 }
 
+// streams of freed contexts are kept (per device, up to kStreamCache) for the next init
+constexpr size_t kStreamCache = 16;
+static std::mutex g_stream_mu;
+static std::vector<std::pair<int, cudaStream_t>> g_streams;
+
+static cudaError_t stream_acquire(int dev, cudaStream_t* s)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_stream_mu);
+        for (size_t k = 0; k < g_streams.size(); ++k)
+            if (g_streams[k].first == dev) {
+                *s = g_streams[k].second;
+                g_streams.erase(g_streams.begin() + k);
+                return cudaSuccess;
+            }
+    }
+    return cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+}
+
+static void stream_release(int dev, cudaStream_t s)   // s has no pending work
+{
+    {
+        std::lock_guard<std::mutex> lk(g_stream_mu);
+        if (g_streams.size() < kStreamCache) {
+            g_streams.push_back({dev, s});
+            return;
+        }
+    }
+    cudaStreamDestroy(s);
+}
+
 static void destroy_context(Context* c)
 {
     if (!c) return;
@@ -187,7 +218,7 @@ static void destroy_context(Context* c)
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream) stream_release(c->dev, c->stream);
     delete c;
 }
 
@@ -324,7 +355,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
         return set_error(DUGMA_ERR_CUDA, "init: no CUDA device");
     }
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev);
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (stream_acquire(c->dev, &c->stream) != cudaSuccess)
         return fail(set_error(DUGMA_ERR_CUDA, "init: stream creation failed"));
     // One device arena holds every per-context buffer.  Its scratch region first receives
     // the FP64 host inputs during init and afterwards the kernels' partial sums.
