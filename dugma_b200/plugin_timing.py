@@ -1,11 +1,12 @@
 """Wall-clock timing of the reference-interface plugin calls (update_sig, compi) through the C ABI.
 
-    python -m dugma_b200.plugin_timing [--n 4096] [--reps 20]
+    python -m dugma_b200.plugin_timing [--n 4096] [--reps 20] [--knn K]
 
 On the 1K workload's generator (bumpy sphere, sensor covariances) at N = M = n: one init,
 3 warm-up compi calls, `reps` timed compi calls, then `reps` timed update_sig calls, each a
-host-to-host call like the reference's MEX gateway makes.  Prints one JSON line with the
-medians in ms.
+host-to-host call like the reference's MEX gateway makes.  With --knn K it also times the
+k-nearest-neighbour covariance estimator (dugma_knn_covariance) on the source cloud.  Prints
+one JSON line with the medians in ms.
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--knn", type=int, default=0, help="also time the k-NN covariance estimator with this k")
     a = ap.parse_args(argv)
     P = synth.workload0(n=a.n)
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
@@ -42,8 +44,18 @@ def main(argv=None):
             ts.append(time.perf_counter() - t0)
     finally:
         api.fr_m(h)
-    print(json.dumps({"n": a.n, "compi_ms": 1e3 * float(np.median(tc)), "update_sig_ms": 1e3 * float(np.median(ts)),
-                      "compi_pair_terms_per_s": a.n * a.n / float(np.median(tc))}), flush=True)
+    line = {"n": a.n, "compi_ms": 1e3 * float(np.median(tc)), "update_sig_ms": 1e3 * float(np.median(ts)),
+            "compi_pair_terms_per_s": a.n * a.n / float(np.median(tc))}
+    if a.knn:
+        api.knn_covariance(P.X, k=a.knn)
+        tk = []
+        for _ in range(max(1, a.reps // 4)):
+            t0 = time.perf_counter()
+            api.knn_covariance(P.X, k=a.knn)
+            tk.append(time.perf_counter() - t0)
+        line["knn_covariance_ms"] = 1e3 * float(np.median(tk))
+        line["knn_k"] = a.knn
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
