@@ -136,6 +136,18 @@ def profiled_traffic(shape_key):
     return traffic if shape == tuple(shape_key) else None
 
 
+def hbm_view(bytes_per_launch, kernel_ms):
+    """The same launch against the HBM roofline of MEASURED_PEAKS.json (the algorithmic bytes,
+    every record read once): shows how far from memory-bound the kernel is."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        peak = float(json.load(open(path))["hbm_gbs"])
+    except Exception:
+        return None
+    gbs = bytes_per_launch / (kernel_ms * 1e-3) / 1e9
+    return {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}
+
+
 def eval_pose(P, unit):
     """Multistart pose number `unit`: ground truth perturbed by a seeded 10 deg, 2 cm offset."""
     from dugma_b200.pose import expmap
@@ -529,7 +541,8 @@ def main():
                          "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json has "
                                         "no FP32-pipe figure)",
                          "sfu_frac": sfu_frac, "kernel_ms": kernel_ms,
-                         "instr_per_pair": instr},
+                         "instr_per_pair": instr,
+                         "hbm_view": hbm_view(64 * (P.N + P.M), kernel_ms)},
             "gpu_launches": 3 * args.steps * npose,
             "result": {"E": float(res[0]), "g": [float(v) for v in res[1:7]]},
             "autotune": tune,
