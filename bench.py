@@ -41,7 +41,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic per-pair operation counts of the REF kernels, 3D (see the kernel sources)
-FP32_INSTR_ADJOINT = 44     # d 6, u = kC'd 9, exponent 3, d d^T 6, exponent 6, accumulations 14
+# REF adjoint: d 6, u = kC'd 9, d.u 3, B exponent (Horner) 9, energy 2, S1 += e1 u 3, w = e2 d 3,
+# D2 += w 3, Q2 += w d^T 6
+FP32_INSTR_ADJOINT = 44
 # CONV adjoint: d 6, S = Sx + C'y 6, adjugate 12, det 3, singularity test 3, h = adj d 9, d.h 3,
 # exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
 FP32_INSTR_CONV_ADJOINT = 68
