@@ -309,6 +309,14 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     // the k = 8 / 16 kernels keep fewer sources per thread (see the variant table)
     if (K == 8) sh.ipt = sh.nt == 128 ? 4 : 2;
     if (K == 16) sh.ipt = sh.nt == 128 ? 2 : 1;
+    if (K > 1) {
+        // every target chunk restarts the sorted lists, and a list insertion (taken by some lane
+        // of a warp far more often than by one thread) costs the whole warp ~4K instructions:
+        // few long chunks, just enough items to fill the GPU about once
+        const int n_ib = (rows + sh.ipt * sh.nt - 1) / (sh.ipt * sh.nt);
+        const int want_jc = std::max(1, (4 * c.num_sms + n_ib - 1) / n_ib);
+        sh.min_chunk = std::max(1, (c.M_pad / 2 + want_jc - 1) / want_jc);
+    }
     double* hp = nullptr;
     int n_jc = 0;
     DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad / 2, 1, 0.0, pose_dev, i0, i1, nullptr,
