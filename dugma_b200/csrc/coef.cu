@@ -468,8 +468,8 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
             *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 128, 16, 2>
                             : coef_pass_kernel<PackedCoefBody<D, 2, false>, 128, 16, 2>;
         else
-            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 64, 16, 4>
-                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 64, 16, 4>;
+            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 64, 16, 6>
+                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 64, 16, 6>;
         return big ? KernelShape{2, 128, 16, 2, 0, min_chunk} : KernelShape{2, 64, 16, 2, 0, min_chunk};
     };
     {
