@@ -153,6 +153,10 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     const int resident = c.num_sms * occupancy_blocks(fn, sh.nt);
     const int target = 4 * resident;
     int n_jc = std::max(1, std::min(total_tiles, (target + n_ib - 1) / n_ib));
+    // small problems: rather than many one-tile items (each pays the per-item set-up, FP64
+    // contraction and block reduction), one wave of items that fills the resident blocks,
+    // unless that makes items longer than 1/8 of the targets
+    n_jc = std::min(n_jc, std::max(std::max(1, resident / n_ib), total_tiles / 8));
     if (sh.max_chunk > 0) n_jc = std::max(n_jc, (total_tiles * sh.tj + sh.max_chunk - 1) / sh.max_chunk);
     if (sh.min_chunk > 0) n_jc = std::min(n_jc, std::max(1, total_tiles * sh.tj / sh.min_chunk));
     n_jc = std::min(n_jc, total_tiles);
