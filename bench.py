@@ -492,7 +492,8 @@ def main():
         Xh, Yh = pinned(P.X), pinned(P.Y)
         X_C = pinned(np.transpose(P.X_C, (0, 2, 1))).transpose(0, 2, 1)
         Y_C = pinned(np.transpose(P.Y_C, (0, 2, 1))).transpose(0, 2, 1)
-        h2d = 8 * (Xh.size + X_C.size + Yh.size + Y_C.size)
+        # the clouds and covariances, plus the 16-double pose block dugma_energy_grad uploads
+        h2d = 8 * (Xh.size + X_C.size + Yh.size + Y_C.size) + 8 * 16
         # warm-up of the end-to-end path
         _, h2 = api.init(Xh, X_C, Yh, Y_C)
         api.energy_grad(h2, R, t, sig, model=args.model)
