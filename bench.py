@@ -18,6 +18,8 @@ roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instruc
             against the FP32 fused-multiply-add rate measured in this run.
 plain_fd    the plain form: energy + central finite differences (13 energy evaluations).
 cpu_baseline  the FP64 C/OpenMP oracle on a bounded sample of source rows, all host cores.
+accuracy    this run's relative error against that FP64 oracle on the same sampled rows
+            (energy and the pose gradient of source rows [0, rows) over all targets).
 
 With --poses P a step evaluates P multistart poses of the problem back to back (one
 launch sequence per pose); the depth-camera workload is quoted with P = 64.  The
@@ -208,23 +210,27 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_rate(P, R, t, sig, budget_s=8.0):
-    """Oracle (FP64, OpenMP, all host threads) pair-terms/s on a bounded sample of source rows."""
+def cpu_rate(P, R, t, sig, model=0, budget_s=8.0):
+    """Oracle (FP64, OpenMP, all host threads) pair-terms/s on a bounded sample of source rows
+    [0, i0); also returns the oracle's energy and pose gradient summed over those rows."""
     from oracle import oracle as orc
     orc.use_all_cores()
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+    fn = st.energy_conv if model == 1 else st.energy
     rows = 64
     done = 0
+    E, g = 0.0, 0.0
     t0 = time.perf_counter()
     i0 = 0
     while time.perf_counter() - t0 < budget_s and i0 < st.N:
         i1 = min(st.N, i0 + rows)
-        st.energy(R, t, sig, i0=i0, i1=i1)
+        e, gg, _ = fn(R, t, sig, i0=i0, i1=i1)
+        E, g = E + e, g + gg
         done += (i1 - i0) * st.M
         i0 = i1
         rows = min(rows * 2, 4096)
     el = time.perf_counter() - t0
-    return done / el, done, el, orc.num_threads()
+    return done / el, done, el, orc.num_threads(), (i0, E, g)
 
 
 def run_reference(args, rank, world):
@@ -522,9 +528,17 @@ def main():
 
     cpu = None
     if not args.no_cpu and world == 1:
-        rate, done, el, cores = cpu_rate(P, R, t, sig)
+        rate, done, el, cores, (nrow, Eo, go) = cpu_rate(P, R, t, sig, args.model)
         cpu = {"value": rate, "unit": "pair-terms/s", "cores": cores, "kind": "port",
                "sample": f"{done // P.M} source rows x {P.M} targets ({el:.1f} s, FP64 oracle, OpenMP)"}
+        # this run's error against the FP64 oracle on the same rows: the fused adjoint over source
+        # rows [0, nrow) through the C ABI against the oracle's sum over those rows
+        Eg, gg = api.energy_grad_range(h, R, t, sig, 0, nrow, model=args.model)
+        go = np.asarray(go, np.float64)
+        accuracy = {"rows": int(nrow), "targets": int(P.M), "E_oracle": float(Eo), "E": float(Eg),
+                    "E_rel_err": abs(Eg - Eo) / abs(Eo) if Eo else None,
+                    "grad_rel_err": float(np.max(np.abs(gg - go)) / np.max(np.abs(go))) if np.any(go) else None,
+                    "tolerance": {"E": 1e-6, "grad": 1e-5}}
 
     if rank == 0:
         clocks = clk.summary()
@@ -555,6 +569,7 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+            line["accuracy"] = accuracy
         if clocks:
             line["clocks"] = clocks
         line.update(extra)
