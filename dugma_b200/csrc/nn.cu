@@ -29,7 +29,7 @@ struct NNBody {
     using StreamRec = NNRec2;
     static constexpr int IPT = IPT_;
     static constexpr int NV = 1;
-    float x[IPT][D];
+    float2 X[IPT][D];   // source coordinates, duplicated in both halves
     float bd[IPT][K];
     int bi[IPT][K];
     int row[IPT];
@@ -40,7 +40,10 @@ struct NNBody {
         const float* xs = static_cast<const float*>(a.xrec);
         row[ii] = i < a.i_end ? i : -1;
 #pragma unroll
-        for (int q = 0; q < D; ++q) x[ii][q] = i < a.i_end ? xs[(size_t)i * D + q] : 0.f;
+        for (int q = 0; q < D; ++q) {
+            const float v = i < a.i_end ? xs[(size_t)i * D + q] : 0.f;
+            X[ii][q] = make_float2(v, v);
+        }
     }
     __device__ void zero_all()
     {
@@ -49,37 +52,44 @@ struct NNBody {
 #pragma unroll
             for (int q = 0; q < K; ++q) { bd[ii][q] = INFINITY; bi[ii][q] = 0x7fffffff; }
     }
+    // both targets of a record in one f32x2 sequence (per half the FP32 operations of the
+    // reference: d = x + (-y'), d2 = fmaf(dz,dz, fmaf(dy,dy, dx*dx))), then one test of the
+    // nearer of the two against the k-th distance; the rare insertions take the targets in
+    // index order, so ties keep the lower j
     __device__ __forceinline__ void consume(const NNRec2& r, int jp)
     {
-        one(r.a.x, r.a.z, r.b.x, 2 * jp);       // targets in index order: ties keep the lower j
-        one(r.a.y, r.a.w, r.b.y, 2 * jp + 1);
-    }
-    __device__ __forceinline__ void one(float n0, float n1, float n2, int j)
-    {
+        const float2 n0 = make_float2(r.a.x, r.a.y), n1 = make_float2(r.a.z, r.a.w), n2 = make_float2(r.b.x, r.b.y);
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
-            const float d0 = x[ii][0] + n0, d1 = x[ii][1] + n1;
-            float dd;
+            const float2 d0 = fadd2(X[ii][0], n0), d1 = fadd2(X[ii][1], n1);
+            float2 dd;
             if (D == 3) {
-                const float d2 = x[ii][2] + n2;
-                dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+                const float2 d2 = fadd2(X[ii][2], n2);
+                dd = ffma2(d2, d2, ffma2(d1, d1, fmul2(d0, d0)));
             } else {
-                dd = fmaf(d1, d1, d0 * d0);
+                dd = ffma2(d1, d1, fmul2(d0, d0));
             }
             if (K == 1) {
-                if (dd < bd[ii][0]) { bd[ii][0] = dd; bi[ii][0] = j; }
-            } else if (dd < bd[ii][K - 1]) {
-                // sorted insertion; strict comparisons keep the earlier index first on ties
-#pragma unroll
-                for (int q = K - 1; q > 0; --q) {
-                    const bool shift = dd < bd[ii][q - 1];
-                    const bool place = !shift && dd < bd[ii][q];
-                    bd[ii][q] = shift ? bd[ii][q - 1] : (place ? dd : bd[ii][q]);
-                    bi[ii][q] = shift ? bi[ii][q - 1] : (place ? j : bi[ii][q]);
-                }
-                if (dd < bd[ii][0]) { bd[ii][0] = dd; bi[ii][0] = j; }
+                if (dd.x < bd[ii][0]) { bd[ii][0] = dd.x; bi[ii][0] = 2 * jp; }
+                if (dd.y < bd[ii][0]) { bd[ii][0] = dd.y; bi[ii][0] = 2 * jp + 1; }
+            } else if (fminf(dd.x, dd.y) < bd[ii][K - 1]) {
+                insert(ii, dd.x, 2 * jp);
+                insert(ii, dd.y, 2 * jp + 1);
             }
         }
+    }
+    __device__ __forceinline__ void insert(int ii, float dd, int j)
+    {
+        if (!(dd < bd[ii][K - 1])) return;
+        // sorted insertion; strict comparisons keep the earlier index first on ties
+#pragma unroll
+        for (int q = K - 1; q > 0; --q) {
+            const bool shift = dd < bd[ii][q - 1];
+            const bool place = !shift && dd < bd[ii][q];
+            bd[ii][q] = shift ? bd[ii][q - 1] : (place ? dd : bd[ii][q]);
+            bi[ii][q] = shift ? bi[ii][q - 1] : (place ? j : bi[ii][q]);
+        }
+        if (dd < bd[ii][0]) { bd[ii][0] = dd; bi[ii][0] = j; }
     }
     __device__ void fold() {}
     __device__ void finish(const PairArgs& a, int jc, double (&)[NV])
