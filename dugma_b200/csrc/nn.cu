@@ -53,28 +53,37 @@ struct NNBody {
             for (int q = 0; q < K; ++q) { bd[ii][q] = INFINITY; bi[ii][q] = 0x7fffffff; }
     }
     // both targets of a record in one f32x2 sequence (per half the FP32 operations of the
-    // reference: d = x + (-y'), d2 = fmaf(dz,dz, fmaf(dy,dy, dx*dx))), then one test of the
-    // nearer of the two against the k-th distance; the rare insertions take the targets in
-    // index order, so ties keep the lower j
+    // reference: d = x + (-y'), d2 = fmaf(dz,dz, fmaf(dy,dy, dx*dx))), then one test per source
+    // of the nearer of the two against its k-th distance; the rare insertions take the targets
+    // in index order, so ties keep the lower j
     __device__ __forceinline__ void consume(const NNRec2& r, int jp)
     {
         const float2 n0 = make_float2(r.a.x, r.a.y), n1 = make_float2(r.a.z, r.a.w), n2 = make_float2(r.b.x, r.b.y);
+        float2 dd[IPT];
+        bool hit = false;
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
             const float2 d0 = fadd2(X[ii][0], n0), d1 = fadd2(X[ii][1], n1);
-            float2 dd;
             if (D == 3) {
                 const float2 d2 = fadd2(X[ii][2], n2);
-                dd = ffma2(d2, d2, ffma2(d1, d1, fmul2(d0, d0)));
+                dd[ii] = ffma2(d2, d2, ffma2(d1, d1, fmul2(d0, d0)));
             } else {
-                dd = ffma2(d1, d1, fmul2(d0, d0));
+                dd[ii] = ffma2(d1, d1, fmul2(d0, d0));
             }
             if (K == 1) {
-                if (dd.x < bd[ii][0]) { bd[ii][0] = dd.x; bi[ii][0] = 2 * jp; }
-                if (dd.y < bd[ii][0]) { bd[ii][0] = dd.y; bi[ii][0] = 2 * jp + 1; }
-            } else if (fminf(dd.x, dd.y) < bd[ii][K - 1]) {
-                insert(ii, dd.x, 2 * jp);
-                insert(ii, dd.y, 2 * jp + 1);
+                if (dd[ii].x < bd[ii][0]) { bd[ii][0] = dd[ii].x; bi[ii][0] = 2 * jp; }
+                if (dd[ii].y < bd[ii][0]) { bd[ii][0] = dd[ii].y; bi[ii][0] = 2 * jp + 1; }
+            } else {
+                hit |= fminf(dd[ii].x, dd[ii].y) < bd[ii][K - 1];
+            }
+        }
+        // one branch per record for all the sources: the distance arithmetic above stays
+        // branch-free and schedules like the distance-only kernel
+        if (K > 1 && hit) {
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) {
+                insert(ii, dd[ii].x, 2 * jp);
+                insert(ii, dd[ii].y, 2 * jp + 1);
             }
         }
     }
