@@ -70,16 +70,11 @@ struct NNBody {
             } else {
                 dd[ii] = ffma2(d1, d1, fmul2(d0, d0));
             }
-            if (K == 1) {
-                if (dd[ii].x < bd[ii][0]) { bd[ii][0] = dd[ii].x; bi[ii][0] = 2 * jp; }
-                if (dd[ii].y < bd[ii][0]) { bd[ii][0] = dd[ii].y; bi[ii][0] = 2 * jp + 1; }
-            } else {
-                hit |= fminf(dd[ii].x, dd[ii].y) < bd[ii][K - 1];
-            }
+            hit |= fminf(dd[ii].x, dd[ii].y) < bd[ii][K - 1];
         }
         // one branch per record for all the sources: the distance arithmetic above stays
         // branch-free and schedules like the distance-only kernel
-        if (K > 1 && hit) {
+        if (hit) {
 #pragma unroll
             for (int ii = 0; ii < IPT; ++ii) {
                 insert(ii, dd[ii].x, 2 * jp);
