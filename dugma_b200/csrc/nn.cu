@@ -277,20 +277,25 @@ __global__ void __launch_bounds__(NT) nn_kernel(PairArgs a)
 
 
 struct NNVariant {
-    KernelShape shape;           // tj counts records of two targets
-    KernelFn k1, k8, k16, kmin;  // kmin: nearest distance only (sigma)
+    KernelShape shape;   // tj counts records of two targets; ipt is the k = 1 sources per thread
+    KernelFn k1;
+    KernelFn k8;
+    int ipt8;            // sources per thread of the k <= 8 kernel
+    KernelFn k16;
+    int ipt16;           // sources per thread of the k <= 16 kernel
+    KernelFn kmin;       // nearest distance only (sigma)
 };
 
 template <int D>
 static const std::vector<NNVariant>& nn_variants()
 {
     static const std::vector<NNVariant> v = {
-        {{4, 128, 64}, nn_kernel<NNBody<D, 4, 1>, 128, 64>, nn_kernel<NNBody<D, 4, 8>, 128, 64>,
-         nn_kernel<NNBody<D, 2, 16>, 128, 64>, nn_kernel<NNMinBody<D, 4>, 128, 64>},
-        {{8, 128, 64}, nn_kernel<NNBody<D, 8, 1>, 128, 64>, nn_kernel<NNBody<D, 4, 8>, 128, 64>,
-         nn_kernel<NNBody<D, 2, 16>, 128, 64>, nn_kernel<NNMinBody<D, 8>, 128, 64>},
-        {{4, 256, 64}, nn_kernel<NNBody<D, 4, 1>, 256, 64>, nn_kernel<NNBody<D, 2, 8>, 256, 64>,
-         nn_kernel<NNBody<D, 1, 16>, 256, 64>, nn_kernel<NNMinBody<D, 4>, 256, 64>},
+        {{4, 128, 64}, nn_kernel<NNBody<D, 4, 1>, 128, 64>, nn_kernel<NNBody<D, 2, 8>, 128, 64>, 2,
+         nn_kernel<NNBody<D, 1, 16>, 128, 64>, 1, nn_kernel<NNMinBody<D, 4>, 128, 64>},
+        {{8, 128, 64}, nn_kernel<NNBody<D, 8, 1>, 128, 64>, nn_kernel<NNBody<D, 1, 8>, 128, 64>, 1,
+         nn_kernel<NNBody<D, 2, 16>, 128, 64>, 2, nn_kernel<NNMinBody<D, 8>, 128, 64>},
+        {{4, 256, 64}, nn_kernel<NNBody<D, 4, 1>, 256, 64>, nn_kernel<NNBody<D, 2, 8>, 256, 64>, 2,
+         nn_kernel<NNBody<D, 1, 16>, 256, 64>, 1, nn_kernel<NNMinBody<D, 4>, 256, 64>},
     };
     return v;
 }
@@ -320,9 +325,9 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     const bool min_only = K == 1 && !idx_dev && !d2_dev;
     KernelFn fn = min_only ? v->kmin : (K == 1 ? v->k1 : (K == 8 ? v->k8 : v->k16));
     KernelShape sh = v->shape;
-    // the k = 8 / 16 kernels keep fewer sources per thread (see the variant table)
-    if (K == 8) sh.ipt = sh.nt == 128 ? 4 : 2;
-    if (K == 16) sh.ipt = sh.nt == 128 ? 2 : 1;
+    // the k = 8 / 16 kernels may keep fewer sources per thread (see the variant table)
+    if (K == 8) sh.ipt = v->ipt8;
+    if (K == 16) sh.ipt = v->ipt16;
     if (K > 1) {
         // every target chunk restarts the sorted lists, and a list insertion (taken by some lane
         // of a warp far more often than by one thread) costs the whole warp ~4K instructions:
