@@ -377,7 +377,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
         {(void**)&c->pose, sizeof(double) * kPoseDoubles * 2}, {(void**)&c->out, sizeof(double) * 64},
         {(void**)&c->poses, sizeof(double) * kPoseDoubles * kMaxPoses},
         {(void**)&c->err, sizeof(int) * 4},             {(void**)&c->counter, sizeof(int) * 8},
-        {(void**)&c->mom, sizeof(double) * 512},        {(void**)&c->arena_scratch, scratch_bytes},
+        {(void**)&c->mom, sizeof(double) * kMomSlots},        {(void**)&c->arena_scratch, scratch_bytes},
     };
     auto up = [](size_t v) { return (v + 255) / 256 * 256; };
     size_t total = 0;

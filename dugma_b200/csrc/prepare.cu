@@ -80,37 +80,49 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
 }
 
 // max_i log2(w_i) over positive weights (single block, fixed reduction order)
-__global__ void max_log2_kernel(const float* __restrict__ w, int n, double* out)
+// max over the positive weights as float bits (positive floats order like their bit patterns),
+// combined across blocks with atomicMax on an int slot zeroed beforehand: order-independent and
+// so deterministic.  log2 is monotonic, so log2 of the largest weight is the largest log2.
+__global__ void max_weight_kernel(const float* __restrict__ w, int n, int* __restrict__ maxbits)
 {
-    __shared__ double red[1024];
-    double m = -INFINITY;
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if (w[i] > 0.0f) m = fmax(m, log2((double)w[i]));
+    __shared__ int red[256];
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (w[i] > 0.0f) m = max(m, __float_as_int(w[i]));
     red[threadIdx.x] = m;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = red[0];
+    if (threadIdx.x == 0 && red[0] > 0) atomicMax(maxbits, red[0]);
 }
 
-__global__ void norm_log2_kernel(const float* __restrict__ w, int n, const double* Lmax, float* __restrict__ lw)
+// lw_i = log2(w_i) - Lmax with Lmax = log2(largest weight) (-inf when no weight is positive);
+// thread 0 also stores Lmax for the host
+__global__ void norm_log2_kernel(const float* __restrict__ w, int n, const int* __restrict__ maxbits,
+                                 double* __restrict__ Lmax, float* __restrict__ lw)
 {
-    const double L = *Lmax;
+    const int mb = *maxbits;
+    const double L = mb > 0 ? log2((double)__int_as_float(mb)) : -INFINITY;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *Lmax = L;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         lw[i] = w[i] > 0.0f ? __double2float_rn(log2((double)w[i]) - L) : -INFINITY;
 }
 
 // CONV covariance scale: the mean of trace / D over both clouds' covariances (the FP64 staged
-// inputs), rounded to a power of two so that dividing by it is exact in FP32.  One block,
-// fixed order.  scale[0] = the scale, scale[1] = its inverse.
-__global__ void cov_scale_kernel(const double* __restrict__ XC, int n, const double* __restrict__ YC, int m, int D,
-                                 double* __restrict__ scale)
+// inputs), rounded to a power of two so that dividing by it is exact in FP32.  Per-block sums
+// over contiguous slices, then one block over the partials, both in fixed order
+// (deterministic).  scale[0] = the scale, scale[1] = its inverse.
+__global__ void cov_trace_partial_kernel(const double* __restrict__ XC, int n, const double* __restrict__ YC, int m,
+                                         int D, double* __restrict__ part)
 {
-    __shared__ double red[1024];
+    __shared__ double red[256];
+    const int tot = n + m;
+    const int per = (tot + gridDim.x - 1) / gridDim.x;
+    const int b0 = blockIdx.x * per, b1 = min(tot, b0 + per);
     double s = 0;
-    for (int i = threadIdx.x; i < n + m; i += blockDim.x) {
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         const double* C = i < n ? XC + (size_t)i * D * D : YC + (size_t)(i - n) * D * D;
         for (int a = 0; a < D; ++a) s += C[a * (D + 1)];
     }
@@ -120,8 +132,22 @@ __global__ void cov_scale_kernel(const double* __restrict__ XC, int n, const dou
         if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
         __syncthreads();
     }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void cov_scale_kernel(const double* __restrict__ part, int nb, int tot, int D, double* __restrict__ scale)
+{
+    __shared__ double red[256];
+    double s = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
-        const double tr = red[0] / ((double)D * (n + m));
+        const double tr = red[0] / ((double)D * tot);
         const double c = (isfinite(tr) && tr > 0) ? exp2(round(log2(tr))) : 1.0;
         scale[0] = c;
         scale[1] = 1.0 / c;
@@ -153,7 +179,9 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     const int gx = std::min((N + bs - 1) / bs, c.num_sms * 8), gy = std::min((M + bs - 1) / bs, c.num_sms * 8);
     double* Lm = c.out;   // scratch: out[0], out[1] max log2 weights; out[2], out[3] the covariance scale
     // CONV covariances are kept divided by the mean of trace / D over both clouds
-    cov_scale_kernel<<<1, 1024, 0, s>>>(tXC, N, tYC, M, D, Lm + 2);
+    const int nb = std::min(kMomSlots, std::max(1, (N + M + 2047) / 2048));
+    cov_trace_partial_kernel<<<nb, 256, 0, s>>>(tXC, N, tYC, M, D, c.mom);
+    cov_scale_kernel<<<1, 256, 0, s>>>(c.mom, nb, N + M, D, Lm + 2);
     if (D == 3) {
         init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
         init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
@@ -161,10 +189,11 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
         init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
         init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
     }
-    max_log2_kernel<<<1, 1024, 0, s>>>(c.wx, N, Lm);
-    max_log2_kernel<<<1, 1024, 0, s>>>(c.wy, M, Lm + 1);
-    norm_log2_kernel<<<gx, bs, 0, s>>>(c.wx, N, Lm, c.lwx);
-    norm_log2_kernel<<<gy, bs, 0, s>>>(c.wy, M, Lm + 1, c.lwy);
+    // counter[2], counter[3]: the largest weight of each cloud as float bits (zeroed above)
+    max_weight_kernel<<<std::min(gx, 4 * c.num_sms), bs, 0, s>>>(c.wx, N, c.counter + 2);
+    max_weight_kernel<<<std::min(gy, 4 * c.num_sms), bs, 0, s>>>(c.wy, M, c.counter + 3);
+    norm_log2_kernel<<<gx, bs, 0, s>>>(c.wx, N, c.counter + 2, Lm, c.lwx);
+    norm_log2_kernel<<<gy, bs, 0, s>>>(c.wy, M, c.counter + 3, Lm + 1, c.lwy);
     ck(cudaGetLastError(), "init kernels");
     ck(cudaMemcpyAsync(c.host, Lm, 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax, scale");
     ck(cudaMemcpyAsync(c.host + 3, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
