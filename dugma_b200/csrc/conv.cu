@@ -429,7 +429,7 @@ __device__ __forceinline__ float2 fld2(const YRec2& r, int f)
     return (f & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
 }
 
-template <int D, int IPT_, bool GRAD>
+template <int D, int IPT_, bool GRAD, int NT>
 struct PackedConvBody {
     using StreamRec = YRec2;
     static constexpr int IPT = IPT_;
@@ -439,6 +439,15 @@ struct PackedConvBody {
     float2 e[IPT];                               // energy, tile level
     float2 U[IPT][GRAD ? D : 1], UU[IPT][GRAD ? NS : 1], A[IPT][GRAD ? NS : 1];   // item level
     double E64[IPT];
+    // set when a pair of the current tile fails the fast path's test; the tile is then redone
+    // from the item-level sums saved at its start (a per-thread copy in shared memory)
+    bool bad;
+    static constexpr int NCK = GRAD ? IPT * (D + 2 * NS) : 1;
+    __device__ static float2* checkpoint()
+    {
+        __shared__ float2 ck[NCK][NT];
+        return &ck[0][threadIdx.x];
+    }
     int row[IPT];
     float kl;
     double c0, lam, t[3];
@@ -485,6 +494,38 @@ struct PackedConvBody {
 #pragma unroll
                 for (int q = 0; q < NS; ++q) { UU[ii][q] = make_float2(0.f, 0.f); A[ii][q] = make_float2(0.f, 0.f); }
             }
+        }
+        bad = false;
+        save();
+    }
+    __device__ __forceinline__ void save()
+    {
+        if (!GRAD) return;
+        float2* ck = checkpoint();
+        int k = 0;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+#pragma unroll
+            for (int q = 0; q < D; ++q) ck[(k++) * NT] = U[ii][q];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) ck[(k++) * NT] = UU[ii][q];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) ck[(k++) * NT] = A[ii][q];
+        }
+    }
+    __device__ __forceinline__ void restore()
+    {
+        if (!GRAD) return;
+        const float2* ck = checkpoint();
+        int k = 0;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+#pragma unroll
+            for (int q = 0; q < D; ++q) U[ii][q] = ck[(k++) * NT];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) UU[ii][q] = ck[(k++) * NT];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) A[ii][q] = ck[(k++) * NT];
         }
     }
     // One half of a pack the fast path cannot take (near-singular, not positive definite):
@@ -535,7 +576,12 @@ struct PackedConvBody {
         rd = rs * rs;
         Nt = rs * ex2(m * (rd * kl));
     }
-    __device__ __forceinline__ void consume(const YRec2& r, int jrec)
+    __device__ __forceinline__ void consume(const YRec2& r, int jrec) { pass<false>(r, jrec); }
+    // EXACT = false: the fast path for every pair, straight-line, and a flag when any pair fails
+    // its test (results of that tile are then discarded and redone); EXACT = true: a pack with a
+    // failing half goes through rare_half (FP64 when near-singular)
+    template <bool EXACT>
+    __device__ __forceinline__ void pass(const YRec2& r, int jrec)
     {
         float2 ny[3], nl[3], cy[6], oy[3];
 #pragma unroll
@@ -575,7 +621,8 @@ struct PackedConvBody {
             // fast path: both halves positive definite and well conditioned (NaN fails too)
             const float2 dd = fmul2(det, EPS);
             const bool fast = (dd.x >= prod.x) & (dd.y >= prod.y) & (det.x > 0.f) & (det.y > 0.f);
-            if (fast) {
+            if (!EXACT) bad |= !fast;
+            if (!EXACT || fast) {
                 if (D == 3) {
                     h[0] = ffma2(adj[4], d[2], ffma2(adj[3], d[1], fmul2(adj[0], d[0])));
                     h[1] = ffma2(adj[5], d[2], ffma2(adj[1], d[1], fmul2(adj[3], d[0])));
@@ -625,13 +672,21 @@ struct PackedConvBody {
             }
         }
     }
-    __device__ void fold()
+    __device__ void fold_tile(const YRec2* tile, int jbase, int ntile)
     {
+        if (bad) {   // rare: redo this tile with the exact per-pair rules
+            restore();
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) e[ii] = make_float2(0.f, 0.f);
+            for (int jj = 0; jj < ntile; ++jj) pass<true>(tile[jj], jbase + jj);
+            bad = false;
+        }
 #pragma unroll
         for (int ii = 0; ii < IPT; ++ii) {
             E64[ii] += (double)e[ii].x + (double)e[ii].y;
             e[ii] = make_float2(0.f, 0.f);
         }
+        save();
     }
     __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
     {
@@ -676,17 +731,17 @@ template <int D>
 static const std::vector<ConvVariant>& conv_variants(bool grad)
 {
     static const std::vector<ConvVariant> g = {
-        {{1, 64, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 64, 32, 6>},
-        {{1, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 128, 32, 3>},
-        {{1, 128, 64, 2, 512}, conv_kernel<PackedConvBody<D, 1, true>, 128, 64, 2>},
+        {{1, 64, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 64>, 64, 32, 6>},
+        {{1, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 128>, 128, 32, 3>},
+        {{1, 128, 64, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 128>, 128, 64, 2>},
         {{1, 128, 64}, conv_kernel<ConvBody<D, 1, true>, 128, 64>},
         {{2, 128, 64}, conv_kernel<ConvBody<D, 2, true>, 128, 64>},
         {{1, 256, 32}, conv_kernel<ConvBody<D, 1, true>, 256, 32>},
         {{1, 64, 64}, conv_kernel<ConvBody<D, 1, true>, 64, 64>},
     };
     static const std::vector<ConvVariant> e = {
-        {{1, 128, 32, 2}, conv_kernel<PackedConvBody<D, 1, false>, 128, 32, 4>},
-        {{2, 128, 32, 2}, conv_kernel<PackedConvBody<D, 2, false>, 128, 32, 3>},
+        {{1, 128, 32, 2}, conv_kernel<PackedConvBody<D, 1, false, 128>, 128, 32, 4>},
+        {{2, 128, 32, 2}, conv_kernel<PackedConvBody<D, 2, false, 128>, 128, 32, 3>},
         {{2, 128, 64}, conv_kernel<ConvBody<D, 2, false>, 128, 64>},
         {{1, 128, 64}, conv_kernel<ConvBody<D, 1, false>, 128, 64>},
         {{4, 128, 64}, conv_kernel<ConvBody<D, 4, false>, 128, 64>},

@@ -9,6 +9,9 @@
 // and written to its own partial slot, so results do not depend on scheduling.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 
 namespace dugma {
@@ -31,6 +34,14 @@ struct PairArgs {
     int* counter;
     int* err;
 };
+
+// Bodies with a fold_tile(tile, first record index, records) member finish each tile with the
+// tile still in shared memory (work deferred out of the per-record loop); the others have fold().
+template <class B, class R, class = void>
+struct HasTileFold : std::false_type {};
+template <class B, class R>
+struct HasTileFold<B, R, std::void_t<decltype(std::declval<B&>().fold_tile(std::declval<const R*>(), 0, 0))>>
+    : std::true_type {};
 
 template <class Body, int NT, int TJ, int STAGES, int UNROLL = 4>
 __device__ __forceinline__ void run_pairs(const PairArgs& a, Body& body)
@@ -83,7 +94,10 @@ __device__ __forceinline__ void run_pairs(const PairArgs& a, Body& body)
             const Rec* yb = ybuf[st];
 #pragma unroll UNROLL
             for (int jj = 0; jj < TJ; ++jj) body.consume(yb[jj], (tile0 + k) * TJ + jj);
-            body.fold();
+            if constexpr (HasTileFold<Body, Rec>::value)
+                body.fold_tile(yb, (tile0 + k) * TJ, TJ);
+            else
+                body.fold();
             if (__syncthreads_or(!ok)) {
                 // a tile never arrived: drain the copies still in flight (bounded), then stop
                 if (tid == 0)

@@ -79,7 +79,6 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
     }
 }
 
-// max_i log2(w_i) over positive weights (single block, fixed reduction order)
 // max over the positive weights as float bits (positive floats order like their bit patterns),
 // combined across blocks with atomicMax on an int slot zeroed beforehand: order-independent and
 // so deterministic.  log2 is monotonic, so log2 of the largest weight is the largest log2.
