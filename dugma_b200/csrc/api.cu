@@ -342,7 +342,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     c->shape_adj = {4, 64, 64, 2, 512};
     c->shape_energy = {4, 128, 32, 2};
     c->shape_nn = {4, 128, 64};
-    c->shape_conv_adj = {1, 64, 32, 2, 512};
+    c->shape_conv_adj = {2, 64, 32, 2, 512};
     c->shape_conv_energy = {1, 128, 32, 2};
     int rc = DUGMA_OK;
     auto fail = [&](int code) {

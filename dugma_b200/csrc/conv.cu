@@ -731,6 +731,8 @@ template <int D>
 static const std::vector<ConvVariant>& conv_variants(bool grad)
 {
     static const std::vector<ConvVariant> g = {
+        {{2, 64, 32, 2, 512}, conv_kernel<PackedConvBody<D, 2, true, 64>, 64, 32, 4>},
+        {{2, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 2, true, 128>, 128, 32, 2>},
         {{1, 64, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 64>, 64, 32, 6>},
         {{1, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 128>, 128, 32, 3>},
         {{1, 128, 64, 2, 512}, conv_kernel<PackedConvBody<D, 1, true, 128>, 128, 64, 2>},
