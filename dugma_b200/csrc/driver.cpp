@@ -9,9 +9,9 @@
 //   sig <= acc_sig or the iteration limit; sig <- update_sig(R, t).
 // fmincon minimises over a general 3x3 dR with det dR = 1 and dR^T dR = I; here dR =
 // exp([w]x) (2D: a rotation by theta), so the constraints hold by construction and the
-// minimisation is unconstrained over (w, dt): damped Newton steps with the analytic
-// gradient of Q (from the monomial exponents) and a Hessian by central differences of
-// that gradient, with backtracking.
+// minimisation is unconstrained over local coordinates (w, dt) at the current iterate:
+// damped Newton steps with the analytic gradient and Hessian of Q (from the monomial
+// exponents and the derivatives of R <- exp([w]x) R at w = 0), with backtracking.
 // Direct mode (DUGMA_DRIVE_DIRECT): maximise E(R, t) at the current sig with BFGS on the
 // left-perturbation coordinates using the fused adjoint's gradient, then update sig; every
 // evaluation replays one captured CUDA graph (pose prologue, adjoint, reduction).
@@ -141,64 +141,134 @@ struct Surrogate {
             }
         }
     }
+    // Hessian in v (nv x nv, row-major): every unordered pair of factor positions of a monomial
+    // contributes the product of its other factors to both off-diagonal entries (a factor
+    // repeated e times so gets e (e - 1) v^(e - 2) on the diagonal)
+    void hess(const double* v, double* H) const
+    {
+        const std::vector<Mono>& T = mono_table(D);
+        for (int q = 0; q < nv * nv; ++q) H[q] = 0;
+        for (int k = 0; k < K; ++k) {
+            const signed char* f = T[k].f;
+            int n = 0;
+            double x[4];
+            for (; n < 4 && f[n] >= 0; ++n) x[n] = v[f[n]];
+            for (int j = 0; j < n; ++j)
+                for (int l = j + 1; l < n; ++l) {
+                    double m = A[k];
+                    for (int o = 0; o < n; ++o)
+                        if (o != j && o != l) m *= x[o];
+                    H[f[j] * nv + f[l]] += m;
+                    H[f[l] * nv + f[j]] += m;
+                }
+        }
+    }
 };
 
-// parameters p = (w (NR), dt (D)) -> surrogate variables v and the value / gradient in p
-struct SurrogateInP {
+// The surrogate along the pose: v(R, t) = (t, the rows of R) in 3D, (t, cos, sin) in 2D.  Local
+// coordinates p = (dw, dt) at the current pose move it as R <- exp([dw]x) R (2D: a rotation
+// by dw) and t <- t + dt; at p = 0 the gradient and Hessian in p follow from those in v:
+//   g = J^T gv,  H = J^T Hv J + sum_q gv_q d2v_q/dp2,
+// with dR/dw_i = [e_i]x R and d2R/dw_i dw_j = (([e_i]x [e_j]x + [e_j]x [e_i]x) / 2) R.
+struct SurrogatePose {
     Surrogate S;
     int D;
     int np() const { return D == 3 ? 6 : 3; }
-    void to_v(const double* p, double* v, Mat3* dR = nullptr) const
+    void v_of(const Mat3& R, const double* t, double* v) const
     {
         if (D == 3) {
-            const Mat3 R = expso3(p);
-            v[0] = p[3];
-            v[1] = p[4];
-            v[2] = p[5];
+            for (int a = 0; a < 3; ++a) v[a] = t[a];
             for (int r = 0; r < 3; ++r)
                 for (int c = 0; c < 3; ++c) v[3 + 3 * r + c] = R(r, c);   // r11 r12 r13 r21 ... (row-major)
-            if (dR) *dR = R;
         } else {
-            v[0] = p[1];
-            v[1] = p[2];
-            v[2] = std::cos(p[0]);
-            v[3] = std::sin(p[0]);
+            v[0] = t[0];
+            v[1] = t[1];
+            v[2] = R(0, 0);
+            v[3] = R(1, 0);
         }
     }
-    double value(const double* p) const
+    double value(const Mat3& R, const double* t) const
     {
         double v[12];
-        to_v(p, v);
+        v_of(R, t, v);
         return S.value(v);
     }
-    void grad(const double* p, double* g) const
+    static Mat3 skew_unit(int i)
     {
-        double v[12], gv[12];
-        to_v(p, v);
+        Mat3 K{};
+        const int a = (i + 1) % 3, b = (i + 2) % 3;
+        K(b, a) = 1.0;
+        K(a, b) = -1.0;
+        return K;
+    }
+    void derivs(const Mat3& R, const double* t, double* g, double* H) const
+    {
+        const int nv = S.nv, n = np();
+        double v[12], gv[12], Hv[144], J[12 * 6] = {};
+        v_of(R, t, v);
         S.grad(v, gv);
-        if (D == 2) {
-            g[0] = -v[3] * gv[2] + v[2] * gv[3];
-            g[1] = gv[0];
-            g[2] = gv[1];
-            return;
+        S.hess(v, Hv);
+        if (D == 3) {
+            for (int i = 0; i < 3; ++i) {
+                const Mat3 G = mul(skew_unit(i), R);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) J[(3 + 3 * r + c) * n + i] = G(r, c);
+                J[i * n + 3 + i] = 1.0;
+            }
+        } else {
+            J[0 * n + 1] = 1.0;
+            J[1 * n + 2] = 1.0;
+            J[2 * n + 0] = -v[3];   // d cos / d theta
+            J[3 * n + 0] = v[2];    // d sin / d theta
         }
-        // dQ/dw by central differences of the (smooth) map w -> R in the analytic v-gradient
-        const double h = 1e-7;
-        for (int k = 0; k < 3; ++k) {
-            double pp[6], pm[6], vp[12], vm[12];
-            memcpy(pp, p, sizeof(pp));
-            memcpy(pm, p, sizeof(pm));
-            pp[k] += h;
-            pm[k] -= h;
-            to_v(pp, vp);
-            to_v(pm, vm);
+        for (int k = 0; k < n; ++k) {
             double s = 0;
-            for (int q = 3; q < 12; ++q) s += gv[q] * (vp[q] - vm[q]) / (2 * h);
+            for (int q = 0; q < nv; ++q) s += J[q * n + k] * gv[q];
             g[k] = s;
         }
-        g[3] = gv[0];
-        g[4] = gv[1];
-        g[5] = gv[2];
+        double HJ[12 * 6];
+        for (int q = 0; q < nv; ++q)
+            for (int l = 0; l < n; ++l) {
+                double s = 0;
+                for (int r = 0; r < nv; ++r) s += Hv[q * nv + r] * J[r * n + l];
+                HJ[q * n + l] = s;
+            }
+        for (int k = 0; k < n; ++k)
+            for (int l = 0; l < n; ++l) {
+                double s = 0;
+                for (int q = 0; q < nv; ++q) s += J[q * n + k] * HJ[q * n + l];
+                H[k * n + l] = s;
+            }
+        if (D == 3) {
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const Mat3 Ki = skew_unit(i), Kj = skew_unit(j);
+                    const Mat3 A = mul(mul(Ki, Kj), R), B = mul(mul(Kj, Ki), R);
+                    double s = 0;
+                    for (int r = 0; r < 3; ++r)
+                        for (int c = 0; c < 3; ++c) s += gv[3 + 3 * r + c] * 0.5 * (A(r, c) + B(r, c));
+                    H[i * n + j] += s;
+                }
+        } else {
+            H[0] -= gv[2] * v[2] + gv[3] * v[3];   // d2 cos = -cos, d2 sin = -sin
+        }
+    }
+    void step(const Mat3& R, const double* t, const double* x, Mat3& Rn, double* tn) const
+    {
+        if (D == 3) {
+            Rn = mul(expso3(x), R);
+            for (int a = 0; a < 3; ++a) tn[a] = t[a] + x[3 + a];
+        } else {
+            const double th = std::atan2(R(1, 0), R(0, 0)) + x[0];
+            Rn = Mat3{};
+            Rn(0, 0) = std::cos(th);
+            Rn(1, 0) = std::sin(th);
+            Rn(0, 1) = -std::sin(th);
+            Rn(1, 1) = std::cos(th);
+            Rn(2, 2) = 1.0;
+            tn[0] = t[0] + x[1];
+            tn[1] = t[1] + x[2];
+        }
     }
 };
 
@@ -229,31 +299,24 @@ bool solve(int n, std::vector<double> H, std::vector<double> b, std::vector<doub
     return true;
 }
 
-// Damped Newton minimisation of the surrogate from p = 0; returns the exit flag (> 0 converged,
+// Damped Newton minimisation of the surrogate from dR = I, dt = 0 in local coordinates (analytic
+// gradient and Hessian, trust region 0.5, backtracking); returns the exit flag (> 0 converged,
 // 0 iteration limit, < 0 failure as fmincon's exitflag).
-int minimise_surrogate(const SurrogateInP& F, std::vector<double>& p, int* evals)
+int minimise_surrogate(const SurrogatePose& F, Mat3& R, double* t, int* evals)
 {
     const int n = F.np();
-    p.assign(n, 0.0);
-    double f = F.value(p.data());
+    R = Mat3{};
+    R(0, 0) = R(1, 1) = R(2, 2) = 1.0;
+    t[0] = t[1] = t[2] = 0.0;
+    double f = F.value(R, t);
     if (!std::isfinite(f)) return -1;
     double lam = 0;
     for (int it = 0; it < 100; ++it) {
         std::vector<double> g(n), H(n * n);
-        F.grad(p.data(), g.data());
+        F.derivs(R, t, g.data(), H.data());
         double gn = 0;
         for (double v : g) gn += v * v;
         gn = std::sqrt(gn);
-        // Hessian by central differences of the gradient
-        for (int k = 0; k < n; ++k) {
-            const double h = 1e-5;
-            std::vector<double> pp = p, pm = p, gp(n), gm(n);
-            pp[k] += h;
-            pm[k] -= h;
-            F.grad(pp.data(), gp.data());
-            F.grad(pm.data(), gm.data());
-            for (int r = 0; r < n; ++r) H[r * n + k] = (gp[r] - gm[r]) / (2 * h);
-        }
         for (int r = 0; r < n; ++r)
             for (int c = r + 1; c < n; ++c) H[r * n + c] = H[c * n + r] = 0.5 * (H[r * n + c] + H[c * n + r]);
         double hmax = 0;
@@ -272,17 +335,19 @@ int minimise_surrogate(const SurrogateInP& F, std::vector<double>& p, int* evals
             double step = 0;
             for (double v : x) step += v * v;
             step = std::sqrt(step);
-            if (step > 0.5) {   // trust region on the rotation vector / translation
+            if (step > 0.5) {   // trust region on the rotation increment / translation
                 for (double& v : x) v *= 0.5 / step;
                 step = 0.5;
             }
-            std::vector<double> pn(n);
-            for (int r = 0; r < n; ++r) pn[r] = p[r] + x[r];
-            const double fn = F.value(pn.data());
+            Mat3 Rn;
+            double tn[3] = {0, 0, 0};
+            F.step(R, t, x.data(), Rn, tn);
+            const double fn = F.value(Rn, tn);
             ++*evals;
             if (std::isfinite(fn) && fn <= f) {
                 const double df = f - fn;
-                p = pn;
+                R = Rn;
+                for (int a = 0; a < 3; ++a) t[a] = tn[a];
                 f = fn;
                 lam = std::max(lam * 0.3, 1e-15 * std::max(hmax, 1e-300));
                 accepted = true;
@@ -309,27 +374,19 @@ struct Timer {
 extern "C" int dugma_minimise_surrogate(int D, const double* A, double* dR, double* dt, double* Qmin, int* exitflag)
 {
     if ((D != 2 && D != 3) || !A || !dR || !dt) return DUGMA_ERR_ARG;
-    SurrogateInP F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
-                    D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
-                   D};
-    std::vector<double> p;
+    SurrogatePose F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
+                     D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
+                    D};
+    Mat3 Rm;
+    double tv[3];
     int evals = 0;
-    const int flag = minimise_surrogate(F, p, &evals);
+    const int flag = minimise_surrogate(F, Rm, tv, &evals);
     if (exitflag) *exitflag = flag;
     if (flag < 0) return DUGMA_ERR_NUMERIC;
-    if (D == 3) {
-        const Mat3 Q = expso3(p.data());
-        memcpy(dR, Q.a, sizeof(Q.a));
-        for (int a = 0; a < 3; ++a) dt[a] = p[3 + a];
-    } else {
-        dR[0] = std::cos(p[0]);
-        dR[1] = std::sin(p[0]);
-        dR[2] = -std::sin(p[0]);
-        dR[3] = std::cos(p[0]);
-        dt[0] = p[1];
-        dt[1] = p[2];
-    }
-    if (Qmin) *Qmin = F.value(p.data());
+    for (int c = 0; c < D; ++c)
+        for (int r = 0; r < D; ++r) dR[r + D * c] = Rm(r, c);
+    for (int a = 0; a < D; ++a) dt[a] = tv[a];
+    if (Qmin) *Qmin = F.value(Rm, tv);
     return DUGMA_OK;
 }
 
@@ -406,24 +463,16 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
             double A[640];
             rc = dugma_compi(Ptr, R, t, &Nd, &Md, &Dd, &sig, A);
             if (rc != DUGMA_OK) break;
-            SurrogateInP F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
-                            D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
-                           D};
-            std::vector<double> p;
-            exitflag = minimise_surrogate(F, p, &evals);
+            SurrogatePose F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
+                             D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
+                            D};
+            Mat3 Q;
+            double tq[3];
+            exitflag = minimise_surrogate(F, Q, tq, &evals);
             if (exitflag < 0) break;
-            if (D == 3) {
-                const Mat3 Q = expso3(p.data());
-                memcpy(dRm, Q.a, sizeof(Q.a));
-                for (int a = 0; a < 3; ++a) dt[a] = p[3 + a];
-            } else {
-                dRm[0] = std::cos(p[0]);
-                dRm[1] = std::sin(p[0]);
-                dRm[2] = -std::sin(p[0]);
-                dRm[3] = std::cos(p[0]);
-                dt[0] = p[1];
-                dt[1] = p[2];
-            }
+            for (int c = 0; c < D; ++c)
+                for (int r = 0; r < D; ++r) dRm[r + D * c] = Q(r, c);
+            for (int a = 0; a < D; ++a) dt[a] = tq[a];
         } else {
             // BFGS ascent of E on the left-perturbation coordinates at fixed sig
             const int n = NR + D;
