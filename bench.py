@@ -164,20 +164,25 @@ def eval_pose(P, unit):
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples during the timed region (one reading right after it when the region is
+    shorter than the sampler's start-up, marked in the summary)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, path, index):
         self.path, self.index = path, index
         self.p = None
+        self.window = "timed region"
+
+    def _cmd(self):
+        return ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"]
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
         try:
             self.f = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+            self.p = subprocess.Popen(self._cmd() + ["-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
@@ -190,6 +195,14 @@ class Clocks:
             except Exception:
                 self.p.kill()
             self.f.close()
+            try:
+                empty = not open(self.path).read().strip()
+                if empty:
+                    with open(self.path, "w") as f:
+                        subprocess.run(self._cmd(), stdout=f, stderr=subprocess.DEVNULL, timeout=30)
+                    self.window = "right after the timed region (shorter than the sampler's start-up)"
+            except Exception:
+                pass
 
     def summary(self):
         try:
@@ -207,7 +220,7 @@ class Clocks:
                 if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "window": self.window}
 
 
 def cpu_rate(P, R, t, sig, model=0, budget_s=8.0):
@@ -328,20 +341,35 @@ def run_batch(args, rank, world):
         b.energy_grad(R, t, sig)
     torch.cuda.synchronize()
     steps = max(3, min(args.steps, 20))
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        E, g = b.energy_grad(R, t, sig)
-    el = time.perf_counter() - t0
+    import tempfile
+    with Clocks(os.path.join(tempfile.gettempdir(), f"dugma_clocks_batch_rank{rank}.csv"),
+                torch.cuda.current_device()) as clk:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            E, g = b.energy_grad(R, t, sig)
+        el = time.perf_counter() - t0
     b.close()
     tot = all_reduce([pairs], "sum") + all_reduce([el], "max")
     if rank == 0:
-        line = {"metric": "energy+grad pair-terms/s", "value": float(tot[0]) * steps / float(tot[1]),
+        value = float(tot[0]) * steps / float(tot[1])
+        n_pose = len(mine) * Q
+        line = {"metric": "energy+grad pair-terms/s", "value": value,
                 "unit": "pair-terms/s", "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup),
                 "ms_per_step": float(tot[1]) / steps * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "batch256x32: 256 problems, N, M uniform in [500, 8000], 32 rotations of a "
                                        "uniform SO(3) grid each, one evaluation per step (host poses in, E and g out)",
-                           "pair_terms_per_step": int(tot[0])}}
+                           "pair_terms_per_step": int(tot[0]),
+                           "timing": "wall clock around the synchronous batch call, max over ranks",
+                           "l2": "inputs of all problems (records) stay resident; no flush"},
+                # the batch call takes host poses and returns host results, so the timed steps are
+                # already end to end (rank 0's bytes)
+                "e2e": {"value": value, "unit": "pair-terms/s", "h2d_bytes_per_step": 8 * 13 * n_pose,
+                        "d2h_bytes_per_step": 8 * (1 + g.shape[-1]) * n_pose},
+                "gpu_launches": 3 * steps}
+        clocks = clk.summary()
+        if clocks:
+            line["clocks"] = clocks
         print(json.dumps(line), flush=True)
 
 

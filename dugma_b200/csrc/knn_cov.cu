@@ -106,37 +106,40 @@ extern "C" int dugma_knn_covariance(const double* points, int n, int D, int k, d
     double* covd = nullptr;
     double* ptsd = nullptr;   // FP64 copy: neighbour sets come from FP32 distances, moments from FP64
     const double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, ident2[4] = {1, 0, 0, 1};
+    cudaStream_t s = c->stream;
     do {
-        double h[16] = {0};
+        // the pose block goes through the context's pinned staging (stream-ordered copy)
+        double* h = c->host;
+        for (int q = 0; q < 16; ++q) h[q] = 0.0;
         for (int q = 0; q < D * D; ++q) h[q] = D == 3 ? ident[q] : ident2[q];
         h[kPoseSig] = 1.0;
-        if (cudaMemcpy(c->pose, h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMalloc(&idx, sizeof(int) * (size_t)n * kk) != cudaSuccess ||
-            cudaMalloc(&d2, sizeof(float) * (size_t)n * kk) != cudaSuccess ||
-            cudaMalloc(&covd, sizeof(double) * (size_t)n * D * D) != cudaSuccess ||
-            cudaMalloc(&ptsd, sizeof(double) * (size_t)n * D) != cudaSuccess ||
-            cudaMemcpy(ptsd, points, sizeof(double) * (size_t)n * D, cudaMemcpyHostToDevice) != cudaSuccess) {
+        if (cudaMemcpyAsync(c->pose, h, sizeof(double) * 16, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMallocAsync(&idx, sizeof(int) * (size_t)n * kk, s) != cudaSuccess ||
+            cudaMallocAsync(&d2, sizeof(float) * (size_t)n * kk, s) != cudaSuccess ||
+            cudaMallocAsync(&covd, sizeof(double) * (size_t)n * D * D, s) != cudaSuccess ||
+            cudaMallocAsync(&ptsd, sizeof(double) * (size_t)n * D, s) != cudaSuccess ||
+            cudaMemcpyAsync(ptsd, points, sizeof(double) * (size_t)n * D, cudaMemcpyHostToDevice, s) != cudaSuccess) {
             cudaGetLastError();
             rc = set_error(DUGMA_ERR_NOMEM, "knn_covariance: device allocation failed");
             break;
         }
-        rc = launch_nn(*c, c->pose, kk, idx, d2, c->stream);
+        rc = launch_nn(*c, c->pose, kk, idx, d2, s);
         if (rc != DUGMA_OK) break;
         const int g = std::min((n + 127) / 128, c->num_sms * 8);
         if (D == 3)
-            knn_cov_kernel<3><<<g, 128, 0, c->stream>>>(ptsd, idx, n, kk, lo, hi, covd);
+            knn_cov_kernel<3><<<g, 128, 0, s>>>(ptsd, idx, n, kk, lo, hi, covd);
         else
-            knn_cov_kernel<2><<<g, 128, 0, c->stream>>>(ptsd, idx, n, kk, lo, hi, covd);
+            knn_cov_kernel<2><<<g, 128, 0, s>>>(ptsd, idx, n, kk, lo, hi, covd);
         if (cudaGetLastError() != cudaSuccess ||
-            cudaMemcpyAsync(cov, covd, sizeof(double) * (size_t)n * D * D, cudaMemcpyDeviceToHost, c->stream) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            cudaMemcpyAsync(cov, covd, sizeof(double) * (size_t)n * D * D, cudaMemcpyDeviceToHost, s) != cudaSuccess)
             rc = set_error(DUGMA_ERR_CUDA, "knn_covariance: kernel failed");
     } while (false);
-    if (idx) cudaFree(idx);
-    if (d2) cudaFree(d2);
-    if (covd) cudaFree(covd);
-    if (ptsd) cudaFree(ptsd);
+    if (idx) cudaFreeAsync(idx, s);
+    if (d2) cudaFreeAsync(d2, s);
+    if (covd) cudaFreeAsync(covd, s);
+    if (ptsd) cudaFreeAsync(ptsd, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == DUGMA_OK)
+        rc = set_error(DUGMA_ERR_CUDA, "knn_covariance: kernel failed");
     dugma_fr_m(Ptr);
     return rc;
 }
