@@ -6,7 +6,7 @@
 //   y'_j = float(FP64(R y_j + t))               (update_sig.cu:247-252, written by the prologue)
 //   d    = x_i - y'_j in FP32,  d2 = fmaf(dz,dz, fmaf(dy,dy, dx*dx))
 // Target records hold two targets each, coordinates negated (d = x + (-y') is the same FP32
-// value), interleaved so that the sigma kernel evaluates both with f32x2 operations.
+// value), interleaved so that the search kernels evaluate both with f32x2 operations.
 //   the k smallest (d2, j) in lexicographic order are kept in registers (ties -> lowest j)
 // Targets are streamed by bulk copy like the energy kernels; target chunks are merged in
 // index order afterwards, so the result is exact and deterministic.  sigma is then
