@@ -15,8 +15,11 @@
 // with axial(A) = (A12 - A21, A20 - A02, A01 - A10) (2D: A01 - A10).  Both extra terms are
 // linear in per-source sums over targets, so the kernel accumulates per source
 //   E~ = sum N~,  U = sum N~ u~,  UU = sum N~ u~ u~^T,  A = sum N~ St^-1     (u~ = St^-1 d)
-// and contracts them with St_x once per source.  Per pair (3D): 44 FP32 for N~ and 20 for
-// the moments, 2 SFU (rsqrt, ex2).
+// and contracts them with St_x once per source.  Per pair (3D): 48 FP32 for N~ and its sum
+// (with the singularity test), 20 for the moments, 2 SFU (rsqrt, ex2).
+// The packed kernels run every pair of a tile through the FP32 fast path without a branch
+// and only flag a pair that fails the test; a flagged tile is redone from the per-source
+// sums saved at its start with the exact per-pair rules, so the common case is straight-line.
 #include <cmath>
 
 #include "context.hpp"
