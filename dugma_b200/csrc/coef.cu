@@ -31,15 +31,40 @@ __host__ __device__ inline void monomials(const double* p, double* f)
 }
 
 // ---------------------------------------------------------------------------
+// Packed form: the streamed side as pair records (256 B, two points per f32x2 operation).
+// Field f (0..31) of a Rec256 is the float2 (field f of point 2p, field f of point 2p+1) of
+// the Rec128 layout read as 32 floats, with the coordinates (fields 0-2 hi, 4-6 lo) negated
+// so that d = (hi_s + f0) + (lo_s + f4) needs only packed adds; field 3 is the log2 weight,
+// 8..13 the matrix, 16.. the monomials.  The prologue writes each point's half of its pair
+// record next to its Rec128.
+// ---------------------------------------------------------------------------
+struct __align__(16) Rec256 {
+    float4 q[16];   // q[k] = (field 2k even, field 2k odd, field 2k+1 even, field 2k+1 odd)
+};
+
+// point j's record r into its half (j & 1) of pair record j / 2
+__device__ __forceinline__ void write_pair_half(Rec256* __restrict__ out, int j, const Rec128& r)
+{
+    const float* a = reinterpret_cast<const float*>(&r);
+    float* o = reinterpret_cast<float*>(out + (j >> 1));
+    const int h = j & 1;
+#pragma unroll
+    for (int f = 0; f < 32; ++f) {
+        const bool neg = f <= 2 || (f >= 4 && f <= 6);
+        o[(f >> 1) * 4 + (f & 1) * 2 + h] = neg ? -a[f] : a[f];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Records: y side (v0 = y'hi, lv; v1 = y'lo; v2/v3 = k C'_j Horner-packed; g = monomials of y')
 //          x side (v0 = x, lw; v1 = 0;     v2/v3 = k B_i Horner-packed;  g = monomials of x)
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void coef_prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
                                      const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
-                                     Rec128* __restrict__ yr, const float* __restrict__ x,
+                                     Rec128* __restrict__ yr, Rec256* __restrict__ yr2, const float* __restrict__ x,
                                      const float* __restrict__ xinv, const float* __restrict__ lwx, int N, int N_pad,
-                                     Rec128* __restrict__ xr)
+                                     Rec128* __restrict__ xr, Rec256* __restrict__ xr2)
 {
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
     double R[9], t[3];
@@ -89,6 +114,7 @@ __global__ void coef_prologue_kernel(const double* __restrict__ pose, const floa
         r.v3 = D == 3 ? make_float4(cp[4], cp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
         for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(g[q]) : 0.f;
         yr[j] = r;
+        write_pair_half(yr2, j, r);
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
         Rec128 r;
@@ -117,46 +143,7 @@ __global__ void coef_prologue_kernel(const double* __restrict__ pose, const floa
         r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
         for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(f[q]) : 0.f;
         xr[i] = r;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Packed form: the streamed side as pair records (256 B, two points per f32x2 operation).
-// Field f (0..31) of a Rec256 is the float2 (field f of point 2p, field f of point 2p+1) of
-// the Rec128 layout read as 32 floats, with the coordinates (fields 0-2 hi, 4-6 lo) negated
-// so that d = (hi_s + f0) + (lo_s + f4) needs only packed adds; field 3 is the log2 weight,
-// 8..13 the matrix, 16.. the monomials.
-// ---------------------------------------------------------------------------
-struct __align__(16) Rec256 {
-    float4 q[16];   // q[k] = (field 2k even, field 2k odd, field 2k+1 even, field 2k+1 odd)
-};
-
-// pairs the records of both sides in one launch: pairs [0, n_pairs_a) of `in_a`, then those of `in_b`
-__global__ void pair_rec128_kernel(const Rec128* __restrict__ in_a, int n_pairs_a, Rec256* __restrict__ out_a,
-                                   const Rec128* __restrict__ in_b, int n_pairs_b, Rec256* __restrict__ out_b)
-{
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_pairs_a + n_pairs_b; k += gridDim.x * blockDim.x) {
-        const bool first = k < n_pairs_a;
-        const int p = first ? k : k - n_pairs_a;
-        const Rec128* in = first ? in_a : in_b;
-        Rec256* out = first ? out_a : out_b;
-        const float* a = reinterpret_cast<const float*>(in + 2 * p);
-        const float* b = reinterpret_cast<const float*>(in + 2 * p + 1);
-        Rec256 r;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            float v[4] = {a[2 * k], b[2 * k], a[2 * k + 1], b[2 * k + 1]};
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int f = 2 * k + h;
-                if (f <= 2 || (f >= 4 && f <= 6)) {
-                    v[2 * h] = -v[2 * h];
-                    v[2 * h + 1] = -v[2 * h + 1];
-                }
-            }
-            r.q[k] = make_float4(v[0], v[1], v[2], v[3]);
-        }
-        out[p] = r;
+        write_pair_half(xr2, i, r);
     }
 }
 
@@ -453,7 +440,8 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     DUGMA_RET(c.ensure_coef_records());
     const int n = std::max(c.M_pad, c.N_pad);
     coef_prologue_kernel<D><<<std::min((n + 255) / 256, c.num_sms * 4), 256, 0, s>>>(
-        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128);
+        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx,
+        c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256));
     DUGMA_CK(cudaGetLastError());
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
@@ -472,13 +460,6 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
                             : coef_pass_kernel<PackedCoefBody<D, 2, false>, 64, 16, 6>;
         return big ? KernelShape{2, 128, 16, 2, 0, min_chunk} : KernelShape{2, 64, 16, 2, 0, min_chunk};
     };
-    {
-        const int np = (c.M_pad + c.N_pad) / 2;
-        const int g = std::min((np + 255) / 256, c.num_sms * 4);
-        pair_rec128_kernel<<<g, 256, 0, s>>>(c.yrec128, c.M_pad / 2, static_cast<Rec256*>(c.yrec256), c.xrec128,
-                                             c.N_pad / 2, static_cast<Rec256*>(c.xrec256));
-        DUGMA_CK(cudaGetLastError());
-    }
     // blocks of the moments kernel: about 32 rows each, at most 2 per SM (the partial buffer's size)
     const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(i1 - i0, j1 - j0) + 31) / 32));
     double* mom = c.mom_part;
