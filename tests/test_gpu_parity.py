@@ -250,6 +250,42 @@ def test_conv_near_singular_pairs_use_fp64_inverse():
         api.fr_m(h)
 
 
+@pytest.mark.parametrize("D", [3, 2])
+def test_conv_few_near_singular_targets(D):
+    """A handful of near-singular targets among thousands: most tiles of the packed CONV kernels
+    stay on the straight-line fast path, a few are redone exactly from the sums saved at their
+    start, so the saved sums must carry over correctly between fast and redone tiles."""
+    rng = np.random.default_rng(17)
+    n, m = 700, 3001
+    X = rng.standard_normal((n, D)) * 0.4
+    Y = X[rng.integers(0, n, m)] + 0.02 * rng.standard_normal((m, D))
+    v = np.ones(D) / np.sqrt(D)
+    XC = np.tile(np.eye(D) * 2e-3, (n, 1, 1))
+    YC = np.tile(np.eye(D) * 2e-3, (m, 1, 1))
+    rare = np.array([5, 6, 1000, 2047, 2999])
+    # rank-one plus a tiny floor, on both sides of the pairs it meets: near-singular combined
+    # covariances for the sources that are degenerate along the same direction
+    YC[rare] = np.eye(D) * 1e-10 + 1e-2 * np.outer(v, v)
+    XC[:40] = np.eye(D) * 1e-10 + 1e-2 * np.outer(v, v)
+    st = orc.State(X, XC, Y, YC)
+    _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D, seed=4, scale=0.05)
+        for sig in (0.3, 1.0):
+            Eo, go, dxo = st.energy_conv(R, t, sig, with_dx=True)
+            for shape in api.shapes(3):
+                api.set_shape(h, 3, shape)
+                E, g, dx = api.energy_grad(h, R, t, sig, model=1, with_dx=True)
+                assert abs(E - Eo) <= 1e-5 * Eo, (shape, E, Eo)
+                assert _rel(g, go) <= 1e-4, shape
+                assert _rel(dx, dxo) <= 1e-3, shape
+            for shape in api.shapes(4):
+                api.set_shape(h, 4, shape)
+                assert abs(api.energy(h, R, t, sig, model=1) - Eo) <= 1e-5 * Eo, shape
+    finally:
+        api.fr_m(h)
+
+
 def test_energy_adjoint_workload1_ill_conditioned():
     P = synth.workload1()
     st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
