@@ -16,10 +16,14 @@ e2e         the same metric through the C ABI with host buffers: dugma_init (FP6
 roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instructions per
             pair x pairs per launch / launch time from CUDA events inside the library)
             against the FP32 fused-multiply-add rate measured in this run.
-plain_fd    the plain form: energy + central finite differences (13 energy evaluations).
+plain_fd    the plain form: energy + central finite differences (13 energy evaluations, 7 in 2D).
 cpu_baseline  the FP64 C/OpenMP oracle on a bounded sample of source rows, all host cores.
 accuracy    this run's relative error against that FP64 oracle on the same sampled rows
             (energy and the pose gradient of source rows [0, rows) over all targets).
+
+Workloads (--workload): 0 1K sphere, 1 6K sphere with outliers, 2 the 64K harmonic surface
+(default), 3 256 problems x 32 poses in one persistent launch, 4 300K depth views, 5 the 2D
+path on two 64K samples of a closed curve.
 
 With --poses P a step evaluates P multistart poses of the problem back to back (one
 launch sequence per pose); the depth-camera workload is quoted with P = 64.  The
@@ -46,6 +50,8 @@ sys.path.insert(0, ROOT)
 # REF adjoint: d 6, u = kC'd 9, d.u 3, B exponent (Horner) 9, energy 2, S1 += e1 u 3, w = e2 d 3,
 # D2 += w 3, Q2 += w d^T 6
 FP32_INSTR_ADJOINT = 44
+# REF adjoint in 2D: d 4, u 4, d.u 2, B exponent (Horner) 3 + 2, energy 2, S1 2, w 2, D2 2, Q2 3
+FP32_INSTR_ADJOINT_2D = 26
 # CONV adjoint: d 6, S = Sx + C'y 6, adjugate 12, det 3, singularity test 3, h = adj d 9, d.h 3,
 # exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
 FP32_INSTR_CONV_ADJOINT = 68
@@ -154,10 +160,13 @@ def hbm_view(bytes_per_launch, kernel_ms):
 
 def eval_pose(P, unit):
     """Multistart pose number `unit`: ground truth perturbed by a seeded 10 deg, 2 cm offset."""
-    from dugma_b200.pose import expmap
+    from dugma_b200.pose import expmap, rot2d
     rng = np.random.default_rng(100 + unit)
-    ax = rng.standard_normal(3)
+    D = P.X.shape[1]
+    ax = rng.standard_normal(D)
     ax /= np.linalg.norm(ax)
+    if D == 2:
+        return P.R_G @ rot2d(np.radians(10.0) * np.sign(ax[0])), P.t_G + 0.02 * ax
     R = P.R_G @ expmap(ax * np.radians(10.0))
     t = P.t_G + 0.02 * ax
     return R, t
@@ -396,6 +405,10 @@ def main():
     L = _lib.load(build_if_missing=False)
 
     P = workload(args.workload, args.n)
+    D = P.X.shape[1]
+    ng = 6 if D == 3 else 3
+    if D == 2 and args.model == 1:
+        raise SystemExit("the CONV model is measured on the 3D workloads")
     R, t = eval_pose(P, rank * max(1, args.poses))
     _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
     sig = api.update_sig(h, R, t)
@@ -425,8 +438,8 @@ def main():
     pose = torch.zeros(npose, 16, dtype=torch.float64, device="cuda")
     for k in range(npose):
         Rk, tk = (R, t) if k == 0 else eval_pose(P, rank * npose + k)
-        pose[k, :9] = torch.tensor(np.asarray(Rk).T.reshape(-1))
-        pose[k, 9:12] = torch.tensor(tk)
+        pose[k, :D * D] = torch.tensor(np.asarray(Rk).T.reshape(-1))
+        pose[k, 9:9 + D] = torch.tensor(tk)
         pose[k, 12] = sig
     out = torch.zeros(npose, 8, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -480,13 +493,13 @@ def main():
     sfu = ctypes.c_double(0)
     L.dugma_calibrate(1, ctypes.byref(sfu), None)
     kernel_ms = kms.value / max(kl.value, 1)
-    instr = FP32_INSTR_ADJOINT if args.model == 0 else FP32_INSTR_CONV_ADJOINT
+    instr = (FP32_INSTR_ADJOINT if D == 3 else FP32_INSTR_ADJOINT_2D) if args.model == 0 else FP32_INSTR_CONV_ADJOINT
     achieved = instr * pairs / (kernel_ms * 1e-3)
     sfu_frac = SFU_PER_PAIR * pairs / (kernel_ms * 1e-3) / sfu.value if sfu.value else None
 
     extra = {}
     if not args.no_fd and rank == 0:
-        # plain form: energy + central FD over 6 pose coordinates (13 energy evaluations)
+        # plain form: energy + central FD over the pose coordinates (13 energy evaluations in 3D, 7 in 2D)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         api.energy_fd_grad(h, R, t, sig, model=args.model)
@@ -500,7 +513,7 @@ def main():
         adj_ms = ms / (args.steps * npose)
         extra["plain_fd"] = {"ms_per_gradient": fd_ms, "evals_per_s": 1e3 / fd_ms,
                              "adjoint_evals_per_s": 1e3 / adj_ms, "adjoint_speedup": fd_ms / adj_ms,
-                             "energy_evals_per_gradient": 13}
+                             "energy_evals_per_gradient": 1 + 2 * ng}
         if args.model == 0:
             # the same at the reference's per-pair precision (FP64 d, quadratic forms and exp)
             api.energy_fd_grad(h, R, t, sig, model=2)
@@ -513,7 +526,7 @@ def main():
                 fd64.append(t0.elapsed_time(t1))
             fd64_ms = min(fd64)
             extra["plain_fd"].update({"fp64_ms_per_gradient": fd64_ms,
-                                      "fp64_energy_pair_terms_per_s": 13 * pairs / (fd64_ms * 1e-3),
+                                      "fp64_energy_pair_terms_per_s": (1 + 2 * ng) * pairs / (fd64_ms * 1e-3),
                                       "adjoint_speedup_vs_fp64": fd64_ms / adj_ms})
 
     e2e = None
@@ -550,7 +563,7 @@ def main():
         el = all_reduce([el], "max")[0]
         e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "host_memory": "pinned",
                "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": 8 * 7 + 4, "steps": ksteps,
+               "d2h_bytes_per_step": 8 * (1 + ng) + 4, "steps": ksteps,
                "ms_per_step": {"init": 1e3 * ph[0] / ksteps, "energy_grad": 1e3 * ph[1] / ksteps,
                                "fr_m": 1e3 * ph[2] / ksteps}}
 
@@ -589,7 +602,7 @@ def main():
                          "instr_per_pair": instr,
                          "hbm_view": hbm_view(64 * (P.N + P.M), kernel_ms)},
             "gpu_launches": 3 * args.steps * npose,
-            "result": {"E": float(res[0]), "g": [float(v) for v in res[1:7]]},
+            "result": {"E": float(res[0]), "g": [float(v) for v in res[1:1 + ng]]},
             "autotune": tune,
             "autotune_energy": tune_energy,
         }

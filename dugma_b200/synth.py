@@ -329,4 +329,44 @@ def kinect_like(trial: int = 0) -> Problem:
     return Problem(X, Y, XC, YC, Rv, tv, f"twoview{trial}")
 
 
-WORKLOADS = {0: workload0, 1: workload1, 2: workload2, 4: workload4}
+def curve_shape(rng: np.random.Generator, n_bumps: int = 6, amp: float = 0.08):
+    """A closed curve r(a) = 1 + sum_k c_k sin(k a + p_k), k = 1..n_bumps: returns (c, p)."""
+    return rng.uniform(-amp, amp, n_bumps), rng.uniform(0.0, 2.0 * np.pi, n_bumps)
+
+
+def curve_points(shape, a: np.ndarray):
+    """Points of the curve at angles a, with the unit tangent at each."""
+    c, ph = shape
+    k = np.arange(1, len(c) + 1)
+    r = 1.0 + np.sin(np.outer(a, k) + ph) @ c
+    dr = np.cos(np.outer(a, k) + ph) @ (c * k)
+    P = np.stack([r * np.cos(a), r * np.sin(a)], axis=1)
+    T = np.stack([dr * np.cos(a) - r * np.sin(a), dr * np.sin(a) + r * np.cos(a)], axis=1)
+    return P, T / np.linalg.norm(T, axis=1, keepdims=True)
+
+
+def _tangent_cov(T: np.ndarray, s_t: float, s_n: float) -> np.ndarray:
+    """Covariance s_t^2 t t^T + s_n^2 n n^T per point (t the tangent, n its normal)."""
+    N = np.stack([-T[:, 1], T[:, 0]], axis=1)
+    return s_t ** 2 * T[:, :, None] * T[:, None, :] + s_n ** 2 * N[:, :, None] * N[:, None, :]
+
+
+def workload5(trial: int = 0, n: int = 65536) -> Problem:
+    """2D: 65536 x 65536 samples (random angles, random order) of one closed curve, radius
+    1 + six random sine bumps of amplitude <= 0.08; the moving cloud rotated by up to 90 deg,
+    shifted in [-0.5, 0.5]^2, noise 0.005; covariances along the local tangent (sigma 0.01)
+    and across it (0.004)."""
+    rng = rng_for(5, trial)
+    shape = curve_shape(rng)
+    X, TX = curve_points(shape, rng.uniform(0.0, 2.0 * np.pi, n))
+    S, TS = curve_points(shape, rng.uniform(0.0, 2.0 * np.pi, n))
+    ang = rng.uniform(-np.pi / 2, np.pi / 2)
+    Rm = np.array([[np.cos(ang), -np.sin(ang)], [np.sin(ang), np.cos(ang)]])
+    tm = rng.uniform(-0.5, 0.5, 2)
+    Y = S @ Rm.T + tm + 0.005 * rng.standard_normal(S.shape)
+    XC = _tangent_cov(TX, 0.01, 0.004)
+    YC = _tangent_cov(TS @ Rm.T, 0.01, 0.004)
+    return Problem(X, Y, XC, YC, Rm.T, -Rm.T @ tm, "curve64k_2d")
+
+
+WORKLOADS = {0: workload0, 1: workload1, 2: workload2, 4: workload4, 5: workload5}
