@@ -44,6 +44,14 @@ def test_reference_arm_line():
     _check_reference_line(lines[0], 1)
 
 
+def test_reference_arm_line_2d():
+    lines = _json_lines([sys.executable, "bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1",
+                         "--workload", "5", "--n", "2048"])
+    assert len(lines) == 1
+    _check_reference_line(lines[0], 1)
+    assert "2d" in lines[0]["config"]["workload"]
+
+
 def test_reference_arm_two_ranks_print_one_line():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--gpus", "2",
