@@ -175,6 +175,38 @@ def test_energy_adjoint_ragged_sizes(D, n, m):
         api.fr_m(h)
 
 
+@pytest.mark.parametrize("D", [3, 2])
+@pytest.mark.parametrize("n,m", [(1, 1), (1, 300), (300, 1), (1025, 130), (77, 1031)])
+def test_conv_and_knn_ragged_sizes_every_shape(D, n, m):
+    """Ragged sizes (one source, one target, sizes off every tile and block multiple) through
+    every compiled CONV adjoint / energy shape and every nearest-neighbour shape, k up to 16."""
+    X, XC, Y, YC = _problem_small(D, n, m, seed=3 * n + m)
+    st = orc.State(X, XC, Y, YC)
+    _, h = api.init(X, XC, Y, YC)
+    try:
+        R, t = _pose(D, seed=11)
+        Eo, go, dxo = st.energy_conv(R, t, 0.3, with_dx=True)
+        for shape in api.shapes(3):
+            api.set_shape(h, 3, shape)
+            E, g, dx = api.energy_grad(h, R, t, 0.3, model=1, with_dx=True)
+            assert abs(E - Eo) <= 1e-6 * abs(Eo), (shape, E, Eo)
+            assert _rel(g, go) <= 1e-5, shape
+            assert _rel(dx, dxo) <= 1e-4, shape
+        for shape in api.shapes(4):
+            api.set_shape(h, 4, shape)
+            assert abs(api.energy(h, R, t, 0.3, model=1) - Eo) <= 1e-6 * abs(Eo), shape
+        for shape in api.shapes(2):
+            api.set_shape(h, 2, shape)
+            for k in (1, 5, 9, 16):
+                if k > m:
+                    continue
+                idx, d2 = api.nn(h, R, t, k)
+                oi, od = st.nn(R, t, k)
+                assert np.array_equal(idx, oi) and np.array_equal(d2, od), (shape, k)
+    finally:
+        api.fr_m(h)
+
+
 @pytest.mark.parametrize("what", [0, 1, 3, 4])
 @pytest.mark.parametrize("D", [3, 2])
 def test_every_kernel_shape_matches_oracle(what, D):
