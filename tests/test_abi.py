@@ -65,6 +65,37 @@ def test_errors_are_returned_not_fatal():
     assert rc == _lib.ERR_ARG and coef.value == 0
 
 
+def test_argument_errors_before_any_device_work():
+    """Entry points check their arguments before touching the device: each bad call returns
+    the argument status and a message (no GPU needed)."""
+    import ctypes
+
+    import numpy as np
+    L = _lib.load()
+    pts = np.zeros((8, 3))
+    cov = np.zeros((8, 3, 3))
+    dp = _lib.dp
+    for k, n, D in [(0, 8, 3), (16, 8, 3), (8, 8, 3), (3, 1, 3), (3, 8, 4)]:
+        rc = L.dugma_knn_covariance(pts.ctypes.data_as(dp), n, D, k, 1e-6, 1e-2, cov.ctypes.data_as(dp))
+        assert rc == _lib.ERR_ARG, (k, n, D)
+        assert b"knn_covariance" in L.dugma_last_error()
+    rc = L.dugma_knn_covariance(pts.ctypes.data_as(dp), 8, 3, 3, 0.0, 1e-2, cov.ctypes.data_as(dp))
+    assert rc == _lib.ERR_ARG   # lo must be positive
+    A = np.zeros(640)
+    out = np.zeros(9)
+    assert L.dugma_minimise_surrogate(4, A.ctypes.data_as(dp), out.ctypes.data_as(dp),
+                                      out.ctypes.data_as(dp), None, None) == _lib.ERR_ARG
+    buf = (ctypes.c_int * 64)()
+    assert L.dugma_shapes(7, buf, 16) < 0
+    eye = np.eye(3).reshape(-1)
+    R_out = np.zeros(9)
+    t_out = np.zeros(3)
+    rc = L.dugma_register(pts.ctypes.data_as(dp), cov.ctypes.data_as(dp), pts.ctypes.data_as(dp),
+                          cov.ctypes.data_as(dp), 8, 8, 3, eye.ctypes.data_as(dp), t_out.ctypes.data_as(dp),
+                          10, 1e-5, 1e-5, 1e-5, 99, R_out.ctypes.data_as(dp), t_out.ctypes.data_as(dp), None)
+    assert rc == _lib.ERR_ARG and b"mode" in L.dugma_last_error()
+
+
 def build_mex_harness(out_dir):
     """Compile tests/abi/mex_harness.cpp against include/dugma_mex.hpp and link it to the
     library: the reference's C++ signatures resolve against the exported symbols."""
