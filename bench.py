@@ -61,14 +61,18 @@ SFU_PER_PAIR = 2            # two ex2
 
 def parse():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
-    ap.add_argument("--workload", type=int, default=2)
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-fd", action="store_true")
+    ap.add_argument("--gpus", type=int, default=1, help="ranks (one per GPU; launched by torchrun for N > 1)")
+    ap.add_argument("--steps", type=int, default=50, help="timed steps")
+    ap.add_argument("--warmup", type=int, default=3, help="untimed warm-up steps (at least 3 are run)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"],
+                    help="ours: this library; reference: the path's CPU implementation (FP64 oracle port); "
+                         "reference-gpu: the reference's own CUDA plugins built from its sources")
+    ap.add_argument("--workload", type=int, default=2,
+                    help="0 1K sphere, 1 6K sphere, 2 64K harmonic surface, 3 batched problems, 4 300K depth "
+                         "views, 5 2D 64K curve")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and the accuracy check")
+    ap.add_argument("--no-fd", action="store_true", help="skip the plain form (energy + finite differences)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shape (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="override the cloud size (small profiling cases)")
     ap.add_argument("--shape", default="", help="pin the adjoint kernel shape ipt,nt,tj,pack (skips tuning)")
