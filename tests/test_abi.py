@@ -111,3 +111,15 @@ def build_mex_harness(out_dir):
 def test_reference_gateway_calls_link(tmp_path):
     exe = build_mex_harness(tmp_path)
     assert os.access(exe, os.X_OK)
+
+
+def test_default_kernel_shapes_are_compiled():
+    """The shapes a new context uses by default (adjoint, energy, nearest neighbours, CONV
+    adjoint, CONV energy) are among the compiled ones, and every listed shape is unique (the
+    host tables only: no GPU needed)."""
+    from dugma_b200 import api
+    defaults = {0: (4, 64, 64, 2), 1: (4, 128, 32, 2), 2: (4, 128, 64, 1), 3: (2, 64, 32, 2), 4: (1, 128, 32, 2)}
+    for what, shape in defaults.items():
+        listed = api.shapes(what)
+        assert shape in listed, (what, shape, listed)
+        assert len(set(listed)) == len(listed), what
