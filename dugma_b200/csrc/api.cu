@@ -66,6 +66,9 @@ void unregister_context(Context* c)
 int Context::ensure_scratch(size_t bytes)
 {
     if (bytes <= scratch_bytes) return DUGMA_OK;
+    if (no_alloc)
+        return set_error(DUGMA_ERR_STATE, "a launch needs %zu bytes of scratch beyond the fixed %zu bytes", bytes,
+                         scratch_bytes);
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(stream, &cs);
     if (cs != cudaStreamCaptureStatusNone)
@@ -372,6 +375,7 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
         {(void**)&c->wx, sizeof(float) * N},            {(void**)&c->wy, sizeof(float) * M},
         {(void**)&c->xcov, sizeof(float) * N * NS},     {(void**)&c->ycov, sizeof(float) * M * NS},
         {(void**)&c->lwx, sizeof(float) * N},           {(void**)&c->lwy, sizeof(float) * M},
+        {(void**)&c->ux, sizeof(double) * N * NS},
         {(void**)&c->yrec, sizeof(YRec) * c->M_pad},    {(void**)&c->xrec, sizeof(XRec) * c->N_pad},
         {(void**)&c->yp32, sizeof(float4) * c->M_pad},  {(void**)&c->dmin, sizeof(float) * N},
         {(void**)&c->pose, sizeof(double) * kPoseDoubles * 2}, {(void**)&c->out, sizeof(double) * 64},

@@ -25,6 +25,7 @@ constexpr int kBatchNT = 64, kBatchTJ = 64, kBatchIPT = 4, kBatchChunk = 512;   
 
 struct PQDesc {
     const float *x, *xinv, *lwx, *y, *yinv, *lwy, *wx;
+    const double* ux;   // the problem's Cholesky factors (Cholesky-form source records) or null
     const double* pose;
     XRec* xrec;
     YRec2* yrec;
@@ -36,7 +37,8 @@ struct BatchItem {
     int pq, ib, tile0, ntiles;
 };
 
-// one block row per pq: targets (paired layout, kC' unmodified) then sources
+// one block row per pq: targets (paired layout, kC' unmodified) then sources (the Cholesky form
+// sqrt(|k| s) U_i when the descriptor carries factors, else the Horner form)
 template <int D>
 __global__ void batch_prologue_kernel(const PQDesc* __restrict__ desc, int max_span)
 {
@@ -53,6 +55,7 @@ __global__ void batch_prologue_kernel(const PQDesc* __restrict__ desc, int max_s
             float f[16];
             for (int q = 0; q < 16; ++q) f[q] = 0.f;
             f[3] = -INFINITY;
+            f[13] = INFINITY;
             if (j < pd.M && pd.lwy[j] != -INFINITY) {
                 double A[3][3], T[3][3];
                 for (int a = 0; a < D; ++a) {
@@ -64,6 +67,7 @@ __global__ void batch_prologue_kernel(const PQDesc* __restrict__ desc, int max_s
                     f[4 + a] = -__double2float_rn(v - (double)hi);
                 }
                 f[3] = pd.lwy[j];
+                f[13] = -pd.lwy[j];
                 for (int r0 = 0; r0 < D; ++r0)
                     for (int c0 = 0; c0 < D; ++c0)
                         A[r0][c0] = 0.5 * ((double)pd.yinv[(size_t)j * D * D + r0 + D * c0] +
@@ -92,7 +96,10 @@ __global__ void batch_prologue_kernel(const PQDesc* __restrict__ desc, int max_s
             float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
             for (int a = 0; a < D; ++a) xv[a] = pd.x[(size_t)i * D + a];
             const float lw = pd.lwx[i];
-            if (lw != -INFINITY)
+            if (lw != -INFINITY && pd.ux) {
+                const double r = sqrt(-ks);
+                for (int k = 0; k < NS; ++k) bp[k] = __double2float_rn(r * pd.ux[(size_t)i * NS + k]);
+            } else if (lw != -INFINITY)
                 for (int k = 0; k < NS; ++k) {
                     const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
                     const double b = 0.5 * ((double)pd.xinv[(size_t)i * D * D + ra + D * rb] +
@@ -224,6 +231,7 @@ struct Batch {
     double* host = nullptr;           // pinned: poses in, results out
     size_t host_doubles = 0;
     int max_span = 0;
+    bool chol = true;                 // every problem's weighted sources have Cholesky factors
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
 
@@ -326,6 +334,7 @@ static int batch_prepare(Batch& b, int n_poses)
             d.yinv = c.yinv;
             d.lwy = c.lwy;
             d.wx = c.wx;
+            d.ux = b.chol ? c.ux : nullptr;
             d.pose = b.poses + 16 * (size_t)pq;
             d.xrec = reinterpret_cast<XRec*>(xbase + xoff[pq]);
             d.yrec = reinterpret_cast<YRec2*>(ybase + yoff[pq]);
@@ -352,8 +361,8 @@ static int batch_prepare(Batch& b, int n_poses)
 template <int D>
 static int batch_enqueue(Batch& b, cudaStream_t s)
 {
-    using Body = PackedBody<D, kBatchIPT, true>;
-    auto fn = batch_pairs_kernel<Body, kBatchNT, kBatchTJ, 4>;
+    auto fn = b.chol ? batch_pairs_kernel<PackedBody<D, kBatchIPT, true, true>, kBatchNT, kBatchTJ, 4>
+                     : batch_pairs_kernel<PackedBody<D, kBatchIPT, true, false>, kBatchNT, kBatchTJ, 4>;
     const int n_pq = b.P * b.n_poses;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.ctx[0]->dev);
@@ -395,6 +404,7 @@ int dugma_batch_create(int n_problems, int D, const int* N, const int* M, const 
             return rc;
         }
         b->ctx.push_back(find_context(&b->ptrs[6 * (size_t)p]));
+        if (b->ctx.back()->x_indef > 0) b->chol = false;
     }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         for (int k = 0; k < n_problems; ++k) dugma_fr_m(&b->ptrs[6 * (size_t)k]);

@@ -310,14 +310,19 @@ __device__ __forceinline__ float2 fld(const YRec2& r, int f)
     return (f & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
 }
 
-template <int D, int IPT_, bool GRAD>
+// CHOL: the source side in the Cholesky form of the x record (U^T U = |k| B_i, z = U d): the B
+// exponent is lv - |z|^2 (9 FP32 operations in 3D, as the Horner form), a sum of squares, so the FP32
+// rounding of the record moves it by ~sqrt(cond B_i) ulps instead of ~cond B_i; the e2 moments are
+// kept in the z frame (D2 = sum e2 z, Q2 = sum e2 z z^T) and mapped back per source in FP64.
+// !CHOL: the Horner form of k B_i (sources whose sym(Sigma_x^-1) has no Cholesky factor).
+template <int D, int IPT_, bool GRAD, bool CHOL = true>
 struct PackedBody {
     using StreamRec = YRec2;
     static constexpr int IPT = IPT_;
     static constexpr int NS = Sym<D>::N;
     static constexpr int NR = Sym<D>::NR;
     static constexpr int NV = GRAD ? 1 + NR + D : 1;
-    float2 X[IPT][D], B[IPT][NS];                 // source coordinates and k B_i, duplicated in both halves
+    float2 X[IPT][D], B[IPT][NS];                 // source coordinates and k B_i (or U), duplicated in both halves
     float2 e[IPT];                                // energy, tile level
     float2 S1[IPT][GRAD ? D : 1], D2[IPT][GRAD ? D : 1], Q2[IPT][GRAD ? NS : 1];   // item level
     double E64[IPT];
@@ -361,6 +366,7 @@ struct PackedBody {
 #pragma unroll
         for (int q = 0; q < D; ++q) { ny[q] = fld(r, q); nl[q] = fld(r, 4 + q); }
         const float2 lv = fld(r, 3);
+        const float2 nlv = fld(r, 13);
 #pragma unroll
         for (int k = 0; k < NS; ++k) c[k] = fld(r, 7 + k);
 #pragma unroll
@@ -370,25 +376,18 @@ struct PackedBody {
             for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(X[ii][q], ny[q]), nl[q]);
             const float2* b = B[ii];
             float2 t1, t2;
-            float2 u[3];
+            float2 u[3], z[3];   // u = k C' d (gradient); z = U d (Cholesky form) or d (Horner form)
             if (!GRAD) {
-                // Horner forms (off-diagonals doubled in both matrices)
+                // Horner form of k C' (off-diagonals doubled)
                 if (D == 3) {
                     const float2 g0 = ffma2(c[4], d[2], ffma2(c[3], d[1], fmul2(c[0], d[0])));
                     const float2 g1 = ffma2(c[5], d[2], fmul2(c[1], d[1]));
                     const float2 g2 = fmul2(c[2], d[2]);
                     t1 = ffma2(d[0], g0, ffma2(d[1], g1, ffma2(d[2], g2, lv)));
-                    const float2 h0 = ffma2(b[4], d[2], ffma2(b[3], d[1], fmul2(b[0], d[0])));
-                    const float2 h1 = ffma2(b[5], d[2], fmul2(b[1], d[1]));
-                    const float2 h2 = fmul2(b[2], d[2]);
-                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, ffma2(d[2], h2, lv)));
                 } else {
                     const float2 g0 = ffma2(c[2], d[1], fmul2(c[0], d[0]));
                     const float2 g1 = fmul2(c[1], d[1]);
                     t1 = ffma2(d[0], g0, ffma2(d[1], g1, lv));
-                    const float2 h0 = ffma2(b[2], d[1], fmul2(b[0], d[0]));
-                    const float2 h1 = fmul2(b[1], d[1]);
-                    t2 = ffma2(d[0], h0, ffma2(d[1], h1, lv));
                 }
             } else {
                 if (D == 3) {
@@ -396,34 +395,56 @@ struct PackedBody {
                     u[1] = ffma2(c[5], d[2], ffma2(c[1], d[1], fmul2(c[3], d[0])));
                     u[2] = ffma2(c[2], d[2], ffma2(c[5], d[1], fmul2(c[4], d[0])));
                     t1 = ffma2(d[2], u[2], ffma2(d[1], u[1], ffma2(d[0], u[0], lv)));
-                    // B exponent in Horner form (the x record's off-diagonals are doubled)
+                } else {
+                    u[0] = ffma2(c[2], d[1], fmul2(c[0], d[0]));
+                    u[1] = ffma2(c[1], d[1], fmul2(c[2], d[0]));
+                    t1 = ffma2(d[1], u[1], ffma2(d[0], u[0], lv));
+                }
+            }
+            float2 e2;
+            if (CHOL) {
+                // z = U d; e2 = 2^(lv - |z|^2)
+                float2 m2;
+                if (D == 3) {
+                    z[0] = ffma2(b[4], d[2], ffma2(b[3], d[1], fmul2(b[0], d[0])));
+                    z[1] = ffma2(b[5], d[2], fmul2(b[1], d[1]));
+                    z[2] = fmul2(b[2], d[2]);
+                    m2 = ffma2(z[0], z[0], ffma2(z[1], z[1], ffma2(z[2], z[2], nlv)));
+                } else {
+                    z[0] = ffma2(b[2], d[1], fmul2(b[0], d[0]));
+                    z[1] = fmul2(b[1], d[1]);
+                    m2 = ffma2(z[0], z[0], ffma2(z[1], z[1], nlv));
+                }
+                e2 = make_float2(ex2(-m2.x), ex2(-m2.y));
+            } else {
+                // Horner form of k B_i (the x record's off-diagonals are doubled)
+                if (D == 3) {
                     const float2 h0 = ffma2(b[4], d[2], ffma2(b[3], d[1], fmul2(b[0], d[0])));
                     const float2 h1 = ffma2(b[5], d[2], fmul2(b[1], d[1]));
                     const float2 h2 = fmul2(b[2], d[2]);
                     t2 = ffma2(d[0], h0, ffma2(d[1], h1, ffma2(d[2], h2, lv)));
                 } else {
-                    u[0] = ffma2(c[2], d[1], fmul2(c[0], d[0]));
-                    u[1] = ffma2(c[1], d[1], fmul2(c[2], d[0]));
-                    t1 = ffma2(d[1], u[1], ffma2(d[0], u[0], lv));
                     const float2 h0 = ffma2(b[2], d[1], fmul2(b[0], d[0]));
                     const float2 h1 = fmul2(b[1], d[1]);
                     t2 = ffma2(d[0], h0, ffma2(d[1], h1, lv));
                 }
+#pragma unroll
+                for (int q = 0; q < D; ++q) z[q] = d[q];
+                e2 = make_float2(ex2(t2.x), ex2(t2.y));
             }
             const float2 e1 = make_float2(ex2(t1.x), ex2(t1.y));
-            const float2 e2 = make_float2(ex2(t2.x), ex2(t2.y));
             e[ii] = fadd2(fadd2(e[ii], e1), e2);
             if (GRAD) {
-                // moments of e2: w = e2 d, then sum w and w d^T (only d lives across the SFU latency)
+                // moments of e2: w = e2 z, then sum w and w z^T (only z lives across the SFU latency)
                 float2 w[3];
 #pragma unroll
                 for (int q = 0; q < D; ++q) {
                     S1[ii][q] = ffma2(e1, u[q], S1[ii][q]);
-                    w[q] = fmul2(e2, d[q]);
+                    w[q] = fmul2(e2, z[q]);
                     D2[ii][q] = fadd2(D2[ii][q], w[q]);
                 }
 #pragma unroll
-                for (int k = 0; k < NS; ++k) Q2[ii][k] = ffma2(w[Sym<D>::a(k)], d[Sym<D>::b(k)], Q2[ii][k]);
+                for (int k = 0; k < NS; ++k) Q2[ii][k] = ffma2(w[Sym<D>::a(k)], z[Sym<D>::b(k)], Q2[ii][k]);
             }
         }
     }
@@ -436,6 +457,89 @@ struct PackedBody {
         }
     }
     __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
+    {
+        if (CHOL)
+            finish_chol(a, jc, acc);
+        else
+            finish_horner(a, jc, acc);
+    }
+    // Cholesky form: with U the record's factor (U^T U = |k| B), V = U^-1 and the z-frame moments,
+    //   B D2 = U^T D2z / |k|,   sum e2 d x B d = sum_ab Q2z_ab (V e_a) x (U^T e_b) / |k|.
+    __device__ void finish_chol(const PairArgs& a, int jc, double (&acc)[NV])
+    {
+        const double kinv = 1.0 / K_EXP2, rk = -kinv;
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) {
+            if (row[ii] < 0) continue;
+            const int i = row[ii];
+            const double w = (double)a.wx[i] * G;
+            acc[0] += w * E64[ii];
+            if (!GRAD) continue;
+            double gt[3] = {0, 0, 0};
+            if (w != 0.0) {   // neglected sources carry U = 0 and weight 0
+                double U[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Qm[3][3], s1[3], d2[3];
+#pragma unroll
+                for (int q = 0; q < NS; ++q) {
+                    const int ra = Sym<D>::a(q), rb = Sym<D>::b(q);
+                    U[ra][rb] = (double)B[ii][q].x;
+                    Qm[ra][rb] = Qm[rb][ra] = (double)Q2[ii][q].x + (double)Q2[ii][q].y;
+                }
+#pragma unroll
+                for (int q = 0; q < D; ++q) {
+                    s1[q] = (double)S1[ii][q].x + (double)S1[ii][q].y;
+                    d2[q] = (double)D2[ii][q].x + (double)D2[ii][q].y;
+                }
+                double V[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                V[0][0] = 1.0 / U[0][0];
+                V[1][1] = 1.0 / U[1][1];
+                V[0][1] = -U[0][1] * V[0][0] * V[1][1];
+                if (D == 3) {
+                    V[2][2] = 1.0 / U[2][2];
+                    V[1][2] = -U[1][2] * V[1][1] * V[2][2];
+                    V[0][2] = (U[0][1] * U[1][2] - U[0][2] * U[1][1]) * V[0][0] * V[1][1] * V[2][2];
+                }
+                double p[3];
+#pragma unroll
+                for (int q = 0; q < D; ++q) {
+                    double bd = 0;
+#pragma unroll
+                    for (int cc = 0; cc < D; ++cc) bd += U[cc][q] * d2[cc];
+                    gt[q] = s1[q] * kinv + rk * bd;
+                    p[q] = (double)X[ii][q].x - t[q];
+                }
+                if (D == 3) {
+                    double qx[3] = {0, 0, 0};
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                        for (int bb = 0; bb < 3; ++bb) {
+                            const double q = Qm[aa][bb];
+                            qx[0] += q * (V[1][aa] * U[bb][2] - V[2][aa] * U[bb][1]);
+                            qx[1] += q * (V[2][aa] * U[bb][0] - V[0][aa] * U[bb][2]);
+                            qx[2] += q * (V[0][aa] * U[bb][1] - V[1][aa] * U[bb][0]);
+                        }
+                    acc[1] += w * (p[1] * gt[2] - p[2] * gt[1] - rk * qx[0]);
+                    acc[2] += w * (p[2] * gt[0] - p[0] * gt[2] - rk * qx[1]);
+                    acc[3] += w * (p[0] * gt[1] - p[1] * gt[0] - rk * qx[2]);
+                } else {
+                    double qx = 0;
+#pragma unroll
+                    for (int aa = 0; aa < 2; ++aa)
+#pragma unroll
+                        for (int bb = 0; bb < 2; ++bb) qx += Qm[aa][bb] * (V[0][aa] * U[bb][1] - V[1][aa] * U[bb][0]);
+                    acc[1] += w * (p[0] * gt[1] - p[1] * gt[0] - rk * qx);
+                }
+#pragma unroll
+                for (int q = 0; q < D; ++q) acc[1 + NR + q] += w * gt[q];
+            }
+            if (a.dx_part) {
+                const int rows = a.i_end - a.i0;
+#pragma unroll
+                for (int q = 0; q < D; ++q) a.dx_part[((size_t)jc * rows + (i - a.i0)) * D + q] = -w * gt[q];
+            }
+        }
+    }
+    __device__ void finish_horner(const PairArgs& a, int jc, double (&acc)[NV])
     {
         const double kinv = 1.0 / K_EXP2;
 #pragma unroll

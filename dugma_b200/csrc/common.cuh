@@ -93,20 +93,63 @@ struct __align__(16) YRec {
 
 // Paired target record (128 B) for the packed f32x2 kernels: targets 2p and 2p+1 side by side.
 // Field f (f = 0..15) is the float2 (value of target 2p, value of target 2p+1):
-//   f0..f2  -y'hi,  f3 lv,  f4..f6  -y'lo,  f7 + k  k C'_j packed entry k (Sym order), rest 0.
+//   f0..f2  -y'hi,  f3 lv,  f4..f6  -y'lo,  f7 + k  k C'_j packed entry k (Sym order),
+//   f13 -lv, rest 0.
 // Coordinates are stored negated so that d = (x + f0) + f4 needs only packed adds.
 struct __align__(16) YRec2 {
     float4 q[8];   // q[k] = (field 2k even, field 2k odd, field 2k+1 even, field 2k+1 odd)
 };
 
-// Source record, one per x_i and sigma (64 B):
+// Source record, one per x_i and sigma (64 B), in one of two forms:
 //   v0 = (x.x, x.y, x.z, lw)            lw = log2(w_i) - Lmax_x
 //   v1 = (0, 0, 0, 0)
+// Horner form (scalar kernels):
 //   v2 = (b00, b11, b22, 2 b01)         k * B_i packed, off-diagonals doubled
 //   v3 = (2 b02, 2 b12, 0, 0)
+// Cholesky form (packed kernels): U upper triangular with U^T U = |k| B_i, so the exponent is
+// lv - |U d|^2, a sum of squares whatever the condition of B_i
+//   v2 = (u00, u11, u22, u01)
+//   v3 = (u02, u12, 0, 0)
+// In 2D v2 = (b00, b11, 2 b01, 0) or (u00, u11, u01, 0).
 struct __align__(16) XRec {
     float4 v0, v1, v2, v3;
 };
+
+// Upper Cholesky factor of a symmetric positive definite D x D matrix, both packed in Sym order
+// (3D: 00, 11, 22, 01, 02, 12; 2D: 00, 11, 01): U^T U = P.  Returns false, with u zeroed, when a
+// pivot is not above 1e-13 times its diagonal entry (P not safely positive definite).
+template <int D>
+__device__ inline bool chol_upper(const double* p, double* u)
+{
+    constexpr double kRel = 1e-13;
+    bool ok = p[0] > 0.0;
+    double u00 = ok ? sqrt(p[0]) : 0.0;
+    if (D == 2) {
+        const double u01 = ok ? p[2] / u00 : 0.0;
+        const double piv = p[1] - u01 * u01;
+        ok = ok && piv > kRel * p[1] && isfinite(piv);
+        u[0] = u00;
+        u[1] = ok ? sqrt(piv) : 0.0;
+        u[2] = u01;
+    } else {
+        const double u01 = ok ? p[3] / u00 : 0.0, u02 = ok ? p[4] / u00 : 0.0;
+        const double piv1 = p[1] - u01 * u01;
+        ok = ok && piv1 > kRel * p[1];
+        const double u11 = ok ? sqrt(piv1) : 1.0;
+        const double u12 = (p[5] - u01 * u02) / u11;
+        const double piv2 = p[2] - u02 * u02 - u12 * u12;
+        ok = ok && piv2 > kRel * p[2] && isfinite(piv2);
+        u[0] = u00;
+        u[1] = u11;
+        u[2] = ok ? sqrt(piv2) : 0.0;
+        u[3] = u01;
+        u[4] = u02;
+        u[5] = u12;
+    }
+    if (!ok)
+        for (int k = 0; k < (D == 3 ? 6 : 3); ++k) u[k] = 0.0;
+    return ok;
+}
 
 // Coefficient-pass records (128 B): the 64-B record followed by the degree <= 2 monomials
 // of the point, g = (1, v_0..v_{D-1}, packed v_a v_b) (10 in 3D, 6 in 2D), zero padded.

@@ -52,6 +52,9 @@ struct Context {
     // extra state
     float *xcov = nullptr, *ycov = nullptr;   // packed symmetric FP32 covariances (CONV model)
     float *lwx = nullptr, *lwy = nullptr;     // log2(w) - Lmax, -inf when neglected
+    double* ux = nullptr;                     // upper Cholesky factor of sym(Sigma_x^-1) per source (packed,
+                                              // FP64); zero for neglected and not positive definite sources
+    int x_indef = 0;                          // weighted sources whose sym(Sigma_x^-1) is not positive definite
     double Lmax_x = 0, Lmax_y = 0;
     double cscale = 1.0;                      // CONV covariances are stored divided by this
     // per-evaluation records
@@ -79,6 +82,7 @@ struct Context {
     void* scratch_extra = nullptr;
     double* scratch = nullptr;
     size_t scratch_bytes = 0;
+    bool no_alloc = false;                    // scratch is fixed: ensure_scratch fails rather than allocating
     // pinned host staging
     // [0,16) pose, [63] error word, [64,128) results, [256,512) multi-pose staging
     double* host = nullptr;                   // kHostDoubles doubles
@@ -131,8 +135,9 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
                         cudaStream_t s, const float* w_stationary = nullptr);
-// Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy), x records.
-int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s);
+// Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy, 2 / 3 their paired
+// forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form.
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol = false);
 // Pairwise energy (grad = false) or fused adjoint (grad = true) over source rows [i0, i1);
 // writes {E, g} to out_dev and, if dEdx_dev, dE/dx for rows [i0, i1) (relative index).
 int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1,

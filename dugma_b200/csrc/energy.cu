@@ -111,6 +111,22 @@ static const std::vector<Variant>& energy_variants()
     return v;
 }
 
+// Problems with a weighted source whose sym(Sigma_x^-1) has no Cholesky factor (an indefinite
+// inverse covariance: not a covariance, but the reference evaluates it) run the packed kernels on
+// the Horner form of k B_i instead, whatever shape is pinned.
+template <int D>
+static const Variant& adjoint_fallback()
+{
+    static const Variant v = {{4, 64, 64, 2, 512}, pair_kernel_occ<PackedBody<D, 4, true, false>, 64, 64, 4>};
+    return v;
+}
+template <int D>
+static const Variant& energy_fallback()
+{
+    static const Variant v = {{4, 128, 32, 2}, pair_kernel<PackedBody<D, 4, false, false>, 128, 32>};
+    return v;
+}
+
 std::vector<KernelShape> adjoint_shapes()
 {
     std::vector<KernelShape> s;
@@ -240,9 +256,17 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
     const Variant* v = &vars[0];
     for (auto& cand : vars)
         if (cand.shape.same(want)) v = &cand;
+    // the packed kernels read the Cholesky form of the source records when every weighted source
+    // has a factor, else the Horner form
+    bool xchol = v->shape.pack == 2;
+    if (xchol && c.x_indef > 0) {
+        v = c.D == 3 ? (grad ? &adjoint_fallback<3>() : &energy_fallback<3>())
+                     : (grad ? &adjoint_fallback<2>() : &energy_fallback<2>());
+        xchol = false;
+    }
     // record layout: 0 scalar adjoint, 1 scalar Horner energy, 2 / 3 their packed-pair forms
     const int layout = (grad ? 0 : 1) + (v->shape.pack == 2 ? 2 : 0);
-    DUGMA_RET(launch_prologue(c, pose_dev, layout, s));
+    DUGMA_RET(launch_prologue(c, pose_dev, layout, s, xchol));
     const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
     return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad / v->shape.pack, nv, c.Lmax_y,
                                pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
@@ -251,14 +275,14 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
 // ---------------------------------------------------------------------------
 // Allocation-free fused adjoint.
 //
-// For callers that cannot allocate device memory while they evaluate: code that runs
-// while a CUDA graph is being captured (allocation calls are not allowed there), loops
-// with a latency budget that must never enter an allocator, and host applications that
-// own every device allocation themselves.  They pass the six input arrays and the
-// output buffer; everything the evaluation needs besides them (per-pose records,
-// normalised weights, work-queue counter, per-item partial sums) lives in one
-// file-scope device array of kNoAllocScratchBytes, which every GPU that loads this
-// library holds until the process exits.
+// For callers that cannot allocate device memory while they evaluate: loops with a
+// latency budget that must never enter an allocator, and host applications that own
+// every device allocation themselves.  They pass the six input arrays and the output
+// buffer; everything the evaluation needs besides them (per-pose records, normalised
+// weights, work-queue counter, per-item partial sums, the device error word) lives in
+// one file-scope device array of kNoAllocScratchBytes, which every GPU that loads this
+// library holds until the process exits.  The context built here is marked no_alloc,
+// so a launch that would need more scratch fails instead of allocating.
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;   // 4 MiB
 constexpr int kNoAllocMaxPadded = 16384;                     // N and M, after padding to 1024 / 128
@@ -288,10 +312,11 @@ __global__ void noalloc_norm_log2_kernel(const float* __restrict__ w, int n, con
         lw[i] = w[i] > 0.0f ? __double2float_rn(log2((double)w[i]) - L) : -INFINITY;
 }
 
-// the pair kernel ran with a zero weight offset: restore the 2^Lmax_y factor of every output
-__global__ void noalloc_scale_kernel(double* out, int n, const double* Lmax)
+// the pair kernel ran with a zero weight offset: restore the 2^Lmax_y factor of every output;
+// if a bounded wait of the pair kernel gave up (error word set), every output becomes NaN
+__global__ void noalloc_scale_kernel(double* out, int n, const double* Lmax, const int* err)
 {
-    if (threadIdx.x < n) out[threadIdx.x] *= exp2(*Lmax);
+    if (threadIdx.x < n) out[threadIdx.x] = *err ? (double)NAN : out[threadIdx.x] * exp2(*Lmax);
 }
 
 static std::mutex g_noalloc_mu;
@@ -343,7 +368,8 @@ extern "C" int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv,
     c.N_pad = N_pad;
     c.M_pad = M_pad;
     c.dev = dev;
-    cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, dev);
+    DUGMA_CK(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    c.no_alloc = true;
     c.x = const_cast<float*>(x);
     c.xinv = const_cast<float*>(x_cov_inv);
     c.wx = const_cast<float*>(det_x);
@@ -377,7 +403,7 @@ extern "C" int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv,
     const int nv = 1 + (D == 3 ? 6 : 3);
     DUGMA_RET(launch_pair_variant(c, var.fn, var.shape, c.xrec, c.yrec, (size_t)M_pad, nv, 0.0, pose_dev, 0, N,
                                   out_dev, nullptr, nullptr, 0, nullptr, s));
-    noalloc_scale_kernel<<<1, 32, 0, s>>>(out_dev, nv, Lm + 1);
+    noalloc_scale_kernel<<<1, 32, 0, s>>>(out_dev, nv, Lm + 1, c.err);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }

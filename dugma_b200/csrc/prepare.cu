@@ -18,11 +18,14 @@ namespace dugma {
 // and rounded to FP32.  det <= 0: all entries 1e5, weight 0 (init.cu:48-57, 86-100).
 // Also writes the packed symmetric FP32 covariance used by the CONV model.
 // ---------------------------------------------------------------------------
+// ufac (nullable): the upper Cholesky factor of sym(cinv) per point (packed, FP64) for the
+// Cholesky-form source records; zero for neglected points, and zero with a count in *indef for
+// weighted points whose sym(cinv) is not positive definite.
 template <int D>
 __global__ void init_points_kernel(const double* __restrict__ P, const double* __restrict__ C, int n,
                                    float* __restrict__ p32, float* __restrict__ cinv,
                                    float* __restrict__ w, float* __restrict__ cpack, const double* __restrict__ scale,
-                                   int* nonpd)
+                                   int* nonpd, double* __restrict__ ufac, int* indef)
 {
     constexpr int NS = Sym<D>::N;
     const double inv_scale = scale[1];
@@ -75,6 +78,18 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
                 w[i] = 0.0f;
                 atomicAdd(nonpd, 1);
             }
+        }
+        if (ufac) {
+            double pk[NS], u[NS];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                pk[k] = 0.5 * ((double)o[ra + D * rb] + (double)o[rb + D * ra]);
+            }
+            const bool ok = chol_upper<D>(pk, u);
+            if (w[i] > 0.0f && !ok) atomicAdd(indef, 1);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) ufac[(size_t)i * NS + k] = w[i] > 0.0f ? u[k] : 0.0;
         }
     }
 }
@@ -181,12 +196,17 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     const int nb = std::min(kMomSlots, std::max(1, (N + M + 2047) / 2048));
     cov_trace_partial_kernel<<<nb, 256, 0, s>>>(tXC, N, tYC, M, D, c.mom);
     cov_scale_kernel<<<1, 256, 0, s>>>(c.mom, nb, N + M, D, Lm + 2);
+    // counter[4]: weighted sources without a Cholesky factor
     if (D == 3) {
-        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
-        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
+        init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter, c.ux,
+                                                c.counter + 4);
+        init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter, nullptr,
+                                                nullptr);
     } else {
-        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter);
-        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter);
+        init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter, c.ux,
+                                                c.counter + 4);
+        init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter, nullptr,
+                                                nullptr);
     }
     // counter[2], counter[3]: the largest weight of each cloud as float bits (zeroed above)
     max_weight_kernel<<<std::min(gx, 4 * c.num_sms), bs, 0, s>>>(c.wx, N, c.counter + 2);
@@ -196,6 +216,7 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     ck(cudaGetLastError(), "init kernels");
     ck(cudaMemcpyAsync(c.host, Lm, 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax, scale");
     ck(cudaMemcpyAsync(c.host + 3, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
+    ck(cudaMemcpyAsync(c.host + 4, c.counter + 4, sizeof(int), cudaMemcpyDeviceToHost, s), "copy indefinite count");
     ck(cudaStreamSynchronize(s), "sync");
     if (rc != DUGMA_OK) return rc;
     c.Lmax_x = std::isfinite(c.host[0]) ? c.host[0] : 0.0;
@@ -204,6 +225,9 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     int nonpd = 0;
     memcpy(&nonpd, c.host + 3, sizeof(int));
     c.nonpd = nonpd;
+    int indef = 0;
+    memcpy(&indef, c.host + 4, sizeof(int));
+    c.x_indef = c.ux ? indef : N;
     return DUGMA_OK;
 }
 
@@ -214,7 +238,9 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
 //              C'_j = R (s sym(Sigma_y_j^-1)) R^T (compi.cu:757-765) scaled by k = -1/2 log2 e
 //              (layout 0: packed as is; layout 1: off-diagonals doubled for the Horner form);
 //              lv_j = log2(w_j) - Lmax_y.
-//   x records: x_i, lw_i, k * s * sym(Sigma_x_i^-1) with doubled off-diagonals.
+//   x records: x_i, lw_i and either k * s * sym(Sigma_x_i^-1) with doubled off-diagonals (Horner
+//              form) or, when ux is given, sqrt(|k| s) U_i from the init-time Cholesky factor U_i
+//              of sym(Sigma_x_i^-1) (Cholesky form: (sqrt(|k| s) U_i)^T (sqrt(|k| s) U_i) = |k| B_i).
 // Rows past N / M are null records (lw = -inf, zero matrices): they contribute exactly 0.
 // ---------------------------------------------------------------------------
 template <int D>
@@ -222,7 +248,8 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
                                 const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
                                 int ylayout, YRec* __restrict__ yrec, float4* __restrict__ yp32,
                                 const float* __restrict__ x, const float* __restrict__ xinv,
-                                const float* __restrict__ lwx, int N, int N_pad, XRec* __restrict__ xrec)
+                                const float* __restrict__ lwx, int N, int N_pad, XRec* __restrict__ xrec,
+                                const double* __restrict__ ux)
 {
     constexpr int NS = Sym<D>::N;
     double R[9], t[3];
@@ -291,6 +318,7 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
                 f[4 + a] = -lo[a];
             }
             f[3] = lv;
+            f[13] = -lv;
 #pragma unroll
             for (int k = 0; k < NS; ++k) f[7 + k] = cp[k];
             float* base = reinterpret_cast<float*>(yrec) + (size_t)(j >> 1) * 32 + (j & 1);
@@ -326,7 +354,11 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
 #pragma unroll
             for (int a = 0; a < D; ++a) xv[a] = x[(size_t)i * D + a];
             lw = lwx[i];
-            if (lw != -INFINITY) {
+            if (lw != -INFINITY && ux) {
+                const double r = sqrt(-ks);
+#pragma unroll
+                for (int k = 0; k < NS; ++k) bp[k] = __double2float_rn(r * ux[(size_t)i * NS + k]);
+            } else if (lw != -INFINITY) {
 #pragma unroll
                 for (int k = 0; k < NS; ++k) {
                     const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
@@ -351,17 +383,20 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
     }
 }
 
-int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s)
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol)
 {
+    if (xchol && (!c.ux || c.x_indef > 0))
+        return set_error(DUGMA_ERR_STATE, "Cholesky-form source records need a positive definite factor per source");
+    const double* ux = xchol ? c.ux : nullptr;
     const int n = std::max(c.M_pad, c.N_pad);
     const int bs = 256;
     const int g = std::min((n + bs - 1) / bs, c.num_sms * 4);
     if (c.D == 3)
         prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux);
     else
         prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }

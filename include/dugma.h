@@ -132,8 +132,7 @@ int dugma_energy_grad_async(float* Ptr[6], const double* pose_dev, int model, do
 int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double* out_dev, void* stream);
 
 /* Allocation-free fused adjoint.  No counterpart in the reference: it is for callers that
- * cannot allocate device memory while they evaluate — code running during CUDA-graph
- * capture (allocation calls are not permitted there), latency-bounded loops that must never
+ * cannot allocate device memory while they evaluate — latency-bounded loops that must never
  * enter an allocator, and hosts that own every device allocation themselves.  The caller
  * passes the six input arrays in the order and layout of Ptr[6] after dugma_init (source
  * coordinates, source inverse covariances, target coordinates, target inverse covariances,
@@ -146,7 +145,8 @@ int dugma_energy_async(float* Ptr[6], const double* pose_dev, int model, double*
  * reuses the same array, so calls whose work overlaps on the GPU (other streams, other
  * threads) race; the array keeps the last call's contents and each call re-initialises what
  * it needs.  Work is enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream)
- * and the call returns without synchronising. */
+ * and the call returns without synchronising, so device-side failures cannot be returned as
+ * a status: if a bounded device wait gives up, every value written to out_dev is NaN. */
 int dugma_energy_grad_noalloc(const float* x, const float* x_cov_inv, const float* y, const float* y_cov_inv,
                               const float* det_x, const float* det_y, int N, int M, int D,
                               const double* pose_dev, double* out_dev, void* stream);

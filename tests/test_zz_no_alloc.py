@@ -1,13 +1,14 @@
 """The allocation-free entry point dugma_energy_grad_noalloc against dugma_energy_grad.
 
-Some callers cannot allocate device memory while they evaluate (CUDA-graph capture,
-latency-bounded loops, hosts that own all device memory).  For them the library offers
-one entry point whose working memory is a fixed file-scope device array.  This test
-calls it through the C ABI with a context's device arrays as inputs and device tensors
-for the pose and the result, twice in a row (the second call reuses the array the first
-one left behind), and compares each result with the allocating entry point's at the
-tolerances of the other parity tests (energy 1e-6, pose gradient 1e-5, relative).
-It lives in its own file, named to be collected last.
+Some callers cannot allocate device memory while they evaluate (latency-bounded loops
+that must never enter an allocator, hosts that own all device memory).  For them the
+library offers one entry point whose working memory is a fixed file-scope device array.
+This test calls it through the C ABI with a context's device arrays as inputs and device
+tensors for the pose and the result, twice in a row (the second call reuses the array the
+first one left behind), and compares each result with the allocating entry point's and with
+the FP64 oracle's at the tolerances of the other parity tests (energy 1e-6, pose gradient
+1e-5, relative); the second call must leave the device's free memory unchanged.  The size
+limit is checked on both sides of it.  It lives in its own file, named to be collected last.
 """
 import ctypes
 
@@ -16,6 +17,7 @@ import pytest
 
 from dugma_b200 import _lib, api, synth
 from dugma_b200.pose import expmap, rot2d
+from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +46,7 @@ def test_noalloc_matches_allocating_entry_point(D):
     try:
         sig = api.update_sig(h, R, t)
         E_ref, g_ref, _ = api.energy_grad(h, R, t, sig)
+        E_o, g_o, _ = orc.State(X, XC, Y, YC).energy(R, t, sig)
         pose = torch.zeros(16, dtype=torch.float64, device="cuda")
         pose[: D * D] = torch.tensor(np.asarray(R).T.reshape(-1))
         pose[9:9 + D] = torch.tensor(t)
@@ -53,14 +56,21 @@ def test_noalloc_matches_allocating_entry_point(D):
         for call in range(2):
             out = torch.full((8,), float("nan"), dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
             rc = L.dugma_energy_grad_noalloc(*h.ptrs, h.N, h.M, h.D, pose.data_ptr(), out.data_ptr(),
                                              ctypes.c_void_p(stream.cuda_stream))
             assert rc == _lib.OK, L.dugma_last_error()
             stream.synchronize()
+            if call == 1:
+                # the first call may load the library's kernels (and with them the array); after it
+                # nothing may take device memory
+                assert torch.cuda.mem_get_info()[0] >= free0
             res = out.cpu().numpy()
             E, g = res[0], res[1:1 + ng]
             assert abs(E - E_ref) <= 1e-6 * abs(E_ref), (call, E, E_ref)
             assert np.linalg.norm(g - g_ref) <= 1e-5 * np.linalg.norm(g_ref), (call, g, g_ref)
+            assert abs(E - E_o) <= 1e-6 * abs(E_o), (call, E, E_o)
+            assert np.linalg.norm(g - g_o) <= 1e-5 * np.linalg.norm(g_o), (call, g, g_o)
     finally:
         api.fr_m(h)
 
@@ -73,8 +83,38 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
         import torch
         pose = torch.zeros(16, dtype=torch.float64, device="cuda")
         out = torch.zeros(8, dtype=torch.float64, device="cuda")
-        rc = L.dugma_energy_grad_noalloc(*h.ptrs, 20000, h.M, 3, pose.data_ptr(), out.data_ptr(), None)
-        assert rc == _lib.ERR_ARG
-        assert b"16384" in L.dugma_last_error()
+        for n, m in ((20000, h.M), (h.N, 16385), (16385, 16385)):
+            rc = L.dugma_energy_grad_noalloc(*h.ptrs, n, m, 3, pose.data_ptr(), out.data_ptr(), None)
+            assert rc == _lib.ERR_ARG, (n, m)
+            assert b"16384" in L.dugma_last_error()
+    finally:
+        api.fr_m(h)
+
+
+def test_noalloc_accepts_the_largest_size():
+    """N = M = 16384, where the carved scratch (records, log weights, worst-case partial sums) is
+    closest to the array's size: accepted, and equal to the allocating entry point's result."""
+    import torch
+
+    P = synth.workload0(n=16384)
+    R, t = P.R_G @ expmap([0.02, 0.03, -0.01]), P.t_G
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    L = _lib.load()
+    try:
+        assert (h.N, h.M) == (16384, 16384)
+        sig = api.update_sig(h, R, t)
+        E_ref, g_ref, _ = api.energy_grad(h, R, t, sig)
+        pose = torch.zeros(16, dtype=torch.float64, device="cuda")
+        pose[:9] = torch.tensor(np.asarray(R).T.reshape(-1))
+        pose[9:12] = torch.tensor(t)
+        pose[12] = sig
+        out = torch.zeros(8, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        rc = L.dugma_energy_grad_noalloc(*h.ptrs, h.N, h.M, 3, pose.data_ptr(), out.data_ptr(), None)
+        assert rc == _lib.OK, L.dugma_last_error()
+        torch.cuda.synchronize()
+        res = out.cpu().numpy()
+        assert abs(res[0] - E_ref) <= 1e-6 * abs(E_ref), (res[0], E_ref)
+        assert np.linalg.norm(res[1:7] - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
     finally:
         api.fr_m(h)
