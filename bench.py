@@ -20,6 +20,11 @@ plain_fd    the plain form: energy + central finite differences (13 energy evalu
 cpu_baseline  the FP64 C/OpenMP oracle on a bounded sample of source rows, all host cores.
 accuracy    this run's relative error against that FP64 oracle on the same sampled rows
             (energy and the pose gradient of source rows [0, rows) over all targets).
+configs     (default run, one GPU) compact results of the other configured workloads, each
+            with its own device timing, roofline fraction, error against the FP64 oracle and
+            clock record: the 1K and 6K spheres, the batch of 256 problems x 32 rotations, the
+            300K depth views with 64 poses and the k = 8 neighbour pass, the 2D curve, the CONV
+            model, and update_sig / compi through the plugin interface at 64K.
 
 Workloads (--workload): 0 1K sphere, 1 6K sphere with outliers, 2 the 64K harmonic surface
 (default), 3 256 problems x 32 poses in one persistent launch, 4 300K depth views, 5 the 2D
@@ -47,10 +52,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic per-pair operation counts of the REF kernels, 3D (see the kernel sources)
-# REF adjoint: d 6, u = kC'd 9, d.u 3, B exponent (Horner) 9, energy 2, S1 += e1 u 3, w = e2 d 3,
-# D2 += w 3, Q2 += w d^T 6
+# REF adjoint: d 6, u = kC'd 9, d.u 3, B exponent (z = U d 6, |z|^2 3) 9, energy 2, S1 += e1 u 3,
+# w = e2 z 3, D2 += w 3, Q2 += w z^T 6
 FP32_INSTR_ADJOINT = 44
-# REF adjoint in 2D: d 4, u 4, d.u 2, B exponent (Horner) 3 + 2, energy 2, S1 2, w 2, D2 2, Q2 3
+# REF adjoint in 2D: d 4, u 4, d.u 2, B exponent (z = U d 3, |z|^2 2) 5, energy 2, S1 2, w 2, D2 2, Q2 3
 FP32_INSTR_ADJOINT_2D = 26
 # CONV adjoint: d 6, S = Sx + C'y 6, adjugate 12, det 3, singularity test 3, h = adj d 9, d.h 3,
 # exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
@@ -80,6 +85,8 @@ def parse():
                     help="0: the reference's per-pair model (REF), 1: convolved GMM (CONV)")
     ap.add_argument("--poses", type=int, default=1,
                     help="multistart poses evaluated per step and GPU (the depth workload uses 64)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the compact results of the other configured workloads (the `configs` key)")
     return ap.parse_args()
 
 
@@ -386,6 +393,263 @@ def run_batch(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# The other configured workloads, each measured compactly in the default run (`configs`)
+# ---------------------------------------------------------------------------
+def _oracle_rows(P, budget_pairs=2.7e8):
+    """Source rows the FP64 oracle checks: all of them when that is cheap, else a prefix of about
+    budget_pairs pairs."""
+    return int(min(P.N, max(256, budget_pairs // P.M)))
+
+
+def _accuracy(h, st, R, t, sig, model, rows):
+    from dugma_b200 import api
+    Eo, go, _ = (st.energy_conv if model == 1 else st.energy)(R, t, sig, i0=0, i1=rows)
+    Eg, gg = api.energy_grad_range(h, R, t, sig, 0, rows, model=model)
+    return {"rows": int(rows), "E_rel_err": abs(Eg - Eo) / abs(Eo),
+            "grad_rel_err": float(np.linalg.norm(gg - go) / np.linalg.norm(go)),
+            "tolerance": {"E": 1e-6, "grad": 1e-5}, "against": "FP64 oracle, same rows"}
+
+
+def _instr(D, model):
+    if model == 1:
+        return FP32_INSTR_CONV_ADJOINT
+    return FP32_INSTR_ADJOINT if D == 3 else FP32_INSTR_ADJOINT_2D
+
+
+def config_single(L, name, P, model, peak, steps=20, poses=1, nn_k=0, clock_dir="/tmp"):
+    """One problem: pose gradient of `poses` multistart poses per step, device-timed (CUDA events on
+    the launching stream, L2 flushed between steps), the adjoint kernel's share from the library's
+    events, the error against the FP64 oracle on the oracle's rows, clocks during the timed region."""
+    import ctypes
+    import torch
+    from dugma_b200 import api
+    from oracle import oracle as orc
+    D = P.X.shape[1]
+    R, t = eval_pose(P, 0)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    try:
+        ent = {"workload": f"{P.name}: N={P.N}, M={P.M}, {'CONV' if model == 1 else 'REF'} model, "
+                           f"{poses} pose(s) per step"}
+        torch.cuda.synchronize()
+        a0 = time.perf_counter()
+        sig = api.update_sig(h, R, t)
+        ent["update_sig_ms"] = 1e3 * (time.perf_counter() - a0)
+        if nn_k:
+            # the brute-force k-nearest-neighbour pass on the clouds (device time of its kernels)
+            api.nn(h, R, t, nn_k)
+            L.dugma_timing(h.arr, 1, None, None)
+            api.nn(h, R, t, nn_k)
+            kms, kl = ctypes.c_double(0), ctypes.c_int(0)
+            L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
+            L.dugma_timing(h.arr, 0, None, None)
+            ent["nn"] = {"k": nn_k, "kernel_ms": kms.value, "pairs_per_s": P.N * P.M / (kms.value * 1e-3)}
+        ent["autotune"] = api.autotune(h, 0 if model == 0 else 3)
+        stream = torch.cuda.Stream()
+        pose = torch.zeros(poses, 16, dtype=torch.float64, device="cuda")
+        for k in range(poses):
+            Rk, tk = eval_pose(P, k)
+            pose[k, :D * D] = torch.tensor(np.asarray(Rk).T.reshape(-1))
+            pose[k, 9:9 + D] = torch.tensor(tk)
+            pose[k, 12] = sig
+        out = torch.zeros(poses, 8, dtype=torch.float64, device="cuda")
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+        def step(npose=poses):
+            for k in range(npose):
+                rc = L.dugma_energy_grad_async(h.arr, pose[k].data_ptr(), model, out[k].data_ptr(), None,
+                                               stream.cuda_stream)
+                if rc != 0:
+                    raise RuntimeError(L.dugma_last_error().decode())
+
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                step(1)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        L.dugma_timing(h.arr, 1, None, None)
+        with Clocks(os.path.join(clock_dir, f"dugma_clocks_{name}.csv"), torch.cuda.current_device()) as clk:
+            for k in range(steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                step()
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        kms, kl = ctypes.c_double(0), ctypes.c_int(0)
+        L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
+        L.dugma_timing(h.arr, 0, None, None)
+        kernel_ms = kms.value / max(kl.value, 1)
+        pairs = P.N * P.M
+        instr = _instr(D, model)
+        ent.update({"steps": steps, "warmup": 3, "ms_per_step": ms, "pair_terms_per_s": pairs * poses / (ms * 1e-3),
+                    "evals_per_s": poses / (ms * 1e-3),
+                    "roofline": {"bound": "fp32", "instr_per_pair": instr, "kernel_ms": kernel_ms,
+                                 "achieved": instr * pairs / (kernel_ms * 1e-3) / 1e12, "unit": "Tinstr/s",
+                                 "frac": instr * pairs / (kernel_ms * 1e-3) / peak},
+                    "kernel_shape": list(api.get_shape(h, 0 if model == 0 else 3)),
+                    "l2": "flushed between steps (256 MiB write)"})
+        st = orc.State(P.X, P.X_C, P.Y, P.Y_C)
+        ent["accuracy"] = _accuracy(h, st, R, t, sig, model, _oracle_rows(P))
+        c = clk.summary()
+        if c:
+            ent["clocks"] = c
+        return ent
+    finally:
+        api.fr_m(h)
+
+
+def config_batch(L, peak, steps=5, clock_dir="/tmp"):
+    """The batched workload: 256 problems x 32 grid rotations in one persistent launch per
+    evaluation, tile shape autotuned, device time of each evaluation from the library's events."""
+    import torch
+    from dugma_b200 import api, synth
+    from oracle import oracle as orc
+    probs = synth.workload3()
+    grid = synth.so3_grid(synth.rng_for(3, 1), 32)
+    Q = len(grid)
+    sig = np.zeros((len(probs), Q))
+    for k, P in enumerate(probs):
+        _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+        sig[k, :] = api.update_sig(h, np.eye(3), P.t_G)
+        api.fr_m(h)
+    R = np.array([[g @ P.R_G for g in grid] for P in probs])
+    t = np.array([[P.t_G for _ in grid] for P in probs])
+    pairs = Q * sum(P.N * P.M for P in probs)
+    b = api.Batch([(P.X, P.X_C, P.Y, P.Y_C) for P in probs])
+    try:
+        tune = b.autotune(R, t, sig)
+        for _ in range(3):
+            E, g = b.energy_grad(R, t, sig)
+        torch.cuda.synchronize()
+        b.timing(1)
+        with Clocks(os.path.join(clock_dir, "dugma_clocks_batch.csv"), torch.cuda.current_device()) as clk:
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                E, g = b.energy_grad(R, t, sig)
+            wall = time.perf_counter() - t0
+        dev_ms, n = b.timing(2)
+        b.timing(0)
+        ms = dev_ms / max(n, 1)
+        instr = FP32_INSTR_ADJOINT
+        rng = np.random.default_rng(7)
+        errs = []
+        for p, q in zip(rng.choice(len(probs), 4, replace=False), rng.integers(0, Q, 4)):
+            P = probs[p]
+            Eo, go, _ = orc.State(P.X, P.X_C, P.Y, P.Y_C).energy(R[p, q], t[p, q], sig[p, q])
+            errs.append((abs(E[p, q] - Eo) / abs(Eo), float(np.linalg.norm(g[p, q] - go) / np.linalg.norm(go))))
+        ent = {"workload": "batch256x32: 256 problems, N, M uniform in [500, 8000], 32 rotations of a uniform "
+                           "SO(3) grid each, one persistent launch per evaluation (graph replay)",
+               "pair_terms_per_eval": int(pairs), "steps": steps, "warmup": 3, "ms_per_step": ms,
+               "pair_terms_per_s": pairs / (ms * 1e-3), "e2e_pair_terms_per_s": pairs * steps / wall,
+               "e2e_ms_per_step": 1e3 * wall / steps,
+               "roofline": {"bound": "fp32", "instr_per_pair": instr, "kernel_ms": ms,
+                            "achieved": instr * pairs / (ms * 1e-3) / 1e12, "unit": "Tinstr/s",
+                            "frac": instr * pairs / (ms * 1e-3) / peak,
+                            "note": "device time of the whole evaluation (records prologue, pair launch, reduction)"},
+               "kernel_shape": list(b.get_shape()), "autotune": tune,
+               "accuracy": {"pairs_checked": len(errs), "E_rel_err": max(e[0] for e in errs),
+                            "grad_rel_err": max(e[1] for e in errs), "tolerance": {"E": 1e-6, "grad": 1e-5},
+                            "against": "FP64 oracle, 4 sampled (problem, pose) pairs, all rows"},
+               "l2": "the records of all problems (4.5 GB) exceed L2; no flush"}
+        c = clk.summary()
+        if c:
+            ent["clocks"] = c
+        return ent
+    finally:
+        b.close()
+
+
+def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
+    """update_sig and compi through the plugin interface at the headline size (host R, t in, sigma /
+    637 coefficients out, like the reference's MEX gateways): wall time per call and the device
+    time of the pair kernels; compi's coefficients checked against the FP64 oracle on the 6K
+    workload, update_sig's nearest squared distances bit for bit on 4096 rows."""
+    import ctypes
+    import torch
+    from dugma_b200 import api, synth
+    from oracle import oracle as orc
+    R, t = eval_pose(P, 0)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    res = {}
+    try:
+        sig = api.update_sig(h, R, t)
+        for name, fn, instr in (("update_sig", lambda: api.update_sig(h, R, t), None),
+                                ("compi", lambda: api.compi(h, R, t, sig=sig), 2 * 35)):
+            fn()
+            torch.cuda.synchronize()
+            L.dugma_timing(h.arr, 1, None, None)
+            with Clocks(os.path.join(clock_dir, f"dugma_clocks_{name}.csv"), torch.cuda.current_device()) as clk:
+                walls = []
+                for _ in range(reps):
+                    a0 = time.perf_counter()
+                    fn()
+                    walls.append(time.perf_counter() - a0)
+            kms, kl = ctypes.c_double(0), ctypes.c_int(0)
+            L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
+            L.dugma_timing(h.arr, 0, None, None)
+            ms = 1e3 * float(np.median(walls))
+            ent = {"workload": f"{P.name}: N={P.N}, M={P.M}, host-to-host plugin call", "reps": reps, "warmup": 1,
+                   "ms_per_call": ms, "pair_terms_per_s": P.N * P.M / (ms * 1e-3),
+                   "pair_kernel_ms_per_call": kms.value / reps}
+            if instr:
+                ent["roofline"] = {"bound": "fp32", "instr_per_pair": instr,
+                                   "frac": instr * P.N * P.M / (kms.value / reps * 1e-3) / peak,
+                                   "note": "two coefficient passes of 35 FP32 lane-ops per pair each"}
+            c = clk.summary()
+            if c:
+                ent["clocks"] = c
+            res[name] = ent
+        # nearest squared distances of 4096 sampled rows, bit for bit
+        rows = 4096
+        idx, d2 = api.nn(h, R, t, 1)
+        st = orc.State(P.X[:rows], P.X_C[:rows], P.Y, P.Y_C)
+        oi, od = st.nn(R, t, 1)
+        res["update_sig"]["accuracy"] = {"rows": rows, "nn_idx_exact": bool(np.array_equal(idx[:rows], oi)),
+                                         "nn_d2_bit_exact": bool(np.array_equal(d2[:rows], od)),
+                                         "against": "FP64 oracle's FP32 distance sequence (update_sig.cu:238-259)"}
+    finally:
+        api.fr_m(h)
+    P1 = synth.workload1()
+    R1, t1 = eval_pose(P1, 0)
+    _, h = api.init(P1.X, P1.X_C, P1.Y, P1.Y_C)
+    try:
+        s1 = api.update_sig(h, R1, t1)
+        A = api.compi(h, R1, t1, sig=s1)
+        Ao = orc.State(P1.X, P1.X_C, P1.Y, P1.Y_C).coef(R1, t1, s1)[:637]
+        res["compi"]["accuracy"] = {"workload": "sphere6k", "max_abs_err_over_max_abs": float(
+            np.abs(A - Ao).max() / np.abs(Ao).max()), "tolerance": 2e-6, "against": "FP64 oracle, all 637"}
+    finally:
+        api.fr_m(h)
+    return res
+
+
+def run_configs(L, peak, clock_dir):
+    """Compact results of every configured workload besides the headline one."""
+    from dugma_b200 import synth
+    out = {}
+    timings = {}
+
+    def run(key, fn):
+        a0 = time.perf_counter()
+        try:
+            out[key] = fn()
+        except Exception as e:   # one failing entry must not hide the others
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+        timings[key] = round(time.perf_counter() - a0, 1)
+
+    run("cfg0_sphere1k", lambda: config_single(L, "cfg0", synth.workload0(), 0, peak, clock_dir=clock_dir))
+    run("cfg1_sphere6k", lambda: config_single(L, "cfg1", synth.workload1(), 0, peak, clock_dir=clock_dir))
+    run("cfg3_batch256x32", lambda: config_batch(L, peak, clock_dir=clock_dir))
+    run("cfg4_depth300k_64poses", lambda: config_single(L, "cfg4", synth.workload4(), 0, peak, steps=1, poses=64,
+                                                         nn_k=8, clock_dir=clock_dir))
+    run("curve2d_64k", lambda: config_single(L, "cfg5", synth.workload5(), 0, peak, clock_dir=clock_dir))
+    run("conv_harmonic64k", lambda: config_single(L, "conv", synth.workload2(), 1, peak, clock_dir=clock_dir))
+    run("plugins_harmonic64k", lambda: config_plugins(L, synth.workload2(), peak, clock_dir=clock_dir))
+    out["seconds"] = timings
+    return out
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args.gpus)
@@ -585,6 +849,11 @@ def main():
                     "grad_rel_err": float(np.max(np.abs(gg - go)) / np.max(np.abs(go))) if np.any(go) else None,
                     "tolerance": {"E": 1e-6, "grad": 1e-5}}
 
+    configs = None
+    if not args.no_configs and world == 1 and args.workload == 2 and not args.n and args.model == 0:
+        import tempfile
+        configs = run_configs(L, peak.value, tempfile.gettempdir())
+
     if rank == 0:
         clocks = clk.summary()
         line = {
@@ -599,6 +868,9 @@ def main():
                          "unit": "Tinstr/s (FP32 pipe, lane ops)", "frac": achieved / peak.value,
                          "traffic": profiled_traffic(shape_key) if (args.workload == 2 and not args.n and args.model == 0)
                          else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this bench command, "
+                                           "committed in profiles/adjoint_packed_harmonic64k.txt (shape 4,64,64,2); "
+                                           "null when this run's shape or workload differs",
                          "algorithmic_bytes": 64 * (P.N + P.M),
                          "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json has "
                                         "no FP32-pipe figure)",
@@ -618,6 +890,8 @@ def main():
         if clocks:
             line["clocks"] = clocks
         line.update(extra)
+        if configs:
+            line["configs"] = configs
         print(json.dumps(line), flush=True)
     api.fr_m(h)
     if world > 1:

@@ -47,6 +47,11 @@ EXPORTS = {
     "dugma_batch_create": (c_int, [c_int, c_int, ip, ip, P(dp), P(dp), P(dp), P(dp), P(c_void_p)]),
     "dugma_batch_energy_grad": (c_int, [c_void_p, c_int, dp, c_int, dp]),
     "dugma_batch_destroy": (c_int, [c_void_p]),
+    "dugma_batch_shapes": (c_int, [ip, c_int]),
+    "dugma_batch_set_shape": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "dugma_batch_get_shape": (c_int, [c_void_p, ip]),
+    "dugma_batch_autotune": (c_int, [c_void_p, c_int, dp, ctypes.c_char_p, c_size_t]),
+    "dugma_batch_timing": (c_int, [c_void_p, c_int, dp, ip]),
     "dugma_register": (c_int, [dp, dp, dp, dp, c_int, c_int, c_int, dp, dp, c_int, c_double, c_double, c_double,
                                c_int, dp, dp, dp]),
     "dugma_version": (ctypes.c_char_p, []),

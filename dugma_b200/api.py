@@ -239,18 +239,50 @@ class Batch:
         self.b = ctypes.c_void_p()
         check(_lib.load().dugma_batch_create(P, D, N, M, ptr(0), ptr(1), ptr(2), ptr(3), ctypes.byref(self.b)))
 
-    def energy_grad(self, R, t, sig):
-        """R (P, Q, D, D), t (P, Q, D), sig (P, Q) -> E (P, Q), g (P, Q, NG)."""
+    def _poses(self, R, t, sig):
         R, t, sig = np.asarray(R, float), np.asarray(t, float), np.asarray(sig, float)
         P, Q = sig.shape
         rec = np.zeros((P, Q, 13))
         rec[:, :, : self.D * self.D] = np.transpose(R, (0, 1, 3, 2)).reshape(P, Q, -1)
         rec[:, :, 9:9 + self.D] = t
         rec[:, :, 12] = sig
+        return _d(rec), Q
+
+    def energy_grad(self, R, t, sig):
+        """R (P, Q, D, D), t (P, Q, D), sig (P, Q) -> E (P, Q), g (P, Q, NG)."""
+        rec, Q = self._poses(R, t, sig)
         ng = ngrad(self.D)
-        out = np.zeros((P, Q, 1 + ng))
-        check(_lib.load().dugma_batch_energy_grad(self.b, Q, _ptr(_d(rec)), 0, _ptr(out)))
+        out = np.zeros((self.P, Q, 1 + ng))
+        check(_lib.load().dugma_batch_energy_grad(self.b, Q, _ptr(rec), 0, _ptr(out)))
         return out[:, :, 0].copy(), out[:, :, 1:].copy()
+
+    def autotune(self, R, t, sig) -> str:
+        """Times every batch tile shape on these poses and keeps the fastest; returns the report."""
+        rec, Q = self._poses(R, t, sig)
+        buf = ctypes.create_string_buffer(2048)
+        check(_lib.load().dugma_batch_autotune(self.b, Q, _ptr(rec), buf, len(buf)))
+        return buf.value.decode()
+
+    def set_shape(self, shape):
+        check(_lib.load().dugma_batch_set_shape(self.b, *[int(v) for v in shape]))
+
+    def get_shape(self):
+        s = (ctypes.c_int * 4)()
+        check(_lib.load().dugma_batch_get_shape(self.b, s))
+        return tuple(s)
+
+    def timing(self, mode):
+        """mode 1 start, 0 stop, 2 -> (total device ms, evaluations) since mode 1."""
+        ms, n = ctypes.c_double(0), ctypes.c_int(0)
+        check(_lib.load().dugma_batch_timing(self.b, int(mode), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    @staticmethod
+    def shapes():
+        n = _lib.load().dugma_batch_shapes(None, 0)
+        s = (ctypes.c_int * (4 * n))()
+        _lib.load().dugma_batch_shapes(s, n)
+        return [tuple(s[4 * k:4 * k + 4]) for k in range(n)]
 
     def close(self):
         if self.b:

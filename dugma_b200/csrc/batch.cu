@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "bodies.cuh"
@@ -21,7 +22,12 @@
 
 namespace dugma {
 
-constexpr int kBatchNT = 64, kBatchTJ = 64, kBatchIPT = 4, kBatchChunk = 512;   // chunk in pair records
+// Tile shapes of the batched launch: sources per thread, threads per block, pair records per
+// shared-memory tile, and pair records per work item (the chunk of a problem's targets one item
+// covers).  dugma_batch_autotune times them on the caller's poses and keeps the fastest.
+struct BatchShape {
+    int ipt, nt, tj, chunk;
+};
 
 struct PQDesc {
     const float *x, *xinv, *lwx, *y, *yinv, *lwy, *wx;
@@ -215,8 +221,38 @@ __global__ void batch_reduce_kernel(const double* __restrict__ partials, const i
     }
 }
 
+using BatchKernelFn = void (*)(const PQDesc*, const BatchItem*, int, double*, int*, int*);
+struct BatchVariant {
+    BatchShape sh;
+    BatchKernelFn chol, horner;   // Cholesky-form and Horner-form source records
+};
+
+template <int D, int IPT, int NT, int TJ>
+static BatchVariant batch_variant(int chunk)
+{
+    return {{IPT, NT, TJ, chunk}, batch_pairs_kernel<PackedBody<D, IPT, true, true>, NT, TJ, 4>,
+            batch_pairs_kernel<PackedBody<D, IPT, true, false>, NT, TJ, 4>};
+}
+
+template <int D>
+static const std::vector<BatchVariant>& batch_variants()
+{
+    static const std::vector<BatchVariant> v = {
+        batch_variant<D, 4, 64, 64>(512),  batch_variant<D, 4, 64, 64>(256), batch_variant<D, 4, 64, 64>(1024),
+        batch_variant<D, 4, 64, 32>(256),  batch_variant<D, 2, 128, 64>(512), batch_variant<D, 2, 128, 32>(256),
+    };
+    return v;
+}
+
+static const BatchShape& batch_shape_of(int D, int k)
+{
+    return D == 3 ? batch_variants<3>()[k].sh : batch_variants<2>()[k].sh;
+}
+
 struct Batch {
     int D = 3, P = 0;
+    int shape = 0;                    // index into batch_variants<D>()
+    int prepared_shape = -1;          // the shape the pose-count state below was built for
     std::vector<float*> ptrs;          // 6 per problem
     std::vector<Context*> ctx;
     cudaStream_t stream = nullptr;
@@ -230,6 +266,10 @@ struct Batch {
     double *partials = nullptr, *out = nullptr;
     double* host = nullptr;           // pinned: poses in, results out
     size_t host_doubles = 0;
+    // optional device timing of each evaluation (dugma_batch_timing)
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tevents;
+    size_t tused = 0;
     int max_span = 0;
     bool chol = true;                 // every problem's weighted sources have Cholesky factors
     cudaGraphExec_t exec = nullptr;
@@ -251,13 +291,14 @@ struct Batch {
 
 static int batch_prepare(Batch& b, int n_poses)
 {
-    if (b.n_poses == n_poses) return DUGMA_OK;
+    if (b.n_poses == n_poses && b.prepared_shape == b.shape) return DUGMA_OK;
     cudaStreamSynchronize(b.stream);
     b.release_pose_state();
     const int D = b.D, NG = D == 3 ? 6 : 3;
     b.nv = 1 + NG;
     const int n_pq = b.P * n_poses;
-    constexpr int BI = kBatchIPT * kBatchNT;
+    const BatchShape& sh = batch_shape_of(D, b.shape);
+    const int BI = sh.ipt * sh.nt;
     // sizes and the work list (cost = rows x tiles; largest first)
     std::vector<size_t> yoff(n_pq), xoff(n_pq);
     size_t ybytes = 0, xbytes = 0;
@@ -266,8 +307,8 @@ static int batch_prepare(Batch& b, int n_poses)
     b.max_span = 0;
     for (int p = 0; p < b.P; ++p) {
         const Context& c = *b.ctx[p];
-        const int total_tiles = c.M_pad / 2 / kBatchTJ;
-        const int chunk_tiles = kBatchChunk / kBatchTJ;
+        const int total_tiles = c.M_pad / 2 / sh.tj;
+        const int chunk_tiles = sh.chunk / sh.tj;
         b.max_span = std::max(b.max_span, std::max(c.M_pad, c.N));
         for (int q = 0; q < n_poses; ++q) {
             const int pq = p * n_poses + q;
@@ -355,27 +396,85 @@ static int batch_prepare(Batch& b, int n_poses)
         return set_error(DUGMA_ERR_NOMEM, "batch: pinned staging allocation failed");
     }
     b.n_poses = n_poses;
+    b.prepared_shape = b.shape;
     return DUGMA_OK;
 }
 
 template <int D>
 static int batch_enqueue(Batch& b, cudaStream_t s)
 {
-    auto fn = b.chol ? batch_pairs_kernel<PackedBody<D, kBatchIPT, true, true>, kBatchNT, kBatchTJ, 4>
-                     : batch_pairs_kernel<PackedBody<D, kBatchIPT, true, false>, kBatchNT, kBatchTJ, 4>;
+    const BatchVariant& var = batch_variants<D>()[b.shape];
+    const BatchKernelFn fn = b.chol ? var.chol : var.horner;
     const int n_pq = b.P * b.n_poses;
     int sms = 148, per_sm = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.ctx[0]->dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBatchNT, 0);
+    DUGMA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.ctx[0]->dev));
+    DUGMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, var.sh.nt, 0));
     const int grid = std::min(std::max(per_sm, 1) * sms, b.n_items);
     const int gx = std::min((b.max_span + 255) / 256, 64);
     batch_prologue_kernel<D><<<dim3(gx, n_pq), 256, 0, s>>>(b.desc, b.max_span);
     DUGMA_CK(cudaGetLastError());
     DUGMA_CK(cudaMemsetAsync(b.counter, 0, 8 * sizeof(int), s));
-    fn<<<grid, kBatchNT, 0, s>>>(b.desc, b.items, b.n_items, b.partials, b.counter, b.err);
+    fn<<<grid, var.sh.nt, 0, s>>>(b.desc, b.items, b.n_items, b.partials, b.counter, b.err);
     DUGMA_CK(cudaGetLastError());
     batch_reduce_kernel<<<n_pq, 128, 0, s>>>(b.partials, b.pq_start, b.pq_items, b.nv, b.out);
     DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
+// Replays (or, the first time at this pose count and shape, runs eagerly and captures) one
+// evaluation on the batch stream, with CUDA events around it when timing is on.
+static int batch_launch(Batch& b)
+{
+    cudaEvent_t ev1 = nullptr;
+    if (b.timing) {
+        if (b.tused == b.tevents.size()) {
+            cudaEvent_t e0, e1;
+            DUGMA_CK(cudaEventCreate(&e0));
+            DUGMA_CK(cudaEventCreate(&e1));
+            b.tevents.push_back({e0, e1});
+        }
+        DUGMA_CK(cudaEventRecord(b.tevents[b.tused].first, b.stream));
+        ev1 = b.tevents[b.tused].second;
+        ++b.tused;
+    }
+    if (!b.exec) {
+        DUGMA_RET(b.D == 3 ? batch_enqueue<3>(b, b.stream) : batch_enqueue<2>(b, b.stream));
+        if (ev1) DUGMA_CK(cudaEventRecord(ev1, b.stream));
+        DUGMA_CK(cudaStreamSynchronize(b.stream));
+        DUGMA_CK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = b.D == 3 ? batch_enqueue<3>(b, b.stream) : batch_enqueue<2>(b, b.stream);
+        const cudaError_t e = cudaStreamEndCapture(b.stream, &b.graph);
+        if (rc != DUGMA_OK || e != cudaSuccess) return rc != DUGMA_OK ? rc : set_error(DUGMA_ERR_CUDA, "batch capture failed");
+        DUGMA_CK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+        return DUGMA_OK;
+    }
+    DUGMA_CK(cudaGraphLaunch(b.exec, b.stream));
+    if (ev1) DUGMA_CK(cudaEventRecord(ev1, b.stream));
+    return DUGMA_OK;
+}
+
+static int batch_eval(Batch& b, int n_poses, const double* poses, double* out)
+{
+    DUGMA_RET(batch_prepare(b, n_poses));
+    const int n_pq = b.P * n_poses, D = b.D;
+    for (int k = 0; k < n_pq; ++k) {
+        double* h = b.host + 16 * (size_t)k;
+        for (int q = 0; q < 16; ++q) h[q] = 0.0;
+        const double* src = poses + 13 * (size_t)k;
+        for (int q = 0; q < D * D; ++q) h[q] = src[q];
+        for (int a = 0; a < D; ++a) h[kPoseT + a] = src[9 + a];
+        h[kPoseSig] = src[12];
+        if (!(src[12] > 0)) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: sig of pose %d is not positive", k);
+    }
+    DUGMA_CK(cudaMemcpyAsync(b.poses, b.host, sizeof(double) * 16 * n_pq, cudaMemcpyHostToDevice, b.stream));
+    DUGMA_RET(batch_launch(b));
+    const int nv = b.nv;
+    DUGMA_CK(cudaMemcpyAsync(out, b.out, sizeof(double) * nv * n_pq, cudaMemcpyDeviceToHost, b.stream));
+    int err = 0;
+    DUGMA_CK(cudaMemcpyAsync(b.host + 16 * (size_t)n_pq, b.err, sizeof(int), cudaMemcpyDeviceToHost, b.stream));
+    DUGMA_CK(cudaStreamSynchronize(b.stream));
+    memcpy(&err, b.host + 16 * (size_t)n_pq, sizeof(int));
+    if (err) return set_error(DUGMA_ERR_TIMEOUT, "batch: a device wait gave up (0x%x)", err);
     return DUGMA_OK;
 }
 
@@ -420,37 +519,122 @@ int dugma_batch_energy_grad(void* batch, int n_poses, const double* poses, int m
     Batch* b = static_cast<Batch*>(batch);
     if (!b || n_poses < 1 || !poses || !out) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: bad arguments");
     if (model != DUGMA_MODEL_REF) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: the batched path is REF only");
-    DUGMA_RET(batch_prepare(*b, n_poses));
-    const int n_pq = b->P * n_poses, D = b->D;
-    for (int k = 0; k < n_pq; ++k) {
-        double* h = b->host + 16 * (size_t)k;
-        for (int q = 0; q < 16; ++q) h[q] = 0.0;
-        const double* src = poses + 13 * (size_t)k;
-        for (int q = 0; q < D * D; ++q) h[q] = src[q];
-        for (int a = 0; a < D; ++a) h[kPoseT + a] = src[9 + a];
-        h[kPoseSig] = src[12];
-        if (!(src[12] > 0)) return set_error(DUGMA_ERR_ARG, "batch_energy_grad: sig of pose %d is not positive", k);
+    return batch_eval(*b, n_poses, poses, out);
+}
+
+int dugma_batch_shapes(int* shapes, int max)
+{
+    const std::vector<BatchVariant>& v = batch_variants<3>();
+    const int n = (int)v.size();
+    for (int k = 0; k < n && k < max && shapes; ++k) {
+        shapes[4 * k] = v[k].sh.ipt;
+        shapes[4 * k + 1] = v[k].sh.nt;
+        shapes[4 * k + 2] = v[k].sh.tj;
+        shapes[4 * k + 3] = v[k].sh.chunk;
     }
-    DUGMA_CK(cudaMemcpyAsync(b->poses, b->host, sizeof(double) * 16 * n_pq, cudaMemcpyHostToDevice, b->stream));
-    if (!b->exec) {
-        // first evaluation at this pose count: run eagerly, then capture the same work as a graph
-        DUGMA_RET(D == 3 ? batch_enqueue<3>(*b, b->stream) : batch_enqueue<2>(*b, b->stream));
-        DUGMA_CK(cudaStreamSynchronize(b->stream));
-        DUGMA_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = D == 3 ? batch_enqueue<3>(*b, b->stream) : batch_enqueue<2>(*b, b->stream);
-        const cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
-        if (rc != DUGMA_OK || e != cudaSuccess) return rc != DUGMA_OK ? rc : set_error(DUGMA_ERR_CUDA, "batch capture failed");
-        DUGMA_CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
-    } else {
-        DUGMA_CK(cudaGraphLaunch(b->exec, b->stream));
+    return n;
+}
+
+int dugma_batch_set_shape(void* batch, int ipt, int nt, int tj, int chunk)
+{
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b) return set_error(DUGMA_ERR_ARG, "batch_set_shape: null batch");
+    const int n = (int)batch_variants<3>().size();
+    for (int k = 0; k < n; ++k) {
+        const BatchShape& sh = batch_shape_of(b->D, k);
+        if (sh.ipt == ipt && sh.nt == nt && sh.tj == tj && sh.chunk == chunk) {
+            b->shape = k;
+            return DUGMA_OK;
+        }
     }
-    const int nv = b->nv;
-    DUGMA_CK(cudaMemcpyAsync(out, b->out, sizeof(double) * nv * n_pq, cudaMemcpyDeviceToHost, b->stream));
-    int err = 0;
-    DUGMA_CK(cudaMemcpyAsync(b->host + 16 * (size_t)n_pq, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
-    DUGMA_CK(cudaStreamSynchronize(b->stream));
-    memcpy(&err, b->host + 16 * (size_t)n_pq, sizeof(int));
-    if (err) return set_error(DUGMA_ERR_TIMEOUT, "batch: a device wait gave up (0x%x)", err);
+    return set_error(DUGMA_ERR_ARG, "batch_set_shape: (%d, %d, %d, %d) is not a compiled shape", ipt, nt, tj, chunk);
+}
+
+int dugma_batch_get_shape(void* batch, int shape[4])
+{
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b || !shape) return set_error(DUGMA_ERR_ARG, "batch_get_shape: null argument");
+    const BatchShape& sh = batch_shape_of(b->D, b->shape);
+    shape[0] = sh.ipt;
+    shape[1] = sh.nt;
+    shape[2] = sh.tj;
+    shape[3] = sh.chunk;
+    return DUGMA_OK;
+}
+
+int dugma_batch_autotune(void* batch, int n_poses, const double* poses, char* report, size_t report_len)
+{
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b || n_poses < 1 || !poses) return set_error(DUGMA_ERR_ARG, "batch_autotune: bad arguments");
+    const int nv = 1 + (b->D == 3 ? 6 : 3);
+    std::vector<double> out((size_t)b->P * n_poses * nv);
+    const int n = (int)batch_variants<3>().size();
+    const bool was_timing = b->timing;
+    const size_t was_used = b->tused;
+    std::string rep;
+    double best = 1e300;
+    int best_k = b->shape;
+    cudaEvent_t e0, e1;
+    DUGMA_CK(cudaEventCreate(&e0));
+    DUGMA_CK(cudaEventCreate(&e1));
+    b->timing = false;
+    int rc = DUGMA_OK;
+    for (int k = 0; k < n && rc == DUGMA_OK; ++k) {
+        b->shape = k;
+        rc = batch_eval(*b, n_poses, poses, out.data());   // first run: prepares and captures
+        if (rc != DUGMA_OK) break;
+        const int reps = 2;
+        float ms = 0;
+        cudaEventRecord(e0, b->stream);
+        for (int r = 0; r < reps && rc == DUGMA_OK; ++r) rc = batch_launch(*b);
+        cudaEventRecord(e1, b->stream);
+        if (rc != DUGMA_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            rc = set_error(DUGMA_ERR_CUDA, "batch_autotune: event timing failed");
+        ms /= reps;
+        const BatchShape& sh = batch_shape_of(b->D, k);
+        char buf[96];
+        snprintf(buf, sizeof(buf), "%s(ipt=%d,nt=%d,tj=%d,chunk=%d):%.3fms", rep.empty() ? "" : " ", sh.ipt, sh.nt,
+                 sh.tj, sh.chunk, ms);
+        rep += buf;
+        if (ms < best) {
+            best = ms;
+            best_k = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->timing = was_timing;
+    b->tused = was_used;
+    b->shape = best_k;
+    if (rc != DUGMA_OK) return rc;
+    if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
+    return DUGMA_OK;
+}
+
+int dugma_batch_timing(void* batch, int mode, double* total_ms, int* launches)
+{
+    Batch* b = static_cast<Batch*>(batch);
+    if (!b) return set_error(DUGMA_ERR_ARG, "batch_timing: null batch");
+    if (mode == 1) {
+        b->timing = true;
+        b->tused = 0;
+        return DUGMA_OK;
+    }
+    if (mode == 0) {
+        b->timing = false;
+        return DUGMA_OK;
+    }
+    if (mode != 2) return set_error(DUGMA_ERR_ARG, "batch_timing: mode must be 0, 1 or 2");
+    double tot = 0;
+    for (size_t k = 0; k < b->tused; ++k) {
+        DUGMA_CK(cudaEventSynchronize(b->tevents[k].second));
+        float ms = 0;
+        DUGMA_CK(cudaEventElapsedTime(&ms, b->tevents[k].first, b->tevents[k].second));
+        tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = (int)b->tused;
     return DUGMA_OK;
 }
 
@@ -462,6 +646,10 @@ int dugma_batch_destroy(void* batch)
     b->release_pose_state();
     for (int p = 0; p < b->P; ++p) dugma_fr_m(&b->ptrs[6 * (size_t)p]);
     if (b->stream) cudaStreamDestroy(b->stream);
+    for (auto& e : b->tevents) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     delete b;
     return DUGMA_OK;
 }

@@ -219,7 +219,9 @@ def emit_monomials(res3, res2, path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DUGMA_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        raise SystemExit("usage: python -m dugma_b200.gen.gen_coef REFERENCE_TREE (or set DUGMA_REFERENCE)")
     res3 = derive(3, ref)
     res2 = derive(2, ref)
     for r in (res3, res2):

@@ -189,6 +189,20 @@ int dugma_batch_create(int n_problems, int D, const int* N, const int* M, const 
 int dugma_batch_energy_grad(void* batch, int n_poses, const double* poses, int model, double* out);
 int dugma_batch_destroy(void* batch);
 
+/* Tile shapes of the batched launch: writes up to `max` tuples {sources per thread, threads per
+ * block, pair records per tile, pair records per work item} into shapes[4 * k] and returns the
+ * count.  No counterpart in the reference (its kernels have one fixed 32 x 32 launch shape). */
+int dugma_batch_shapes(int* shapes, int max);
+int dugma_batch_set_shape(void* batch, int ipt, int nt, int tj, int chunk);
+int dugma_batch_get_shape(void* batch, int shape[4]);
+/* Times every batch shape on these poses (as dugma_batch_energy_grad takes them) and keeps the
+ * fastest; writes a one-line report into `report` (may be NULL). */
+int dugma_batch_autotune(void* batch, int n_poses, const double* poses, char* report, size_t report_len);
+/* CUDA events around every batched evaluation on the device (the records' prologue, the
+ * persistent pair launch and the per-pose reduction): mode 1 start and clear, 0 stop, 2
+ * synchronise and report the summed duration in ms and the number of evaluations. */
+int dugma_batch_timing(void* batch, int mode, double* total_ms, int* launches);
+
 /* ---------------- registration driver ---------------- */
 
 enum {

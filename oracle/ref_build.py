@@ -16,7 +16,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# the reference tree: DUGMA_REFERENCE, else where this build environment mounts it (the one place
+# the path is named); absent on machines that only run the prebuilt objects
 REF = os.environ.get("DUGMA_REFERENCE", "/root/reference")
+
+
+def reference_tree() -> str | None:
+    """The reference tree if it is present on this machine, else None."""
+    return REF if os.path.isdir(REF) else None
 PLUGINS = ("init", "update_sig", "compi")
 
 

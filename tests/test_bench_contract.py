@@ -84,3 +84,19 @@ def test_bench_line_on_gpu():
     acc = d["accuracy"]
     assert acc["E_rel_err"] <= acc["tolerance"]["E"] and acc["grad_rel_err"] <= acc["tolerance"]["grad"]
     assert d["plain_fd"]["adjoint_speedup"] > 1
+
+
+@pytest.mark.gpu
+def test_configs_entry_on_gpu(tmp_path):
+    """One entry of the default run's `configs` key (the 1K sphere): device timing, roofline,
+    error against the FP64 oracle within the contract, and a clock record."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from dugma_b200 import _lib, synth
+    ent = bench.config_single(_lib.load(), "cfg0", synth.workload0(), 0, 36.0e12, steps=3, clock_dir=str(tmp_path))
+    assert ent["ms_per_step"] > 0 and ent["pair_terms_per_s"] > 0 and ent["steps"] == 3 and ent["warmup"] >= 3
+    assert 0 < ent["roofline"]["frac"] and ent["roofline"]["kernel_ms"] > 0
+    acc = ent["accuracy"]
+    assert acc["rows"] == 1000
+    assert acc["E_rel_err"] <= acc["tolerance"]["E"] and acc["grad_rel_err"] <= acc["tolerance"]["grad"]
+    assert set(ent["clocks"]) >= {"sm_mhz", "sm_max_mhz", "reasons"}

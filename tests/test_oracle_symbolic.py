@@ -13,8 +13,10 @@ import re
 
 import pytest
 
-REF = "/root/reference"
-pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+from oracle.ref_build import reference_tree
+
+REF = reference_tree()
+pytestmark = pytest.mark.skipif(REF is None, reason="reference tree not present (DUGMA_REFERENCE)")
 
 
 def _ref_terms(body):
