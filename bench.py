@@ -24,7 +24,8 @@ configs     (default run, one GPU) compact results of the other configured workl
             with its own device timing, roofline fraction, error against the FP64 oracle and
             clock record: the 1K and 6K spheres, the batch of 256 problems x 32 rotations, the
             300K depth views with 64 poses and the k = 8 neighbour pass, the 2D curve, the CONV
-            model, and update_sig / compi through the plugin interface at 64K.
+            model, update_sig / compi through the plugin interface at 64K, and the end-to-end
+            registration of the reference's 30 real Kinect scenes (both modes).
 
 Workloads (--workload): 0 1K sphere, 1 6K sphere with outliers, 2 the 64K harmonic surface
 (default), 3 256 problems x 32 poses in one persistent launch, 4 300K depth views, 5 the 2D
@@ -624,6 +625,26 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
     return res
 
 
+def config_kinect(modes=(0, 1)):
+    """The reference's 30 real Kinect scenes (tests/golden/kinect_scenes.npz) registered end to end
+    from the identity pose with main_kinect_real_application.m's settings: per mode, the medians of
+    the error measures against the ground truth, the distance to the authors' recorded poses, and
+    the seconds per scene (host clouds in, pose out) against the authors' recorded seconds."""
+    from dugma_b200 import evaluate
+    path = os.path.join(ROOT, "tests", "golden", "kinect_scenes.npz")
+    out = {"workload": "kinect30: the reference's 30 two-Kinect scenes (N, M 463..5334), identity start, 300 "
+                       "iterations, tolerances 1e-4 / 1e-8 / 1e-9"}
+    for mode in modes:
+        rows = [evaluate.register(P, mode, 300, rec) for P, rec in evaluate.scenes_from_npz(path)]
+        s = evaluate.summarise(rows, mode)
+        out[f"mode{mode}"] = {k: s[k]["median"] for k in ("error_R", "error_t", "deg", "iterations", "seconds",
+                                                          "vs_recorded_deg", "vs_recorded_t", "recorded_error_R",
+                                                          "recorded_error_t", "recorded_seconds")}
+        out[f"mode{mode}"]["max_vs_recorded_deg"] = s["vs_recorded_deg"]["max"]
+        out[f"mode{mode}"]["statistic"] = "median over the 30 scenes (max where named)"
+    return out
+
+
 def run_configs(L, peak, clock_dir):
     """Compact results of every configured workload besides the headline one."""
     from dugma_b200 import synth
@@ -646,6 +667,7 @@ def run_configs(L, peak, clock_dir):
     run("curve2d_64k", lambda: config_single(L, "cfg5", synth.workload5(), 0, peak, clock_dir=clock_dir))
     run("conv_harmonic64k", lambda: config_single(L, "conv", synth.workload2(), 1, peak, clock_dir=clock_dir))
     run("plugins_harmonic64k", lambda: config_plugins(L, synth.workload2(), peak, clock_dir=clock_dir))
+    run("kinect30_registration", config_kinect)
     out["seconds"] = timings
     return out
 

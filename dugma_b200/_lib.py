@@ -44,6 +44,9 @@ EXPORTS = {
     "dugma_graph_create": (c_int, [PtrArray, c_int, P(c_void_p)]),
     "dugma_graph_eval": (c_int, [c_void_p, dp, dp, c_double, dp, dp]),
     "dugma_graph_destroy": (c_int, [c_void_p]),
+    "dugma_em_graph_create": (c_int, [PtrArray, P(c_void_p)]),
+    "dugma_em_step": (c_int, [c_void_p, dp, dp, fp, dp]),
+    "dugma_em_graph_destroy": (c_int, [c_void_p]),
     "dugma_batch_create": (c_int, [c_int, c_int, ip, ip, P(dp), P(dp), P(dp), P(dp), P(c_void_p)]),
     "dugma_batch_energy_grad": (c_int, [c_void_p, c_int, dp, c_int, dp]),
     "dugma_batch_destroy": (c_int, [c_void_p]),

@@ -310,6 +310,27 @@ class Graph:
             self.g = ctypes.c_void_p()
 
 
+class EMGraph:
+    """update_sig at a pose followed by compi at that pose and sigma, as one captured graph."""
+
+    def __init__(self, h: Handles):
+        self.h = h
+        self.g = ctypes.c_void_p()
+        check(_lib.load().dugma_em_graph_create(h.arr, ctypes.byref(self.g)))
+
+    def __call__(self, R, t):
+        """-> (sigma as update_sig returns it, the 637 / 45 coefficients as compi returns them)."""
+        sig = ctypes.c_float(0)
+        A = np.zeros(640)
+        check(_lib.load().dugma_em_step(self.g, _ptr(_cm(R)), _ptr(_d(t)), ctypes.byref(sig), _ptr(A)))
+        return float(sig.value), A[:637 if self.h.D == 3 else 45].copy()
+
+    def close(self):
+        if self.g:
+            check(_lib.load().dugma_em_graph_destroy(self.g))
+            self.g = ctypes.c_void_p()
+
+
 def DUGMA(X, Y, X_C, Y_C, R0, t0, Max_Iteration=300, accuracy_rotation=1e-4, accuracy_translation=1e-8,
           accuracy_sig=1e-8, mode=_lib.DRIVE_REFERENCE):
     """The registration loop of DUGMA.m:19-137 (fmincon replaced by a quasi-Newton solver).

@@ -861,6 +861,105 @@ int dugma_graph_destroy(void* graph)
     return DUGMA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// One EM iteration of the reference loop as a CUDA graph: update_sig at the new pose, its
+// sigma written into the device pose block, compi at (R, t, sigma), and one copy of sigma and
+// the surrogate moments back (DUGMA.m:60 and :105 without the host round trip between them)
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace dugma {
+constexpr int kHostMoments = 512;   // c.host[512, 512 + moments): the moments copied back
+
+__global__ void pose_sig_from_sigma_kernel(double* pose, const double* sig_out)
+{
+    pose[kPoseSig] = sig_out[1];   // the quantised sigma, rounded to float as update_sig returns it
+}
+
+static int em_enqueue(Context& c, cudaStream_t s)
+{
+    DUGMA_CK(cudaMemcpyAsync(c.pose, c.host, sizeof(double) * kPoseDoubles, cudaMemcpyHostToDevice, s));
+    DUGMA_CK(cudaMemsetAsync(c.err, 0, sizeof(int), s));
+    DUGMA_RET(launch_sigma(c, c.pose, c.out, s));
+    pose_sig_from_sigma_kernel<<<1, 1, 0, s>>>(c.pose, c.out);
+    DUGMA_CK(cudaGetLastError());
+    DUGMA_RET(launch_coef(c, c.pose, c.mom, s));
+    DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * num_moments(c.D), cudaMemcpyDeviceToHost, s));
+    DUGMA_CK(cudaMemcpyAsync(c.host + 64, c.out, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    DUGMA_CK(cudaMemcpyAsync(c.host + 63, c.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return DUGMA_OK;
+}
+
+struct EMGraph {
+    Context* c = nullptr;
+    float* ptr[6];
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+}  // namespace dugma
+
+extern "C" {
+
+int dugma_em_graph_create(float* Ptr[6], void** out)
+{
+    if (!out) return set_error(DUGMA_ERR_ARG, "em_graph_create: null argument");
+    GET_CTX(c, Ptr);
+    static_assert(kHostMoments + kNumMomentsMax <= kHostDoubles, "moment staging exceeds the pinned block");
+    // one eager step first: sizes the scratch, allocates the coefficient records and uploads the
+    // moment tables, so that nothing allocates or synchronises during the capture
+    const double Rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, R2[4] = {1, 0, 0, 1}, t0[3] = {0, 0, 0};
+    pack_pose(*c, c->D == 3 ? Rm : R2, t0, 0.0, c->host);
+    DUGMA_RET(em_enqueue(*c, c->stream));
+    DUGMA_CK(cudaStreamSynchronize(c->stream));
+    EMGraph* g = new EMGraph;
+    g->c = c;
+    for (int k = 0; k < 6; ++k) g->ptr[k] = Ptr[k];
+    DUGMA_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = em_enqueue(*c, c->stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc != DUGMA_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        delete g;
+        return rc != DUGMA_OK ? rc : set_error(DUGMA_ERR_CUDA, "em graph capture failed: %s", cudaGetErrorString(e));
+    }
+    g->graph = graph;
+    if (cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        delete g;
+        return set_error(DUGMA_ERR_CUDA, "em graph instantiation failed");
+    }
+    *out = g;
+    return DUGMA_OK;
+}
+
+int dugma_em_step(void* graph, const double* R, const double* t, float sig[1], double coefficient[640])
+{
+    EMGraph* g = static_cast<EMGraph*>(graph);
+    if (!g || !R || !t || !sig || !coefficient) return set_error(DUGMA_ERR_ARG, "em_step: null argument");
+    Context* c = find_context(g->ptr);
+    if (c != g->c) return set_error(DUGMA_ERR_STATE, "em_step: the context of this graph was freed");
+    std::lock_guard<std::mutex> lk(c->mu);
+    pack_pose(*c, R, t, 0.0, c->host);
+    DUGMA_CK(cudaGraphLaunch(g->exec, c->stream));
+    DUGMA_CK(cudaStreamSynchronize(c->stream));
+    int err = 0;
+    memcpy(&err, c->host + 63, sizeof(int));
+    if (err) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", err);
+    sig[0] = (float)c->host[65];
+    return coef_from_moments(c->D, c->host + kHostMoments, coefficient);
+}
+
+int dugma_em_graph_destroy(void* graph)
+{
+    EMGraph* g = static_cast<EMGraph*>(graph);
+    if (!g) return set_error(DUGMA_ERR_ARG, "em_graph_destroy: null graph");
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return DUGMA_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

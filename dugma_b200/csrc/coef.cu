@@ -389,6 +389,7 @@ __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, cons
 }
 
 
+static_assert(kNumMoments3D <= kNumMomentsMax && kNumMoments2D <= kNumMomentsMax, "moment count bound");
 int num_moments(int D) { return D == 3 ? kNumMoments3D : kNumMoments2D; }
 
 int Context::ensure_coef_records()

@@ -30,6 +30,7 @@ constexpr int kHostDoubles = 1024;
 constexpr int kPadI = 1024;   // source rows padded to a multiple (largest i-block)
 constexpr int kPadJ = 128;    // target rows padded to a multiple (largest j-tile)
 constexpr int kMomSlots = 512;   // doubles in Context::mom (moments; block partials during init)
+constexpr int kNumMomentsMax = 270;   // surrogate moments of the 3D coefficients (the 2D ones: 66)
 
 struct KernelShape {
     int ipt = 0;      // source points per thread

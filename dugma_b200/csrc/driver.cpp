@@ -12,6 +12,8 @@
 // minimisation is unconstrained over local coordinates (w, dt) at the current iterate:
 // damped Newton steps with the analytic gradient and Hessian of Q (from the monomial
 // exponents and the derivatives of R <- exp([w]x) R at w = 0), with backtracking.
+// Each iteration's update_sig and the next iteration's compi run as one captured CUDA graph
+// (dugma_em_step): the sigma stays on the device between them.
 // Direct mode (DUGMA_DRIVE_DIRECT): maximise E(R, t) at the current sig with BFGS on the
 // left-perturbation coordinates using the fused adjoint's gradient, then update sig; every
 // evaluation replays one captured CUDA graph (pose prologue, adjoint, reduction).
@@ -442,6 +444,14 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
     void* graph = nullptr;
     if (rc == DUGMA_OK && mode == DUGMA_DRIVE_DIRECT && dugma_graph_create(Ptr, DUGMA_MODEL_REF, &graph) != DUGMA_OK)
         graph = nullptr;
+    // reference mode: update_sig at the new pose and the next iteration's compi as one captured
+    // graph per iteration (the same kernels and values as the two plugin calls); without it
+    // (capture refused) the two calls run eagerly
+    void* emg = nullptr;
+    if (rc == DUGMA_OK && mode == DUGMA_DRIVE_REFERENCE && dugma_em_graph_create(Ptr, &emg) != DUGMA_OK)
+        emg = nullptr;
+    double A[640];
+    bool have_A = false;   // A holds compi at the current (R, t, sig)
     auto eval = [&](const double* Rx, const double* tx, double* Ex, double* gx) {
         return graph ? dugma_graph_eval(graph, Rx, tx, sig, Ex, gx)
                      : dugma_energy_grad(Ptr, Rx, tx, sig, DUGMA_MODEL_REF, Ex, gx, nullptr);
@@ -460,8 +470,8 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
     while (rc == DUGMA_OK && iter <= max_iter && (con_angle || std::fabs(tdiff2()) > acc_trans) && sig > acc_sig) {
         double dRm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, dt[3] = {0, 0, 0};
         if (mode == DUGMA_DRIVE_REFERENCE) {
-            double A[640];
-            rc = dugma_compi(Ptr, R, t, &Nd, &Md, &Dd, &sig, A);
+            if (!have_A) rc = dugma_compi(Ptr, R, t, &Nd, &Md, &Dd, &sig, A);
+            have_A = false;
             if (rc != DUGMA_OK) break;
             SurrogatePose F{{D, D == 3 ? 637 : 45, D == 3 ? 12 : 4, A,
                              D == 3 ? &dugma::kMonoExp3D[0][0] : &dugma::kMonoExp2D[0][0]},
@@ -592,7 +602,15 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
             angle[0] = std::asin(std::max(-1.0, std::min(1.0, R[1]))) * 180.0 / M_PI;   // asind(R(2))
             con_angle = std::fabs(angle0[0] - angle[0]) > acc_rot;
         }
-        rc = dugma_update_sig(Ptr, R, t, &Nd, &Md, &Dd, &sigf);
+        // the host-side part of the loop test for the next iteration: when it holds, that
+        // iteration's compi runs in the same graph as this update_sig
+        const bool next = iter + 1 <= max_iter && (con_angle || std::fabs(tdiff2()) > acc_trans);
+        if (emg && next) {
+            rc = dugma_em_step(emg, R, t, &sigf, A);
+            have_A = rc == DUGMA_OK;
+        } else {
+            rc = dugma_update_sig(Ptr, R, t, &Nd, &Md, &Dd, &sigf);
+        }
         sig = sigf;
         ++iter;
     }
@@ -601,6 +619,7 @@ extern "C" int dugma_register(const double* X, const double* X_C, const double* 
         dugma_energy_grad(Ptr, R, t, sig, DUGMA_MODEL_REF, &E, gtmp, nullptr);
     }
     if (graph) dugma_graph_destroy(graph);
+    if (emg) dugma_em_graph_destroy(emg);
     dugma_fr_m(Ptr);
     if (rc != DUGMA_OK) return rc;
     if (exitflag < 0) {   // DUGMA.m:116-118: an unsolvable surrogate returns the identity

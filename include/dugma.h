@@ -177,6 +177,19 @@ int dugma_graph_create(float* Ptr[6], int model, void** graph);
 int dugma_graph_eval(void* graph, const double* R, const double* t, double sig, double* E, double* g);
 int dugma_graph_destroy(void* graph);
 
+/* One iteration of the reference's registration loop on the device as a captured CUDA graph:
+ * update_sig at (R, t) (update_sig.cu:319-394, called at DUGMA.m:105), then compi at (R, t) and
+ * that sigma (compi.cu:511-628, called at DUGMA.m:60 of the next iteration), with the sigma kept
+ * on the device between them and one copy of sigma and the surrogate moments back per step.
+ * sig[0] and coefficient[640] are what dugma_update_sig and then dugma_compi would return, bit
+ * for bit.  Replaces the host round trip between the two reference calls; no counterpart in the
+ * reference.  dugma_em_graph_create runs one step eagerly (at the identity pose) to size the
+ * scratch, then captures; the graph reads the context's state, so it must be destroyed before
+ * dugma_fr_m of that context. */
+int dugma_em_graph_create(float* Ptr[6], void** graph);
+int dugma_em_step(void* graph, const double* R, const double* t, float sig[1], double coefficient[640]);
+int dugma_em_graph_destroy(void* graph);
+
 /* ---------------- batched problems ---------------- */
 
 /* Many independent registration problems of uneven sizes in one persistent launch.

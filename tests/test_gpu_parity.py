@@ -615,3 +615,24 @@ def test_reference_cpp_entry_points_match_python_mirror(tmp_path):
         api.fr_m(h)
     assert res[1] == sig
     assert np.array_equal(res[2:2 + 637], A)
+
+
+@pytest.mark.parametrize("D", [3, 2])
+def test_em_graph_step_equals_update_sig_then_compi(D):
+    """One captured EM step (update_sig at a pose, then compi at that pose and sigma, sigma kept
+    on the device) gives what the two plugin calls give, bit for bit, over several poses (the
+    registration loop uses it; tests/test_kinect.py holds that loop to the recorded poses)."""
+    X, XC, Y, YC = _problem_small(D, 700, 650, seed=21)
+    _, h = api.init(X, XC, Y, YC)
+    g = api.EMGraph(h)
+    try:
+        for seed in range(4):
+            R, t = _pose(D, seed=seed, scale=0.15)
+            sig_g, A_g = g(R, t)
+            sig = api.update_sig(h, R, t)
+            A = api.compi(h, R, t, sig=sig)
+            assert sig_g == sig
+            assert np.array_equal(A_g, A)
+    finally:
+        g.close()
+        api.fr_m(h)
