@@ -312,15 +312,18 @@ def run_reference_gpu(args, rank):
         print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref was not built"}))
         return
     rows = []
-    for n in (1024, 4096):
+    # compi at 65536 points would take the reference ~30 s a call; 16384 is its largest size here
+    for n, names in ((1024, ("update_sig", "compi")), (4096, ("update_sig", "compi")), (16384, ("update_sig", "compi")),
+                     (65536, ("update_sig",))):
         P = synth.workload0(n=n)
         R, t = P.R_G, P.t_G
         ptr = ref_plugins.init(P.X, P.X_C, P.Y, P.Y_C)
         _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
         res = {"N": n, "M": n}
-        for name, fn_ref, fn_ours in (
-                ("update_sig", lambda: ref_plugins.update_sig(ptr, R, t, n, n, 3), lambda: api.update_sig(h, R, t)),
-                ("compi", lambda: ref_plugins.compi(ptr, R, t, n, n, 3, 0.01), lambda: api.compi(h, R, t, sig=0.01))):
+        calls = {"update_sig": (lambda: ref_plugins.update_sig(ptr, R, t, n, n, 3), lambda: api.update_sig(h, R, t)),
+                 "compi": (lambda: ref_plugins.compi(ptr, R, t, n, n, 3, 0.01), lambda: api.compi(h, R, t, sig=0.01))}
+        for name in names:
+            fn_ref, fn_ours = calls[name]
             for tag, fn in (("reference", fn_ref), ("ours", fn_ours)):
                 fn()
                 torch.cuda.synchronize()
@@ -332,6 +335,7 @@ def run_reference_gpu(args, rank):
                 el = time.perf_counter() - t0
                 res[f"{name}_{tag}_ms"] = 1e3 * el / reps
                 res[f"{name}_{tag}_pair_terms_per_s"] = n * n * reps / el
+            res[f"{name}_speedup"] = res[f"{name}_reference_ms"] / res[f"{name}_ours_ms"]
         rows.append(res)
         api.fr_m(h)
     print(json.dumps({"impl": "reference-gpu", "unit": "pair-terms/s (one pair at one pose per term)",
