@@ -274,6 +274,249 @@ __global__ void __launch_bounds__(NT, MINB) coef_pass_kernel(PairArgs a)
     run_pairs<Body, NT, TJ, 4>(a, body);
 }
 
+// ---------------------------------------------------------------------------
+// Single pass over the pairs for both sides.  A work item is (group of SB source blocks,
+// chunk of target tiles); for each source block of its group the block streams the chunk's
+// pair records through the bulk-copy ring and, per tile:
+//   phase 1: every pair's p = 2^t1 + 2^t2 (target log weight folded in) once, accumulated into
+//            the sources' H2 = sum_j p g_j in registers, and written to a shared tile sP;
+//   phase 2: warp w sums its quarter of the sources against one target per lane,
+//            T_j = sum_i fw_i p_ij with fw_i = (w_i / 2^Lmax_x) f(x_i), and the warps' partial
+//            sums are added in fixed order into the group's H1 rows in FP64.
+// H2 is written per (chunk, source), H1 per (group, target), and the moments kernels sum those
+// copies in fixed order: the same moments as the two passes, each pair's exponentials computed
+// once, and no atomics.
+// ---------------------------------------------------------------------------
+struct FusedCoefArgs {
+    const Rec128* xrec;    // sources: x, lw, k B (Horner), monomials f(x)
+    const Rec256* yrec;    // target pair records
+    const float* wx;       // |Sigma_x|^-1/2
+    const double* pose;
+    double Lmax_x, Lmax_y;
+    int N, M, n_ib, SB, n_grp, n_jc, jc_tiles, total_tiles;
+    double* h2_part;       // [n_jc][N][16]
+    double* h1_part;       // [n_grp][M][16]
+    int* counter;
+    int* err;
+};
+
+template <int D>
+struct FusedCoefShape {
+    static constexpr int IPT = 2, NT = 128, TJ = 16, STAGES = 4;
+    static constexpr int BI = IPT * NT, NW = NT / 32, TT = 2 * TJ;
+    static constexpr int NF = Feat<D>::N;          // 10 in 3D, 6 in 2D
+    static constexpr int NFH = NF / 2;             // monomials per half-warp in phase 2
+    static constexpr int NFHP = (NFH + 3) / 4 * 4; // a half's floats, padded to whole float4s
+    static constexpr int SPS = TT + 2;   // sP row stride in floats: even (float2 stores), rows skewed across banks
+    static constexpr size_t kOffBars = (size_t)STAGES * TJ * sizeof(Rec256);
+    static constexpr size_t kOffP = kOffBars + 128;
+    static constexpr size_t kOffF = kOffP + sizeof(float) * BI * SPS;
+    static constexpr size_t kOffT = kOffF + sizeof(float) * BI * 2 * NFHP;
+    static constexpr size_t kBytes = kOffT + sizeof(float) * NW * TT * (NF + 1) + 16;
+};
+
+template <int D>
+__global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
+{
+    using S = FusedCoefShape<D>;
+    constexpr int IPT = S::IPT, NT = S::NT, TJ = S::TJ, STAGES = S::STAGES, BI = S::BI, NW = S::NW, TT = S::TT;
+    constexpr int NF = S::NF, NFH = S::NFH, NFHP = S::NFHP, SPS = S::SPS, NS = Sym<D>::N;
+    static_assert(TT == 32, "phase 2 maps a lane of each half-warp to two targets of a tile");
+    static_assert(BI % NW == 0 && NF % 2 == 0, "sources split evenly over the warps, monomials over the halves");
+    constexpr uint32_t kTileBytes = TJ * sizeof(Rec256);
+    extern __shared__ __align__(128) unsigned char smem[];
+    Rec256(*ybuf)[TJ] = reinterpret_cast<Rec256(*)[TJ]>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::kOffBars);
+    int* s_item = reinterpret_cast<int*>(smem + S::kOffBars + 64);
+    float(*sP)[SPS] = reinterpret_cast<float(*)[SPS]>(smem + S::kOffP);
+    // fw rows: [first NFH monomials | pad | last NFH | pad], each half a whole number of float4s
+    float(*sF)[2 * NFHP] = reinterpret_cast<float(*)[2 * NFHP]>(smem + S::kOffF);
+    float(*sT)[TT][NF + 1] = reinterpret_cast<float(*)[TT][NF + 1]>(smem + S::kOffT);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        for (int st = 0; st < STAGES; ++st) mbar_init(&bars[st], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const double sgm = 1.0 / a.pose[kPoseSig];
+    const double Gs = pow(sgm, (double)D);
+    const double G2 = Gs * exp2(a.Lmax_y);               // H2_i = w_i G2 sum_j p g_j
+    const double G1 = Gs * exp2(a.Lmax_x + a.Lmax_y);    // H1_j = G1 sum_i fw_i p_ij
+    const double inv_wmax = exp2(-a.Lmax_x);
+    const Rec256* yg = a.yrec;
+    const int n_items = a.n_grp * a.n_jc;
+    uint32_t tcount = 0;
+    for (;;) {
+        if (tid == 0) *s_item = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int item = *s_item;
+        if (item >= n_items) break;
+        const int grp = item % a.n_grp, jc = item / a.n_grp;
+        const int tile0 = jc * a.jc_tiles;
+        const int ntiles = min(a.jc_tiles, a.total_tiles - tile0);
+        for (int sb = 0; sb < a.SB; ++sb) {
+            const int ib = grp * a.SB + sb;
+            if (ib >= a.n_ib) break;
+            if (tid == 0)
+                for (int k = 0; k < STAGES && k < ntiles; ++k) {
+                    const int st = (tcount + k) % STAGES;
+                    mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                    bulk_g2s(&ybuf[st][0], yg + (size_t)(tile0 + k) * TJ, kTileBytes, &bars[st]);
+                }
+            // the block's sources: position, k B (Horner), and fw = (w / 2^Lmax_x) f(x) for phase 2
+            float2 PH[IPT][3], Mx[IPT][6], h[IPT][NF];
+            double H[IPT][NF];
+            int row[IPT];
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) {
+                const int il = ii * NT + tid, i = ib * BI + il;
+                const bool ok = i < a.N;
+                row[ii] = ok ? i : -1;
+                const Rec128 r = a.xrec[ok ? i : 0];
+                const float hv[3] = {r.v0.x, r.v0.y, r.v0.z};
+                const float mv[6] = {r.v2.x, r.v2.y, r.v2.z, r.v2.w, r.v3.x, r.v3.y};
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const float v = ok && q < D ? hv[q] : 0.f;
+                    PH[ii][q] = make_float2(v, v);
+                }
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const float v = ok && q < NS ? mv[q] : 0.f;
+                    Mx[ii][q] = make_float2(v, v);
+                }
+                const double ws = ok ? (double)a.wx[i] * inv_wmax : 0.0;
+#pragma unroll
+                for (int q = 0; q < 2 * NFHP; ++q) {
+                    const int qf = (q < NFHP ? q : q - NFHP) + (q < NFHP ? 0 : NFH);
+                    const bool used = (q < NFHP ? q : q - NFHP) < NFH;
+                    sF[il][q] = used ? __double2float_rn(ws * (double)r.g[qf]) : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < NF; ++q) {
+                    h[ii][q] = make_float2(0.f, 0.f);
+                    H[ii][q] = 0.0;
+                }
+            }
+            constexpr int NE = (TT * NF + NT - 1) / NT;   // H1 entries of a tile per thread
+            for (int k = 0; k < ntiles; ++k) {
+                const uint32_t u = tcount + k;
+                const int st = u % STAGES;
+                const int jt = (tile0 + k) * TT;
+                // this thread's H1 entries of the tile as the previous source block left them (the
+                // same thread wrote them), loaded now so that the latency hides behind both phases
+                double prev[NE];
+#pragma unroll
+                for (int n = 0; n < NE; ++n) {
+                    const int e = tid + n * NT, l2 = e / NF, q = e - l2 * NF;
+                    prev[n] = (sb > 0 && e < TT * NF && jt + l2 < a.M)
+                                  ? a.h1_part[((size_t)grp * a.M + jt + l2) * 16 + q]
+                                  : 0.0;
+                }
+                const bool ok = mbar_wait_bounded(&bars[st], (u / STAGES) & 1u, a.err);
+                const Rec256* yb = ybuf[st];
+                // phase 1
+#pragma unroll 4
+                for (int jj = 0; jj < TJ; ++jj) {
+                    const Rec256& r = yb[jj];
+                    float2 nh[3], nl[3], ms[6], g[NF];
+#pragma unroll
+                    for (int q = 0; q < D; ++q) { nh[q] = fld256(r, q); nl[q] = fld256(r, 4 + q); }
+                    const float2 lv = fld256(r, 3);
+#pragma unroll
+                    for (int q = 0; q < NS; ++q) ms[q] = fld256(r, 8 + q);
+#pragma unroll
+                    for (int q = 0; q < NF; ++q) g[q] = fld256(r, 16 + q);
+#pragma unroll
+                    for (int ii = 0; ii < IPT; ++ii) {
+                        float2 d[3];
+#pragma unroll
+                        for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), nl[q]);
+                        const float2 t1 = qform2<D>(Mx[ii], d, lv);
+                        const float2 t2 = qform2<D>(ms, d, lv);
+                        const float2 p = fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+#pragma unroll
+                        for (int q = 0; q < NF; ++q) h[ii][q] = ffma2(p, g[q], h[ii][q]);
+                        *reinterpret_cast<float2*>(&sP[ii * NT + tid][2 * jj]) = p;
+                    }
+                }
+#pragma unroll
+                for (int ii = 0; ii < IPT; ++ii)
+#pragma unroll
+                    for (int q = 0; q < NF; ++q) {
+                        H[ii][q] += (double)h[ii][q].x + (double)h[ii][q].y;
+                        h[ii][q] = make_float2(0.f, 0.f);
+                    }
+                if (__syncthreads_or(!ok)) {
+                    // a tile never arrived: drain the copies still in flight (bounded), then stop
+                    if (tid == 0)
+                        for (int q = k; q < ntiles && q < k + STAGES; ++q) {
+                            const uint32_t uq = tcount + q;
+                            mbar_wait_bounded(&bars[uq % STAGES], (uq / STAGES) & 1u, nullptr);
+                        }
+                    return;
+                }
+                if (tid == 0 && k + STAGES < ntiles) {
+                    mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                    bulk_g2s(&ybuf[st][0], yg + (size_t)(tile0 + k + STAGES) * TJ, kTileBytes, &bars[st]);
+                }
+                // phase 2: warp `warp` sums its quarter of the sources; lane (fh, tl) owns targets 2 tl,
+                // 2 tl + 1 of the tile (one f32x2) and monomials [fh NFH, fh NFH + NFH), so a p pair is
+                // read once for both halves and each half's monomials are one broadcast row
+                {
+                    const int fh = lane >> 4, tl = lane & 15;
+                    float2 acc[NFH];
+#pragma unroll
+                    for (int q = 0; q < NFH; ++q) acc[q] = make_float2(0.f, 0.f);
+                    const int i0 = warp * (BI / NW);
+#pragma unroll 4
+                    for (int i = i0; i < i0 + BI / NW; ++i) {
+                        const float2 pv = *reinterpret_cast<const float2*>(&sP[i][2 * tl]);
+                        const float4* f4 = reinterpret_cast<const float4*>(&sF[i][fh * NFHP]);
+                        float f[NFHP];
+#pragma unroll
+                        for (int v = 0; v < NFHP / 4; ++v) {
+                            const float4 fv = f4[v];
+                            f[4 * v] = fv.x;
+                            f[4 * v + 1] = fv.y;
+                            f[4 * v + 2] = fv.z;
+                            f[4 * v + 3] = fv.w;
+                        }
+#pragma unroll
+                        for (int q = 0; q < NFH; ++q) acc[q] = ffma2(make_float2(f[q], f[q]), pv, acc[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < NFH; ++q) {
+                        sT[warp][2 * tl][fh * NFH + q] = acc[q].x;
+                        sT[warp][2 * tl + 1][fh * NFH + q] = acc[q].y;
+                    }
+                }
+                __syncthreads();
+                // the warps' partials in fixed order, into the group's H1 rows (FP64)
+#pragma unroll
+                for (int n = 0; n < NE; ++n) {
+                    const int e = tid + n * NT, l2 = e / NF, q = e - l2 * NF;
+                    if (e >= TT * NF || jt + l2 >= a.M) continue;
+                    float sum = sT[0][l2][q];
+#pragma unroll
+                    for (int w2 = 1; w2 < NW; ++w2) sum += sT[w2][l2][q];
+                    a.h1_part[((size_t)grp * a.M + jt + l2) * 16 + q] = prev[n] + G1 * (double)sum;
+                }
+            }
+            tcount += ntiles;
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) {
+                if (row[ii] < 0) continue;
+                const double w = (double)a.wx[row[ii]] * G2;
+                double* o = a.h2_part + ((size_t)jc * a.N + row[ii]) * 16;
+#pragma unroll
+                for (int q = 0; q < NF; ++q) o[q] = w * H[ii][q];
+            }
+        }
+    }
+}
+
 __constant__ signed char c_moment3[kNumMoments3D][4];
 __constant__ signed char c_moment2[kNumMoments2D][4];
 // per side, the indices of its moments in the table (kind 2: side 0, kind 1: side 1)
@@ -433,6 +676,96 @@ static int upload_moment_tables(int dev)
     return DUGMA_OK;
 }
 
+// the fused kernel's dynamic shared memory limit, once per device; its resident blocks per SM
+template <int D>
+static int fused_coef_setup(int dev, int* per_sm)
+{
+    static std::mutex mu;
+    static std::vector<int> blocks;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < (int)blocks.size() && blocks[dev] > 0) {
+        *per_sm = blocks[dev];
+        return DUGMA_OK;
+    }
+    DUGMA_CK(cudaFuncSetAttribute(coef_fused_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)FusedCoefShape<D>::kBytes));
+    int nb = 0;
+    DUGMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, coef_fused_kernel<D>, FusedCoefShape<D>::NT,
+                                                           FusedCoefShape<D>::kBytes));
+    if (dev >= (int)blocks.size()) blocks.resize(dev + 1, 0);
+    blocks[dev] = std::max(nb, 1);
+    *per_sm = blocks[dev];
+    return DUGMA_OK;
+}
+
+// Every source row against every target row in one pass (coef_fused_kernel), then the moments
+// of both sides from the H2 copies (one per target chunk) and the H1 copies (one per source group).
+template <int D>
+static int coef_fused_launch(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+{
+    using S = FusedCoefShape<D>;
+    constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
+    int per_sm = 1;
+    DUGMA_RET(fused_coef_setup<D>(c.dev, &per_sm));
+    const int resident = c.num_sms * per_sm;
+    const int n_ib = (c.N + S::BI - 1) / S::BI;
+    const int total_tiles = c.M_pad / 2 / S::TJ;
+    // at most 24 copies of either side's rows; items for about four waves of resident blocks
+    int n_grp = std::min(n_ib, 24);
+    const int SB = (n_ib + n_grp - 1) / n_grp;
+    n_grp = (n_ib + SB - 1) / SB;
+    int n_jc = std::max(1, std::min(std::min(total_tiles, 24), (4 * resident + n_grp - 1) / n_grp));
+    const int jc_tiles = (total_tiles + n_jc - 1) / n_jc;
+    n_jc = (total_tiles + jc_tiles - 1) / jc_tiles;
+    const size_t h2_doubles = (size_t)n_jc * c.N * 16, h1_doubles = (size_t)n_grp * c.M * 16;
+    DUGMA_RET(c.ensure_scratch(sizeof(double) * (h2_doubles + h1_doubles)));
+    FusedCoefArgs a{};
+    a.xrec = c.xrec128;
+    a.yrec = static_cast<const Rec256*>(c.yrec256);
+    a.wx = c.wx;
+    a.pose = pose_dev;
+    a.Lmax_x = c.Lmax_x;
+    a.Lmax_y = c.Lmax_y;
+    a.N = c.N;
+    a.M = c.M;
+    a.n_ib = n_ib;
+    a.SB = SB;
+    a.n_grp = n_grp;
+    a.n_jc = n_jc;
+    a.jc_tiles = jc_tiles;
+    a.total_tiles = total_tiles;
+    a.h2_part = c.scratch;
+    a.h1_part = c.scratch + h2_doubles;
+    a.counter = c.counter;
+    a.err = c.err;
+    DUGMA_CK(cudaMemsetAsync(c.counter, 0, sizeof(int), s));
+    cudaEvent_t ev1 = nullptr;
+    if (c.timing) {
+        if (c.tused == c.tevents.size()) {
+            cudaEvent_t e0, e1;
+            DUGMA_CK(cudaEventCreate(&e0));
+            DUGMA_CK(cudaEventCreate(&e1));
+            c.tevents.push_back({e0, e1});
+        }
+        DUGMA_CK(cudaEventRecord(c.tevents[c.tused].first, s));
+        ev1 = c.tevents[c.tused].second;
+        ++c.tused;
+    }
+    const int grid = std::min(resident, n_grp * n_jc);
+    coef_fused_kernel<D><<<grid, S::NT, S::kBytes, s>>>(a);
+    DUGMA_CK(cudaGetLastError());
+    if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
+    const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
+    const int nb0 = std::min(nblk, c.N), nb1 = std::min(nblk, c.M);
+    moments_kernel<D><<<nb0, kMomThreads, 0, s>>>(a.h2_part, n_jc, c.N, 0, pose_dev, c.x, c.xinv, c.mom_part);
+    moments_kernel<D><<<nb1, kMomThreads, 0, s>>>(a.h1_part, n_grp, c.M, 1, pose_dev, c.y, c.yinv,
+                                                  c.mom_part + (size_t)nblk * NM);
+    moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(c.mom_part, nb0, c.mom_part + (size_t)nblk * NM, nb1, NM,
+                                                       moments_dev);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
 template <int D>
 static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0,
                      int j1)
@@ -444,6 +777,8 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx,
         c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256));
     DUGMA_CK(cudaGetLastError());
+    // all rows on both sides: one pass over the pairs; row ranges (sharding): one pass per side
+    if (i0 == 0 && i1 == c.N && j0 == 0 && j1 == c.M && c.fused_coef) return coef_fused_launch<D>(c, pose_dev, moments_dev, s);
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
     // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
