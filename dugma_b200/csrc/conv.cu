@@ -442,6 +442,12 @@ struct PackedConvBody {
     float2 e[IPT];                               // energy, tile level
     float2 U[IPT][GRAD ? D : 1], UU[IPT][GRAD ? NS : 1], A[IPT][GRAD ? NS : 1];   // item level
     double E64[IPT];
+    // the largest fast-path term N~ of each source in this item, redone in FP64 at the item's end
+    // (a sum carried by a few far pairs has exponents of 40-80, where FP32 holds the exponent to
+    // only ~|exponent| x 6e-8): key = float bits of N~ (>= 0, so they order as integers) with the
+    // low 10 bits replaced by the pair's place in the item (an item spans at most 512 records)
+    uint32_t key[IPT];
+    int j0;   // the item's first record
     // set when a pair of the current tile fails the fast path's test; the tile is then redone
     // from the item-level sums saved at its start (a per-thread copy in shared memory)
     bool bad;
@@ -498,6 +504,9 @@ struct PackedConvBody {
                 for (int q = 0; q < NS; ++q) { UU[ii][q] = make_float2(0.f, 0.f); A[ii][q] = make_float2(0.f, 0.f); }
             }
         }
+#pragma unroll
+        for (int ii = 0; ii < IPT; ++ii) key[ii] = 0u;
+        j0 = 0x7fffffff;
         bad = false;
         save();
     }
@@ -641,6 +650,11 @@ struct PackedConvBody {
                 rd = fmul2(rs, rs);
                 const float2 arg = ffma2(m, fmul2(rd, KL), lv);
                 Nt = fmul2(rs, make_float2(ex2(arg.x), ex2(arg.y)));
+                if (!EXACT) {   // (a redone tile's fast pairs have these same values)
+                    const uint32_t jl = 2u * ((uint32_t)jrec & 511u);
+                    key[ii] = max(key[ii], (__float_as_uint(fmaxf(Nt.x, 0.f)) & 0xfffffc00u) | jl);
+                    key[ii] = max(key[ii], (__float_as_uint(fmaxf(Nt.y, 0.f)) & 0xfffffc00u) | (jl | 1u));
+                }
             } else {
                 float dv[2][3], sv[2][6], av[2][6], hv[2][3], nt[2], rdv[2];
                 for (int hh = 0; hh < 2; ++hh) {
@@ -677,6 +691,7 @@ struct PackedConvBody {
     }
     __device__ void fold_tile(const YRec2* tile, int jbase, int ntile)
     {
+        j0 = min(j0, jbase);
         if (bad) {   // rare: redo this tile with the exact per-pair rules
             restore();
 #pragma unroll
@@ -690,6 +705,92 @@ struct PackedConvBody {
             e[ii] = make_float2(0.f, 0.f);
         }
         save();
+    }
+    // Source ii's largest term of this item: its fast-path contribution re-evaluated in FP32 by the
+    // same operations, one half at a time (f32x2 arithmetic rounds each half as the scalar
+    // operation does, so the values are the ones accumulated), replaced by the exact FP64 pair.
+    __device__ void top_pair_in_fp64(const PairArgs& a, int ii, const float* xs, const float* sxs, double* ur,
+                                     double* uur, double* ar)
+    {
+        const int loc = (int)(key[ii] & 1023u), h = loc & 1;
+        const int jrec = j0 + (((loc >> 1) - (j0 & 511)) & 511);
+        const int j = 2 * jrec + h;
+        const YRec2& r = static_cast<const YRec2*>(a.yrec)[j >> 1];
+        float ny[3] = {0, 0, 0}, nl[3] = {0, 0, 0}, cy[6] = {0, 0, 0, 0, 0, 0}, oy[3] = {0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            const float2 u0 = fld2(r, q), u1 = fld2(r, 4 + q);
+            ny[q] = h ? u0.y : u0.x;
+            nl[q] = h ? u1.y : u1.x;
+        }
+        const float2 l2 = fld2(r, 3);
+        const float lv = h ? l2.y : l2.x;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            const float2 u = fld2(r, 7 + k);
+            cy[k] = h ? u.y : u.x;
+        }
+#pragma unroll
+        for (int k = 0; k < NO; ++k) {
+            const float2 u = fld2(r, 7 + NS + k);
+            oy[k] = h ? u.y : u.x;
+        }
+        float d[3], sm[6], o[3], adj[6], hv[3], det;
+#pragma unroll
+        for (int q = 0; q < D; ++q) d[q] = __fadd_rn(__fadd_rn(xs[q], ny[q]), nl[q]);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) sm[k] = __fadd_rn(sxs[k], cy[k]);
+#pragma unroll
+        for (int k = 0; k < NO; ++k) o[k] = __fadd_rn(-sxs[D + k], oy[k]);
+        if (D == 3) {
+            adj[0] = __fmaf_rn(o[2], sm[5], __fmul_rn(sm[1], sm[2]));
+            adj[1] = __fmaf_rn(o[1], sm[4], __fmul_rn(sm[0], sm[2]));
+            adj[2] = __fmaf_rn(o[0], sm[3], __fmul_rn(sm[0], sm[1]));
+            adj[3] = __fmaf_rn(sm[4], sm[5], __fmul_rn(o[0], sm[2]));
+            adj[4] = __fmaf_rn(sm[3], sm[5], __fmul_rn(o[1], sm[1]));
+            adj[5] = __fmaf_rn(sm[3], sm[4], __fmul_rn(o[2], sm[0]));
+            det = __fmaf_rn(sm[4], adj[4], __fmaf_rn(sm[3], adj[3], __fmul_rn(sm[0], adj[0])));
+            hv[0] = __fmaf_rn(adj[4], d[2], __fmaf_rn(adj[3], d[1], __fmul_rn(adj[0], d[0])));
+            hv[1] = __fmaf_rn(adj[5], d[2], __fmaf_rn(adj[1], d[1], __fmul_rn(adj[3], d[0])));
+            hv[2] = __fmaf_rn(adj[2], d[2], __fmaf_rn(adj[5], d[1], __fmul_rn(adj[4], d[0])));
+        } else {
+            adj[0] = sm[1];
+            adj[1] = sm[0];
+            adj[2] = o[0];
+            det = __fmaf_rn(o[0], sm[2], __fmul_rn(sm[0], sm[1]));
+            hv[0] = __fmaf_rn(adj[2], d[1], __fmul_rn(adj[0], d[0]));
+            hv[1] = __fmaf_rn(adj[1], d[1], __fmul_rn(adj[2], d[0]));
+        }
+        float m = __fmul_rn(d[0], hv[0]);
+#pragma unroll
+        for (int q = 1; q < D; ++q) m = __fmaf_rn(d[q], hv[q], m);
+        float prod = __fmul_rn(sm[0], sm[1]);
+        if (D == 3) prod = __fmul_rn(prod, sm[2]);
+        if (!(__fmul_rn(det, 1e6f) >= prod) || !(det > 0.f)) return;   // that pair took the exact path
+        const float rs = rsqrtf(det), rd = __fmul_rn(rs, rs);
+        const float Nt = __fmul_rn(rs, ex2(__fmaf_rn(m, __fmul_rn(rd, kl), lv)));
+        // the exact pair (FP64 throughout, from the stored inputs)
+        const float4 v0 = make_float4(-ny[0], -ny[1], D == 3 ? -ny[2] : 0.f, 1.f);
+        const float4 v1 = make_float4(-nl[0], -nl[1], D == 3 ? -nl[2] : 0.f, 0.f);
+        float adj64[6] = {0, 0, 0, 0, 0, 0}, h64[3] = {0, 0, 0}, rd64 = 0.f, Nt64 = 0.f;
+        if (!conv_pair_f64<D>(xs, sxs, v0, v1, ycov + (size_t)j * NS, pose, (double)kl, adj64, h64, &rd64, &Nt64))
+            Nt64 = rd64 = 0.f;
+        E64[ii] += (double)Nt64 - (double)Nt;
+        if (!GRAD) return;
+        const float nr = __fmul_rn(Nt, rd), nr2 = __fmul_rn(nr, rd);
+        const double nx = (double)Nt64 * rd64, nx2 = nx * rd64;
+        float w[3];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            w[q] = __fmul_rn(nr2, hv[q]);
+            ur[q] += nx * h64[q] - (double)nr * hv[q];
+        }
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            const int ka = Sym<D>::a(k), kb = Sym<D>::b(k);
+            uur[k] += nx2 * h64[ka] * h64[kb] - (double)w[ka] * hv[kb];
+            ar[k] += nx * adj64[k] - (double)nr * adj[k];
+        }
     }
     __device__ void finish(const PairArgs& a, int jc, double (&acc)[NV])
     {
@@ -711,6 +812,7 @@ struct PackedConvBody {
             for (int q = 0; q < D; ++q) xs[q] = X[ii][q].x;
 #pragma unroll
             for (int k = 0; k < NS; ++k) sxs[k] = SX[ii][k].x;
+            if (key[ii] & 0xfffffc00u) top_pair_in_fp64(a, ii, xs, sxs, ur, uur, ar);
             conv_contract<D, NV, GRAD>(a, jc, row[ii], xs, sxs, E64[ii], ur, uur, ar, lam, c0, t, acc);
         }
     }
@@ -745,8 +847,8 @@ static const std::vector<ConvVariant>& conv_variants(bool grad)
         {{1, 64, 64}, conv_kernel<ConvBody<D, 1, true>, 64, 64>},
     };
     static const std::vector<ConvVariant> e = {
-        {{1, 128, 32, 2}, conv_kernel<PackedConvBody<D, 1, false, 128>, 128, 32, 4>},
-        {{2, 128, 32, 2}, conv_kernel<PackedConvBody<D, 2, false, 128>, 128, 32, 3>},
+        {{1, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 1, false, 128>, 128, 32, 4>},
+        {{2, 128, 32, 2, 512}, conv_kernel<PackedConvBody<D, 2, false, 128>, 128, 32, 3>},
         {{2, 128, 64}, conv_kernel<ConvBody<D, 2, false>, 128, 64>},
         {{1, 128, 64}, conv_kernel<ConvBody<D, 1, false>, 128, 64>},
         {{4, 128, 64}, conv_kernel<ConvBody<D, 4, false>, 128, 64>},
