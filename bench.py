@@ -62,6 +62,9 @@ FP32_INSTR_ADJOINT_2D = 26
 # exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
 FP32_INSTR_CONV_ADJOINT = 68
 FP32_INSTR_ENERGY = 26      # d 6, two Horner quadratic forms 9 + 9, accumulation 2
+# compi in one pass: d 6, two Horner forms 9 + 9, p = e1 + e2 1, source-side H2 += p g 10,
+# target-side T += fw p 10
+FP32_INSTR_COMPI = 45
 SFU_PER_PAIR = 2            # two ex2
 
 
@@ -88,6 +91,13 @@ def parse():
                     help="multistart poses evaluated per step and GPU (the depth workload uses 64)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the compact results of the other configured workloads (the `configs` key)")
+    ap.add_argument("--plugin", default="", choices=["", "compi", "update_sig", "compi_range", "nn", "knn_covariance"],
+                    help="profiling runs: only this call, --warmup + --steps times at the workload's first "
+                         "multistart pose (one JSON line with the wall time per call and the library's device "
+                         "time of its pair kernels): compi, update_sig, compi_range (the source-side coefficient "
+                         "pass alone, as row-range compi runs it), nn (--knn nearest neighbours), knn_covariance "
+                         "(the --knn neighbour covariance estimator on the source cloud)")
+    ap.add_argument("--knn", type=int, default=8, help="k for --plugin nn and knn_covariance")
     return ap.parse_args()
 
 
@@ -580,7 +590,7 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
     try:
         sig = api.update_sig(h, R, t)
         for name, fn, instr in (("update_sig", lambda: api.update_sig(h, R, t), None),
-                                ("compi", lambda: api.compi(h, R, t, sig=sig), 2 * 35)):
+                                ("compi", lambda: api.compi(h, R, t, sig=sig), FP32_INSTR_COMPI)):
             fn()
             torch.cuda.synchronize()
             L.dugma_timing(h.arr, 1, None, None)
@@ -600,7 +610,8 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
             if instr:
                 ent["roofline"] = {"bound": "fp32", "instr_per_pair": instr,
                                    "frac": instr * P.N * P.M / (kms.value / reps * 1e-3) / peak,
-                                   "note": "two coefficient passes of 35 FP32 lane-ops per pair each"}
+                                   "note": "one pass over the pairs: d 6, two Horner forms 18, p 1, source-side "
+                                           "sums 10, target-side sums 10 FP32 lane-ops per pair"}
             c = clk.summary()
             if c:
                 ent["clocks"] = c
@@ -676,9 +687,53 @@ def run_configs(L, peak, clock_dir):
     return out
 
 
+def run_plugin(args):
+    """--plugin: one call repeated on the workload, for profiling."""
+    import ctypes
+    import torch
+    from dugma_b200 import _lib, api
+    P = workload(args.workload, args.n)
+    R, t = eval_pose(P, 0)
+    _, h = api.init(P.X, P.X_C, P.Y, P.Y_C)
+    sig = api.update_sig(h, R, t)
+    calls = {"compi": lambda: api.compi(h, R, t, sig=sig),
+             "update_sig": lambda: api.update_sig(h, R, t),
+             "compi_range": lambda: api.compi_range(h, R, t, sig, 0, P.N, 0, 0),
+             "nn": lambda: api.nn(h, R, t, args.knn),
+             "knn_covariance": lambda: api.knn_covariance(P.X, k=args.knn)}
+    fn = calls[args.plugin]
+    for _ in range(max(1, args.warmup)):
+        fn()
+    torch.cuda.synchronize()
+    L = _lib.load()
+    L.dugma_timing(h.arr, 1, None, None)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    el = time.perf_counter() - t0
+    kms, kl = ctypes.c_double(0), ctypes.c_int(0)
+    L.dugma_timing(h.arr, 2, ctypes.byref(kms), ctypes.byref(kl))
+    L.dugma_timing(h.arr, 0, None, None)
+    api.fr_m(h)
+    line = {"plugin": args.plugin, "workload": P.name, "N": P.N, "M": P.M, "calls": args.steps,
+            "ms_per_call": 1e3 * el / max(1, args.steps)}
+    if kl.value:   # the context's pair kernels (knn_covariance runs on a context of its own)
+        line["pair_kernel_ms_per_call"] = kms.value / max(1, args.steps)
+        line["pair_kernel_pairs_per_s"] = P.N * P.M * args.steps / (kms.value * 1e-3)
+    if args.plugin in ("nn", "knn_covariance"):
+        line["k"] = args.knn
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args.gpus)
+    if args.plugin:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local % max(1, torch.cuda.device_count()))
+            run_plugin(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
