@@ -354,14 +354,16 @@ def run_reference_gpu(args, rank):
 
 def run_batch(args, rank, world):
     """Workload 3: 256 problems (N, M uniform in [500, 8000]) x 32 multistart rotations on a uniform
-    SO(3) grid, one persistent launch per evaluation (graph replay after the first); the problems
-    are split across ranks."""
+    SO(3) grid, one persistent launch per evaluation (graph replay after the first), tile shape
+    autotuned on these poses; the problems are split across ranks.  value: device time of each
+    evaluation (the library's CUDA events, max over ranks); e2e: the synchronous batch call with
+    host poses in and E, g out; accuracy: 4 sampled problem-poses against the FP64 oracle (rank 0);
+    cpu_baseline: the oracle on one whole problem-pose, all host cores."""
     import torch
     from dugma_b200 import api, synth
     probs = synth.workload3()
     mine = probs[rank::world]
-    rng = synth.rng_for(3, 1)
-    grid = synth.so3_grid(rng, 32)
+    grid = synth.so3_grid(synth.rng_for(3, 1), 32)
     Q = len(grid)
     sig = np.zeros((len(mine), Q))
     for k, P in enumerate(mine):
@@ -372,40 +374,81 @@ def run_batch(args, rank, world):
     t = np.array([[P.t_G for _ in grid] for P in mine])
     b = api.Batch([(P.X, P.X_C, P.Y, P.Y_C) for P in mine])
     pairs = Q * sum(P.N * P.M for P in mine)
+    tune = b.autotune(R, t, sig)
     for _ in range(max(3, args.warmup)):
-        b.energy_grad(R, t, sig)
+        E, g = b.energy_grad(R, t, sig)
     torch.cuda.synchronize()
     steps = max(3, min(args.steps, 20))
     import tempfile
+    b.timing(1)
     with Clocks(os.path.join(tempfile.gettempdir(), f"dugma_clocks_batch_rank{rank}.csv"),
                 torch.cuda.current_device()) as clk:
         t0 = time.perf_counter()
         for _ in range(steps):
             E, g = b.energy_grad(R, t, sig)
         el = time.perf_counter() - t0
+    dev_ms, n_ev = b.timing(2)
+    b.timing(0)
+    shape = list(b.get_shape())
     b.close()
-    tot = all_reduce([pairs], "sum") + all_reduce([el], "max")
-    if rank == 0:
-        value = float(tot[0]) * steps / float(tot[1])
-        n_pose = len(mine) * Q
-        line = {"metric": "energy+grad pair-terms/s", "value": value,
-                "unit": "pair-terms/s", "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup),
-                "ms_per_step": float(tot[1]) / steps * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batch256x32: 256 problems, N, M uniform in [500, 8000], 32 rotations of a "
-                                       "uniform SO(3) grid each, one evaluation per step (host poses in, E and g out)",
-                           "pair_terms_per_step": int(tot[0]),
-                           "timing": "wall clock around the synchronous batch call, max over ranks",
-                           "l2": "inputs of all problems (records) stay resident; no flush"},
-                # the batch call takes host poses and returns host results, so the timed steps are
-                # already end to end (rank 0's bytes)
-                "e2e": {"value": value, "unit": "pair-terms/s", "h2d_bytes_per_step": 8 * 13 * n_pose,
-                        "d2h_bytes_per_step": 8 * (1 + g.shape[-1]) * n_pose},
-                "gpu_launches": 3 * steps}
-        clocks = clk.summary()
-        if clocks:
-            line["clocks"] = clocks
-        print(json.dumps(line), flush=True)
+    tot = all_reduce([pairs], "sum") + all_reduce([el, dev_ms], "max")
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    orc.use_all_cores()
+    peak = ctypes_peak()
+    value = float(tot[0]) * steps / (float(tot[2]) * 1e-3)
+    e2e = float(tot[0]) * steps / float(tot[1])
+    n_pose = len(mine) * Q
+    rng = np.random.default_rng(7)
+    errs = []
+    for p, q in zip(rng.choice(len(mine), 4, replace=False), rng.integers(0, Q, 4)):
+        P = mine[p]
+        Eo, go, _ = orc.State(P.X, P.X_C, P.Y, P.Y_C).energy(R[p, q], t[p, q], sig[p, q])
+        errs.append((abs(E[p, q] - Eo) / abs(Eo), float(np.linalg.norm(g[p, q] - go) / np.linalg.norm(go))))
+    P0 = mine[0]
+    st0 = orc.State(P0.X, P0.X_C, P0.Y, P0.Y_C)
+    c0 = time.perf_counter()
+    st0.energy(R[0, 0], t[0, 0], sig[0, 0])
+    cpu_s = time.perf_counter() - c0
+    ms = float(tot[2]) / steps
+    line = {"metric": "energy+grad pair-terms/s", "value": value, "unit": "pair-terms/s", "n_gpus": world,
+            "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch256x32: 256 problems, N, M uniform in [500, 8000], 32 rotations of a "
+                                   "uniform SO(3) grid each, one evaluation per step",
+                       "pair_terms_per_step": int(tot[0]),
+                       "timing": "CUDA events around each evaluation on the batch stream, max over ranks",
+                       "l2": "the records of all problems (4.5 GB) exceed L2; no flush"},
+            "roofline": {"bound": "fp32", "achieved": FP32_INSTR_ADJOINT * float(tot[0]) / (ms * 1e-3) / 1e12,
+                         "peak": peak / 1e12, "unit": "Tinstr/s (FP32 pipe, lane ops)",
+                         "frac": FP32_INSTR_ADJOINT * float(tot[0]) / (ms * 1e-3) / peak,
+                         "traffic": None, "kernel_ms": ms, "instr_per_pair": FP32_INSTR_ADJOINT,
+                         "note": "device time of the whole evaluation (records prologue, pair launch, reduction)"},
+            "kernel_shape": shape, "autotune": tune,
+            # the batch call takes host poses and returns host results: the steps are end to end
+            "e2e": {"value": e2e, "unit": "pair-terms/s", "h2d_bytes_per_step": 8 * 13 * n_pose,
+                    "d2h_bytes_per_step": 8 * (1 + g.shape[-1]) * n_pose},
+            "accuracy": {"pairs_checked": len(errs), "E_rel_err": max(e[0] for e in errs),
+                         "grad_rel_err": max(e[1] for e in errs), "tolerance": {"E": 1e-6, "grad": 1e-5},
+                         "against": "FP64 oracle, 4 sampled (problem, pose) pairs, all rows"},
+            "cpu_baseline": {"value": P0.N * P0.M / cpu_s, "unit": "pair-terms/s", "cores": orc.num_threads(),
+                             "kind": "port", "sample": f"problem 0 at its first pose: {P0.N} x {P0.M} pairs "
+                                                       f"({cpu_s:.2f} s, FP64 oracle, OpenMP)"},
+            "gpu_launches": 3 * steps}
+    clocks = clk.summary()
+    if clocks:
+        line["clocks"] = clocks
+    print(json.dumps(line), flush=True)
+
+
+def ctypes_peak():
+    """The FP32 fused-multiply-add lane rate of this GPU, measured now (dugma_calibrate)."""
+    import ctypes
+    from dugma_b200 import _lib
+    peak = ctypes.c_double(0)
+    _lib.load().dugma_calibrate(0, ctypes.byref(peak), None)
+    return peak.value
 
 
 # ---------------------------------------------------------------------------
