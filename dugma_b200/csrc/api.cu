@@ -247,10 +247,12 @@ static int upload_pose(Context& c, const double* R, const double* t, double sig)
     return DUGMA_OK;
 }
 
+constexpr int kHostMoments = 512;   // c.host[512, 512 + moments): the moments copied back
+
 // copies n doubles of results + the device error word back and checks both
 static int fetch(Context& c, const double* dev, int n, double* dst)
 {
-    DUGMA_CK(cudaMemcpyAsync(c.host + 64, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    if (n > 0) DUGMA_CK(cudaMemcpyAsync(c.host + 64, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
     DUGMA_CK(cudaMemcpyAsync(c.host + 63, c.err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     DUGMA_CK(cudaStreamSynchronize(c.stream));
     int err = 0;
@@ -477,10 +479,9 @@ int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N
     DUGMA_RET(upload_pose(*c, R, t, *sig));
     DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream));
     const int nm = num_moments(c->D);
-    double mom[512];
-    DUGMA_CK(cudaMemcpyAsync(mom, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
+    DUGMA_CK(cudaMemcpyAsync(c->host + kHostMoments, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
     DUGMA_RET(fetch(*c, c->out, 0, nullptr));
-    return coef_from_moments(c->D, mom, coefficient);
+    return coef_from_moments(c->D, c->host + kHostMoments, coefficient);
 }
 
 int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double sig, int i_begin, int i_end,
@@ -496,10 +497,9 @@ int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double si
     const int nm = num_moments(c->D);
     DUGMA_CK(cudaMemsetAsync(c->mom, 0, sizeof(double) * nm, c->stream));
     DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream, i_begin, i_end, j_begin, j_end));
-    double mom[512];
-    DUGMA_CK(cudaMemcpyAsync(mom, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
+    DUGMA_CK(cudaMemcpyAsync(c->host + kHostMoments, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
     DUGMA_RET(fetch(*c, c->out, 0, nullptr));
-    return coef_from_moments(c->D, mom, coefficient);
+    return coef_from_moments(c->D, c->host + kHostMoments, coefficient);
 }
 
 int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, int model, double* E)
@@ -869,7 +869,6 @@ int dugma_graph_destroy(void* graph)
 }  // extern "C"
 
 namespace dugma {
-constexpr int kHostMoments = 512;   // c.host[512, 512 + moments): the moments copied back
 
 __global__ void pose_sig_from_sigma_kernel(double* pose, const double* sig_out)
 {

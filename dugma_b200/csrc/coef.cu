@@ -59,20 +59,55 @@ __device__ __forceinline__ void write_pair_half(Rec256* __restrict__ out, int j,
 // Records: y side (v0 = y'hi, lv; v1 = y'lo; v2/v3 = k C'_j Horner-packed; g = monomials of y')
 //          x side (v0 = x, lw; v1 = 0;     v2/v3 = k B_i Horner-packed;  g = monomials of x)
 // ---------------------------------------------------------------------------
+// One thread per point: indices [0, M_pad) are the targets, [M_pad, M_pad + N_pad) the sources.
+// reset_counter (optional) is zeroed for the pair kernel that follows on the stream.
 template <int D>
 __global__ void coef_prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
                                      const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
                                      Rec128* __restrict__ yr, Rec256* __restrict__ yr2, const float* __restrict__ x,
                                      const float* __restrict__ xinv, const float* __restrict__ lwx, int N, int N_pad,
-                                     Rec128* __restrict__ xr, Rec256* __restrict__ xr2)
+                                     Rec128* __restrict__ xr, Rec256* __restrict__ xr2, int* __restrict__ reset_counter)
 {
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
+    if (reset_counter && blockIdx.x == 0 && threadIdx.x == 0) *reset_counter = 0;
     double R[9], t[3];
     for (int k = 0; k < D * D; ++k) R[k] = pose[k];
     for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
     const double s = 1.0 / pose[kPoseSig], ks = K_EXP2 * s;
     const int stride = gridDim.x * blockDim.x;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < M_pad + N_pad; u += stride) {
+        if (u >= M_pad) {
+            const int i = u - M_pad;
+            Rec128 r;
+            float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
+            double f[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            float lw = -INFINITY;
+            if (i < N) {
+                double xd[3] = {0, 0, 0};
+                for (int a = 0; a < D; ++a) {
+                    xv[a] = x[(size_t)i * D + a];
+                    xd[a] = xv[a];
+                }
+                monomials<D>(xd, f);
+                lw = lwx[i];
+                if (lw != -INFINITY)
+                    for (int k = 0; k < NS; ++k) {
+                        const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                        const double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
+                                                (double)xinv[(size_t)i * D * D + rb + D * ra]);
+                        bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
+                    }
+            }
+            r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+            r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+            r.v2 = D == 3 ? make_float4(bp[0], bp[1], bp[2], bp[3]) : make_float4(bp[0], bp[1], bp[2], 0.f);
+            r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(f[q]) : 0.f;
+            xr[i] = r;
+            write_pair_half(xr2, i, r);
+            continue;
+        }
+        const int j = u;
         Rec128 r;
         float hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, cp[6] = {0, 0, 0, 0, 0, 0};
         double g[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -115,35 +150,6 @@ __global__ void coef_prologue_kernel(const double* __restrict__ pose, const floa
         for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(g[q]) : 0.f;
         yr[j] = r;
         write_pair_half(yr2, j, r);
-    }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
-        Rec128 r;
-        float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
-        double f[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        float lw = -INFINITY;
-        if (i < N) {
-            double xd[3] = {0, 0, 0};
-            for (int a = 0; a < D; ++a) {
-                xv[a] = x[(size_t)i * D + a];
-                xd[a] = xv[a];
-            }
-            monomials<D>(xd, f);
-            lw = lwx[i];
-            if (lw != -INFINITY)
-                for (int k = 0; k < NS; ++k) {
-                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
-                    const double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
-                                            (double)xinv[(size_t)i * D * D + rb + D * ra]);
-                    bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
-                }
-        }
-        r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
-        r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
-        r.v2 = D == 3 ? make_float4(bp[0], bp[1], bp[2], bp[3]) : make_float4(bp[0], bp[1], bp[2], 0.f);
-        r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int q = 0; q < 16; ++q) r.g[q] = q < NF ? __double2float_rn(f[q]) : 0.f;
-        xr[i] = r;
-        write_pair_half(xr2, i, r);
     }
 }
 
@@ -280,7 +286,7 @@ __global__ void __launch_bounds__(NT, MINB) coef_pass_kernel(PairArgs a)
 // pair records through the bulk-copy ring and, per tile:
 //   phase 1: every pair's p = 2^t1 + 2^t2 (target log weight folded in) once, accumulated into
 //            the sources' H2 = sum_j p g_j in registers, and written to a shared tile sP;
-//   phase 2: warp w sums its quarter of the sources against one target per lane,
+//   phase 2: warp w sums its quarter of the sources against the tile's targets,
 //            T_j = sum_i fw_i p_ij with fw_i = (w_i / 2^Lmax_x) f(x_i), and the warps' partial
 //            sums are added in fixed order into the group's H1 rows in FP64.
 // H2 is written per (chunk, source), H1 per (group, target), and the moments kernels sum those
@@ -303,15 +309,16 @@ struct FusedCoefArgs {
 template <int D>
 struct FusedCoefShape {
     static constexpr int IPT = 2, NT = 128, TJ = 16, STAGES = 4;
+    static constexpr int FOLD = 2;       // tiles summed in FP32 before each FP64 fold of the sources' sums
     static constexpr int BI = IPT * NT, NW = NT / 32, TT = 2 * TJ;
     static constexpr int NF = Feat<D>::N;          // 10 in 3D, 6 in 2D
-    static constexpr int NFH = NF / 2;             // monomials per half-warp in phase 2
-    static constexpr int NFHP = (NFH + 3) / 4 * 4; // a half's floats, padded to whole float4s
+    static constexpr int NP = NF / 2;              // monomial pairs (one f32x2 operand each)
+    static constexpr int SF = (NF + 3) / 4 * 4;    // sF row: the monomials padded to whole float4s
     static constexpr int SPS = TT + 2;   // sP row stride in floats: even (float2 stores), rows skewed across banks
     static constexpr size_t kOffBars = (size_t)STAGES * TJ * sizeof(Rec256);
     static constexpr size_t kOffP = kOffBars + 128;
     static constexpr size_t kOffF = kOffP + sizeof(float) * BI * SPS;
-    static constexpr size_t kOffT = kOffF + sizeof(float) * BI * 2 * NFHP;
+    static constexpr size_t kOffT = kOffF + sizeof(float) * BI * SF;
     static constexpr size_t kBytes = kOffT + sizeof(float) * NW * TT * (NF + 1) + 16;
 };
 
@@ -320,17 +327,17 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
 {
     using S = FusedCoefShape<D>;
     constexpr int IPT = S::IPT, NT = S::NT, TJ = S::TJ, STAGES = S::STAGES, BI = S::BI, NW = S::NW, TT = S::TT;
-    constexpr int NF = S::NF, NFH = S::NFH, NFHP = S::NFHP, SPS = S::SPS, NS = Sym<D>::N;
+    constexpr int NF = S::NF, NP = S::NP, SF = S::SF, SPS = S::SPS, NS = Sym<D>::N;
     static_assert(TT == 32, "phase 2 maps a lane of each half-warp to two targets of a tile");
-    static_assert(BI % NW == 0 && NF % 2 == 0, "sources split evenly over the warps, monomials over the halves");
+    static_assert(BI % (2 * NW) == 0 && NF % 2 == 0, "sources split evenly over the half-warps, monomials in pairs");
     constexpr uint32_t kTileBytes = TJ * sizeof(Rec256);
     extern __shared__ __align__(128) unsigned char smem[];
     Rec256(*ybuf)[TJ] = reinterpret_cast<Rec256(*)[TJ]>(smem);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::kOffBars);
     int* s_item = reinterpret_cast<int*>(smem + S::kOffBars + 64);
     float(*sP)[SPS] = reinterpret_cast<float(*)[SPS]>(smem + S::kOffP);
-    // fw rows: [first NFH monomials | pad | last NFH | pad], each half a whole number of float4s
-    float(*sF)[2 * NFHP] = reinterpret_cast<float(*)[2 * NFHP]>(smem + S::kOffF);
+    // fw rows: the NF monomials of a source, padded to whole float4s
+    float(*sF)[SF] = reinterpret_cast<float(*)[SF]>(smem + S::kOffF);
     float(*sT)[TT][NF + 1] = reinterpret_cast<float(*)[TT][NF + 1]>(smem + S::kOffT);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -388,11 +395,7 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
                 }
                 const double ws = ok ? (double)a.wx[i] * inv_wmax : 0.0;
 #pragma unroll
-                for (int q = 0; q < 2 * NFHP; ++q) {
-                    const int qf = (q < NFHP ? q : q - NFHP) + (q < NFHP ? 0 : NFH);
-                    const bool used = (q < NFHP ? q : q - NFHP) < NFH;
-                    sF[il][q] = used ? __double2float_rn(ws * (double)r.g[qf]) : 0.f;
-                }
+                for (int q = 0; q < SF; ++q) sF[il][q] = q < NF ? __double2float_rn(ws * (double)r.g[q]) : 0.f;
 #pragma unroll
                 for (int q = 0; q < NF; ++q) {
                     h[ii][q] = make_float2(0.f, 0.f);
@@ -441,13 +444,14 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
                         *reinterpret_cast<float2*>(&sP[ii * NT + tid][2 * jj]) = p;
                     }
                 }
+                if ((k + 1) % S::FOLD == 0 || k + 1 == ntiles)
 #pragma unroll
-                for (int ii = 0; ii < IPT; ++ii)
+                    for (int ii = 0; ii < IPT; ++ii)
 #pragma unroll
-                    for (int q = 0; q < NF; ++q) {
-                        H[ii][q] += (double)h[ii][q].x + (double)h[ii][q].y;
-                        h[ii][q] = make_float2(0.f, 0.f);
-                    }
+                        for (int q = 0; q < NF; ++q) {
+                            H[ii][q] += (double)h[ii][q].x + (double)h[ii][q].y;
+                            h[ii][q] = make_float2(0.f, 0.f);
+                        }
                 if (__syncthreads_or(!ok)) {
                     // a tile never arrived: drain the copies still in flight (bounded), then stop
                     if (tid == 0)
@@ -461,35 +465,46 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
                     mbar_arrive_expect_tx(&bars[st], kTileBytes);
                     bulk_g2s(&ybuf[st][0], yg + (size_t)(tile0 + k + STAGES) * TJ, kTileBytes, &bars[st]);
                 }
-                // phase 2: warp `warp` sums its quarter of the sources; lane (fh, tl) owns targets 2 tl,
-                // 2 tl + 1 of the tile (one f32x2) and monomials [fh NFH, fh NFH + NFH), so a p pair is
-                // read once for both halves and each half's monomials are one broadcast row
+                // phase 2: warp `warp` sums its quarter of the sources; lane (sh, tl) owns targets 2 tl and
+                // 2 tl + 1 of the tile and takes every other source (parity sh), each f32x2 operation a
+                // pair of monomials; the two halves then swap partials so that lane (sh, tl) holds all
+                // of the warp's sources for target 2 tl + sh
                 {
-                    const int fh = lane >> 4, tl = lane & 15;
-                    float2 acc[NFH];
+                    const int sh = lane >> 4, tl = lane & 15;
+                    float2 a0[NP], a1[NP];
 #pragma unroll
-                    for (int q = 0; q < NFH; ++q) acc[q] = make_float2(0.f, 0.f);
-                    const int i0 = warp * (BI / NW);
+                    for (int q = 0; q < NP; ++q) a0[q] = a1[q] = make_float2(0.f, 0.f);
+                    const int ib0 = warp * (BI / NW) + sh;
 #pragma unroll 4
-                    for (int i = i0; i < i0 + BI / NW; ++i) {
+                    for (int s2 = 0; s2 < BI / NW / 2; ++s2) {
+                        const int i = ib0 + 2 * s2;
                         const float2 pv = *reinterpret_cast<const float2*>(&sP[i][2 * tl]);
-                        const float4* f4 = reinterpret_cast<const float4*>(&sF[i][fh * NFHP]);
-                        float f[NFHP];
+                        const float4* f4 = reinterpret_cast<const float4*>(&sF[i][0]);
+                        float f[SF];
 #pragma unroll
-                        for (int v = 0; v < NFHP / 4; ++v) {
+                        for (int v = 0; v < SF / 4; ++v) {
                             const float4 fv = f4[v];
                             f[4 * v] = fv.x;
                             f[4 * v + 1] = fv.y;
                             f[4 * v + 2] = fv.z;
                             f[4 * v + 3] = fv.w;
                         }
+                        const float2 p0 = make_float2(pv.x, pv.x), p1 = make_float2(pv.y, pv.y);
 #pragma unroll
-                        for (int q = 0; q < NFH; ++q) acc[q] = ffma2(make_float2(f[q], f[q]), pv, acc[q]);
+                        for (int q = 0; q < NP; ++q) {
+                            const float2 fq = make_float2(f[2 * q], f[2 * q + 1]);
+                            a0[q] = ffma2(p0, fq, a0[q]);
+                            a1[q] = ffma2(p1, fq, a1[q]);
+                        }
                     }
 #pragma unroll
-                    for (int q = 0; q < NFH; ++q) {
-                        sT[warp][2 * tl][fh * NFH + q] = acc[q].x;
-                        sT[warp][2 * tl + 1][fh * NFH + q] = acc[q].y;
+                    for (int q = 0; q < NP; ++q) {
+                        const float2 give = sh ? a0[q] : a1[q];
+                        float2 keep = sh ? a1[q] : a0[q];
+                        keep.x += __shfl_xor_sync(0xffffffffu, give.x, 16);
+                        keep.y += __shfl_xor_sync(0xffffffffu, give.y, 16);
+                        sT[warp][2 * tl + sh][2 * q] = keep.x;
+                        sT[warp][2 * tl + sh][2 * q + 1] = keep.y;
                     }
                 }
                 __syncthreads();
@@ -527,17 +542,32 @@ __constant__ int c_side_n[2][2];   // [D == 3][side]
 constexpr int kMomRows = 64;       // rows staged in shared memory per pass
 constexpr int kMomThreads = 256;   // >= moments of one side (168 in 3D)
 
-// Moments of one side from the per-point H: each pass stages kMomRows rows -- H summed over
-// the target chunks (one (row, feature) entry per thread, coalesced), the row's matrix and
-// monomials -- in shared memory; each thread then owns one moment of the side and sums its
-// products over the staged rows.  Per-block partials in fixed order (deterministic).
+// One side's input to the moments kernel.
+struct MomSide {
+    const double* h;      // [copies][n][16]: the per-point H rows, one copy per chunk / group
+    int copies, n, nblk;  // rows, and the blocks that share them
+    int side;             // 0: sources (x, Sigma_x^-1), 1: targets (y, Sigma_y^-1, posed)
+    const float* p;       // the side's points, D per row
+    const float* cinv;    // its inverse covariances, D x D per row
+    double* out;          // [nblk][moments] block partials
+};
+
+// Moments from the per-point H: blockIdx.y picks the side (s0 or s1), and the side's nblk blocks
+// split its rows.  Each pass stages kMomRows rows -- H summed over its copies (one (row, feature)
+// entry per thread, coalesced), the row's matrix and monomials -- in shared memory; each thread
+// then owns one moment of the side and sums its products over the staged rows.  Per-block
+// partials in fixed order (deterministic).
 template <int D>
-__global__ void __launch_bounds__(kMomThreads) moments_kernel(const double* __restrict__ hpart, int n_jc, int n,
-                                                              int side, const double* __restrict__ pose,
-                                                              const float* __restrict__ p,
-                                                              const float* __restrict__ cinv,
-                                                              double* __restrict__ block_out)
+__global__ void __launch_bounds__(kMomThreads) moments_kernel(const MomSide s0, const MomSide s1,
+                                                              const double* __restrict__ pose)
 {
+    const MomSide ms = blockIdx.y == 0 ? s0 : s1;
+    if ((int)blockIdx.x >= ms.nblk) return;
+    const double* __restrict__ hpart = ms.h;
+    const float* __restrict__ p = ms.p;
+    const float* __restrict__ cinv = ms.cinv;
+    double* __restrict__ block_out = ms.out;
+    const int n_jc = ms.copies, n = ms.n, side = ms.side;
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     const signed char(*tab)[4] = D == 3 ? c_moment3 : c_moment2;
@@ -557,7 +587,7 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(const double* __re
     for (int k = 0; k < D * D; ++k) R[k] = pose[k];
     for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
     const double s = 1.0 / pose[kPoseSig];
-    const int per_block = (n + gridDim.x - 1) / gridDim.x;
+    const int per_block = (n + ms.nblk - 1) / ms.nblk;
     const int b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
     double acc = 0.0;
     for (int base = b0; base < b1; base += kMomRows) {
@@ -698,6 +728,44 @@ static int fused_coef_setup(int dev, int* per_sm)
     return DUGMA_OK;
 }
 
+// Work grid of the one-pass kernel: an item is a group of SB source blocks x a chunk of jc_tiles
+// target tiles, and `resident` blocks take items from a counter.  The grid minimises a model of the
+// time in units of one block's tile, fitted to B200 timings at 4K, 6K, 16K and 64K points:
+//   an item costs its SB * jc_tiles tiles plus 2 per source block (loading the sources, refilling
+//   the ring, writing the H2 rows);
+//   items <= resident: one round, 1.1 x an item (no balancing: the slowest block decides);
+//   more items: items / resident x an item, plus a quarter of an item's tiles for the tail;
+//   plus the H2 / H1 copies the moments kernels read, 128 B a row, at 54 MB per tile unit (HBM
+//   bytes in one block's tile time).
+// Up to 64 copies of either side and at most 4 GB of them.  Against the grid it replaced (at most
+// 24 x 24 copies): 64K x 64K 9.5 -> 7.9 ms, 16K 0.58 -> 0.53 ms, 4096 x 4096 0.060 -> 0.054 ms.
+struct FusedGrid {
+    int SB, n_grp, jc_tiles, n_jc;
+};
+
+static FusedGrid fused_grid(int n_ib, int total_tiles, int resident, int N, int M)
+{
+    FusedGrid best{n_ib, 1, total_tiles, 1};
+    double best_cost = INFINITY;
+    for (int g = 1; g <= std::min(n_ib, 64); ++g) {
+        const int SB = (n_ib + g - 1) / g;
+        if ((n_ib + SB - 1) / SB != g) continue;   // this grouping is met at another g
+        for (int jc = 1; jc <= std::min(total_tiles, 64); ++jc) {
+            const int jt = (total_tiles + jc - 1) / jc;
+            if ((total_tiles + jt - 1) / jt != jc) continue;
+            const double copies = ((double)jc * N + (double)g * M) * 128.0;
+            if (copies > 4e9 && (g > 1 || jc > 1)) continue;
+            const double items = (double)g * jc, tiles = (double)SB * jt, item = tiles + 2.0 * SB;
+            const double cost = (items <= resident ? 1.1 * item : items / resident * item + 0.25 * tiles) + copies / 54e6;
+            if (cost < best_cost) {
+                best_cost = cost;
+                best = {SB, g, jt, jc};
+            }
+        }
+    }
+    return best;
+}
+
 // Every source row against every target row in one pass (coef_fused_kernel), then the moments
 // of both sides from the H2 copies (one per target chunk) and the H1 copies (one per source group).
 template <int D>
@@ -710,13 +778,14 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     const int resident = c.num_sms * per_sm;
     const int n_ib = (c.N + S::BI - 1) / S::BI;
     const int total_tiles = c.M_pad / 2 / S::TJ;
-    // at most 24 copies of either side's rows; items for about four waves of resident blocks
-    int n_grp = std::min(n_ib, 24);
-    const int SB = (n_ib + n_grp - 1) / n_grp;
-    n_grp = (n_ib + SB - 1) / SB;
-    int n_jc = std::max(1, std::min(std::min(total_tiles, 24), (4 * resident + n_grp - 1) / n_grp));
-    const int jc_tiles = (total_tiles + n_jc - 1) / n_jc;
-    n_jc = (total_tiles + jc_tiles - 1) / jc_tiles;
+    if (c.coef_grid[0] == 0) {
+        const FusedGrid fg = fused_grid(n_ib, total_tiles, resident, c.N, c.M);
+        c.coef_grid[0] = fg.SB;
+        c.coef_grid[1] = fg.n_grp;
+        c.coef_grid[2] = fg.jc_tiles;
+        c.coef_grid[3] = fg.n_jc;
+    }
+    const int SB = c.coef_grid[0], n_grp = c.coef_grid[1], jc_tiles = c.coef_grid[2], n_jc = c.coef_grid[3];
     const size_t h2_doubles = (size_t)n_jc * c.N * 16, h1_doubles = (size_t)n_grp * c.M * 16;
     DUGMA_RET(c.ensure_scratch(sizeof(double) * (h2_doubles + h1_doubles)));
     FusedCoefArgs a{};
@@ -738,7 +807,7 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     a.h1_part = c.scratch + h2_doubles;
     a.counter = c.counter;
     a.err = c.err;
-    DUGMA_CK(cudaMemsetAsync(c.counter, 0, sizeof(int), s));
+    // (the coefficient prologue zeroed c.counter)
     cudaEvent_t ev1 = nullptr;
     if (c.timing) {
         if (c.tused == c.tevents.size()) {
@@ -757,9 +826,9 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
     const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
     const int nb0 = std::min(nblk, c.N), nb1 = std::min(nblk, c.M);
-    moments_kernel<D><<<nb0, kMomThreads, 0, s>>>(a.h2_part, n_jc, c.N, 0, pose_dev, c.x, c.xinv, c.mom_part);
-    moments_kernel<D><<<nb1, kMomThreads, 0, s>>>(a.h1_part, n_grp, c.M, 1, pose_dev, c.y, c.yinv,
-                                                  c.mom_part + (size_t)nblk * NM);
+    const MomSide m0{a.h2_part, n_jc, c.N, nb0, 0, c.x, c.xinv, c.mom_part};
+    const MomSide m1{a.h1_part, n_grp, c.M, nb1, 1, c.y, c.yinv, c.mom_part + (size_t)nblk * NM};
+    moments_kernel<D><<<dim3(std::max(nb0, nb1), 2), kMomThreads, 0, s>>>(m0, m1, pose_dev);
     moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(c.mom_part, nb0, c.mom_part + (size_t)nblk * NM, nb1, NM,
                                                        moments_dev);
     DUGMA_CK(cudaGetLastError());
@@ -772,13 +841,14 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
 {
     DUGMA_RET(upload_moment_tables(c.dev));
     DUGMA_RET(c.ensure_coef_records());
-    const int n = std::max(c.M_pad, c.N_pad);
-    coef_prologue_kernel<D><<<std::min((n + 255) / 256, c.num_sms * 4), 256, 0, s>>>(
-        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx,
-        c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256));
-    DUGMA_CK(cudaGetLastError());
     // all rows on both sides: one pass over the pairs; row ranges (sharding): one pass per side
-    if (i0 == 0 && i1 == c.N && j0 == 0 && j1 == c.M && c.fused_coef) return coef_fused_launch<D>(c, pose_dev, moments_dev, s);
+    const bool fused = i0 == 0 && i1 == c.N && j0 == 0 && j1 == c.M && c.fused_coef;
+    const int n = c.M_pad + c.N_pad;
+    coef_prologue_kernel<D><<<std::min((n + 127) / 128, c.num_sms * 8), 128, 0, s>>>(
+        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx,
+        c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256), fused ? c.counter : nullptr);
+    DUGMA_CK(cudaGetLastError());
+    if (fused) return coef_fused_launch<D>(c, pose_dev, moments_dev, s);
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
     // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
@@ -820,11 +890,9 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
         const int nb = std::min(nblk, rows);
         nb_side[side] = nb;
         const size_t o1 = (size_t)r0 * c.D, o2 = (size_t)r0 * c.D * c.D;
-        if (side == 0)
-            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 0, pose_dev, c.x + o1, c.xinv + o2, mom);
-        else
-            moments_kernel<D><<<nb, kMomThreads, 0, s>>>(hp, n_jc, rows, 1, pose_dev, c.y + o1, c.yinv + o2,
-                                                         mom + (size_t)nblk * NM);
+        const MomSide ms = side == 0 ? MomSide{hp, n_jc, rows, nb, 0, c.x + o1, c.xinv + o2, mom}
+                                     : MomSide{hp, n_jc, rows, nb, 1, c.y + o1, c.yinv + o2, mom + (size_t)nblk * NM};
+        moments_kernel<D><<<dim3(nb, 1), kMomThreads, 0, s>>>(ms, ms, pose_dev);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moments kernel launch failed");
     }
     if (rc == DUGMA_OK) {
