@@ -262,6 +262,19 @@ static int fetch(Context& c, const double* dev, int n, double* dst)
     return DUGMA_OK;
 }
 
+// the surrogate moments and, after them, the device error word (moments_reduce_kernel puts it
+// there) in one copy; then the coefficients from the moments
+static int fetch_moments(Context& c, double coefficient[640])
+{
+    const int nm = num_moments(c.D);
+    DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * (nm + 1), cudaMemcpyDeviceToHost,
+                             c.stream));
+    DUGMA_CK(cudaStreamSynchronize(c.stream));
+    const double err = c.host[kHostMoments + nm];
+    if (err != 0.0) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", (int)err);
+    return coef_from_moments(c.D, c.host + kHostMoments, coefficient);
+}
+
 static bool check_sizes(const Context& c, const double* N, const double* M, const double* D)
 {
     if (N && (int)*N != c.N) return false;
@@ -478,10 +491,7 @@ int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N
     if (!check_sizes(*c, N, M, D)) return set_error(DUGMA_ERR_ARG, "compi: N, M, D differ from init");
     DUGMA_RET(upload_pose(*c, R, t, *sig));
     DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream));
-    const int nm = num_moments(c->D);
-    DUGMA_CK(cudaMemcpyAsync(c->host + kHostMoments, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
-    DUGMA_RET(fetch(*c, c->out, 0, nullptr));
-    return coef_from_moments(c->D, c->host + kHostMoments, coefficient);
+    return fetch_moments(*c, coefficient);
 }
 
 int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double sig, int i_begin, int i_end,
@@ -497,9 +507,7 @@ int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double si
     const int nm = num_moments(c->D);
     DUGMA_CK(cudaMemsetAsync(c->mom, 0, sizeof(double) * nm, c->stream));
     DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream, i_begin, i_end, j_begin, j_end));
-    DUGMA_CK(cudaMemcpyAsync(c->host + kHostMoments, c->mom, sizeof(double) * nm, cudaMemcpyDeviceToHost, c->stream));
-    DUGMA_RET(fetch(*c, c->out, 0, nullptr));
-    return coef_from_moments(c->D, c->host + kHostMoments, coefficient);
+    return fetch_moments(*c, coefficient);
 }
 
 int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, int model, double* E)
@@ -903,7 +911,8 @@ int dugma_em_graph_create(float* Ptr[6], void** out)
 {
     if (!out) return set_error(DUGMA_ERR_ARG, "em_graph_create: null argument");
     GET_CTX(c, Ptr);
-    static_assert(kHostMoments + kNumMomentsMax <= kHostDoubles, "moment staging exceeds the pinned block");
+    static_assert(kHostMoments + kNumMomentsMax + 1 <= kHostDoubles && kNumMomentsMax + 1 <= kMomSlots,
+                  "moment staging exceeds the pinned block");
     // one eager step first: sizes the scratch, allocates the coefficient records and uploads the
     // moment tables, so that nothing allocates or synchronises during the capture
     const double Rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, R2[4] = {1, 0, 0, 1}, t0[3] = {0, 0, 0};

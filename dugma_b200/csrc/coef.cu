@@ -540,7 +540,7 @@ __constant__ short c_side2[2][kNumMoments2D];
 __constant__ int c_side_n[2][2];   // [D == 3][side]
 
 constexpr int kMomRows = 64;       // rows staged in shared memory per pass
-constexpr int kMomThreads = 256;   // >= moments of one side (168 in 3D)
+constexpr int kMomThreads = 320;   // >= moments of one side (168 in 3D); 32 rows x 10 monomials
 
 // One side's input to the moments kernel.
 struct MomSide {
@@ -592,15 +592,21 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(const MomSide s0, 
     double acc = 0.0;
     for (int base = b0; base < b1; base += kMomRows) {
         const int nr = min(kMomRows, b1 - base);
-        for (int e = threadIdx.x; e < nr * 16; e += blockDim.x) {
-            const int r = e >> 4, q = e & 15;
-            if (q < NF) {
-                const double* h = hpart + (size_t)(base + r) * 16 + q;
-                double v = 0.0;
-#pragma unroll 8
-                for (int c = 0; c < n_jc; ++c) v += h[(size_t)c * n * 16];
-                sH[r][q] = v;
+        // one (row, monomial) entry per thread; its copies loaded 16 at a time and added in order
+        for (int e = threadIdx.x; e < nr * NF; e += blockDim.x) {
+            const int r = e / NF, q = e - r * NF;
+            const double* h = hpart + (size_t)(base + r) * 16 + q;
+            const size_t cs = (size_t)n * 16;
+            double v = 0.0;
+            for (int c = 0; c < n_jc; c += 16) {
+                double u[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) u[k] = c + k < n_jc ? h[(size_t)(c + k) * cs] : 0.0;
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (c + k < n_jc) v += u[k];
             }
+            sH[r][q] = v;
         }
         if ((int)threadIdx.x < nr) {
             const int i = base + threadIdx.x;
@@ -647,10 +653,12 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(const MomSide s0, 
 }
 
 // out[mi] = sum over the na + nb block partials of moment mi; one warp per moment, lanes
-// strided over the blocks, fixed-order warp sum.
+// strided over the blocks, fixed-order warp sum.  out[nm] = the device error word, so that one
+// copy brings back both.
 __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, const double* __restrict__ b, int nb,
-                                      int nm, double* __restrict__ out)
+                                      int nm, double* __restrict__ out, const int* __restrict__ err)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[nm] = (double)*err;
     const int lane = threadIdx.x & 31;
     const int mi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (mi >= nm) return;
@@ -830,7 +838,7 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     const MomSide m1{a.h1_part, n_grp, c.M, nb1, 1, c.y, c.yinv, c.mom_part + (size_t)nblk * NM};
     moments_kernel<D><<<dim3(std::max(nb0, nb1), 2), kMomThreads, 0, s>>>(m0, m1, pose_dev);
     moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(c.mom_part, nb0, c.mom_part + (size_t)nblk * NM, nb1, NM,
-                                                       moments_dev);
+                                                       moments_dev, c.err);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
@@ -897,7 +905,7 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     }
     if (rc == DUGMA_OK) {
         moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(mom, nb_side[0], mom + (size_t)nblk * NM, nb_side[1], NM,
-                                                           moments_dev);
+                                                           moments_dev, c.err);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moment reduction launch failed");
     }
     return rc;
