@@ -309,7 +309,7 @@ struct FusedCoefArgs {
 template <int D>
 struct FusedCoefShape {
     static constexpr int IPT = 2, NT = 128, TJ = 16, STAGES = 4;
-    static constexpr int FOLD = 2;       // tiles summed in FP32 before each FP64 fold of the sources' sums
+    static constexpr int FOLD = 4;       // tiles summed in FP32 before each FP64 fold of the sources' sums
     static constexpr int BI = IPT * NT, NW = NT / 32, TT = 2 * TJ;
     static constexpr int NF = Feat<D>::N;          // 10 in 3D, 6 in 2D
     static constexpr int NP = NF / 2;              // monomial pairs (one f32x2 operand each)
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
                 const bool ok = mbar_wait_bounded(&bars[st], (u / STAGES) & 1u, a.err);
                 const Rec256* yb = ybuf[st];
                 // phase 1
-#pragma unroll 4
+#pragma unroll 8
                 for (int jj = 0; jj < TJ; ++jj) {
                     const Rec256& r = yb[jj];
                     float2 nh[3], nl[3], ms[6], g[NF];
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
 #pragma unroll
                     for (int q = 0; q < NP; ++q) a0[q] = a1[q] = make_float2(0.f, 0.f);
                     const int ib0 = warp * (BI / NW) + sh;
-#pragma unroll 4
+#pragma unroll 8
                     for (int s2 = 0; s2 < BI / NW / 2; ++s2) {
                         const int i = ib0 + 2 * s2;
                         const float2 pv = *reinterpret_cast<const float2*>(&sP[i][2 * tl]);
