@@ -262,13 +262,23 @@ static int fetch(Context& c, const double* dev, int n, double* dst)
     return DUGMA_OK;
 }
 
-// the surrogate moments and, after them, the device error word (moments_reduce_kernel puts it
-// there) in one copy; then the coefficients from the moments
-static int fetch_moments(Context& c, double coefficient[640])
+// The surrogate moments for a compi call: the pose goes to the coefficient prologue by value,
+// which also zeroes the error word, and the moments with the error word after them (the
+// reduction writes it there) come back through the mapped pinned staging, or by one copy when it
+// is not mapped.  Then the coefficients from the moments.
+static int coef_call(Context& c, const double* R, const double* t, double sig, int i0, int i1, int j0, int j1,
+                     double coefficient[640])
 {
+    pack_pose(c, R, t, sig, c.host);
+    CoefOpts o;
+    o.reset_err = true;
+    o.pose_value = c.host;
+    o.host_moments = c.host_dev ? c.host_dev + kHostMoments : nullptr;
+    DUGMA_RET(launch_coef(c, c.pose, c.mom, c.stream, i0, i1, j0, j1, o));
     const int nm = num_moments(c.D);
-    DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * (nm + 1), cudaMemcpyDeviceToHost,
-                             c.stream));
+    if (!o.host_moments)
+        DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * (nm + 1), cudaMemcpyDeviceToHost,
+                                 c.stream));
     DUGMA_CK(cudaStreamSynchronize(c.stream));
     const double err = c.host[kHostMoments + nm];
     if (err != 0.0) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", (int)err);
@@ -412,6 +422,10 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     c->scratch_bytes = c->arena_scratch_bytes = scratch_bytes;
     c->host = pinned_acquire();
     if (!c->host) return fail(set_error(DUGMA_ERR_NOMEM, "init: pinned staging allocation failed"));
+    if (cudaHostGetDevicePointer((void**)&c->host_dev, c->host, 0) != cudaSuccess) {
+        c->host_dev = nullptr;   // not mapped: results come back by copies
+        cudaGetLastError();
+    }
     if (cudaMemsetAsync(c->err, 0, sizeof(int) * 4, c->stream) != cudaSuccess)
         return fail(set_error(DUGMA_ERR_CUDA, "init: memset failed"));
     rc = launch_init(*c, X, X_C, Y, Y_C);
@@ -489,9 +503,7 @@ int dugma_compi(float* Ptr[6], const double* R, const double* t, const double* N
     if (!(*sig > 0)) return set_error(DUGMA_ERR_ARG, "compi: sig must be positive");
     GET_CTX(c, Ptr);
     if (!check_sizes(*c, N, M, D)) return set_error(DUGMA_ERR_ARG, "compi: N, M, D differ from init");
-    DUGMA_RET(upload_pose(*c, R, t, *sig));
-    DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream));
-    return fetch_moments(*c, coefficient);
+    return coef_call(*c, R, t, *sig, 0, -1, 0, -1, coefficient);
 }
 
 int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double sig, int i_begin, int i_end,
@@ -503,11 +515,7 @@ int dugma_compi_range(float* Ptr[6], const double* R, const double* t, double si
     if (i_begin < 0 || i_end > c->N || i_begin > i_end || j_begin < 0 || j_end > c->M || j_begin > j_end)
         return set_error(DUGMA_ERR_ARG, "compi_range: bad row ranges [%d, %d) x [%d, %d)", i_begin, i_end, j_begin,
                          j_end);
-    DUGMA_RET(upload_pose(*c, R, t, sig));
-    const int nm = num_moments(c->D);
-    DUGMA_CK(cudaMemsetAsync(c->mom, 0, sizeof(double) * nm, c->stream));
-    DUGMA_RET(launch_coef(*c, c->pose, c->mom, c->stream, i_begin, i_end, j_begin, j_end));
-    return fetch_moments(*c, coefficient);
+    return coef_call(*c, R, t, sig, i_begin, i_end, j_begin, j_end, coefficient);
 }
 
 int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, int model, double* E)

@@ -59,21 +59,36 @@ __device__ __forceinline__ void write_pair_half(Rec256* __restrict__ out, int j,
 // Records: y side (v0 = y'hi, lv; v1 = y'lo; v2/v3 = k C'_j Horner-packed; g = monomials of y')
 //          x side (v0 = x, lw; v1 = 0;     v2/v3 = k B_i Horner-packed;  g = monomials of x)
 // ---------------------------------------------------------------------------
+struct PoseBlock {
+    double v[kPoseDoubles];
+};
+
 // One thread per point: indices [0, M_pad) are the targets, [M_pad, M_pad + N_pad) the sources.
-// reset_counter (optional) is zeroed for the pair kernel that follows on the stream.
+// The pose is pv when use_pv (block 0 then writes it to `pose` for the kernels that follow), else
+// read from `pose`.  reset_counter and reset_err (each optional) are zeroed for those kernels.
 template <int D>
-__global__ void coef_prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
+__global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __restrict__ pose,
+                                     const float* __restrict__ y,
                                      const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
                                      Rec128* __restrict__ yr, Rec256* __restrict__ yr2, const float* __restrict__ x,
                                      const float* __restrict__ xinv, const float* __restrict__ lwx, int N, int N_pad,
-                                     Rec128* __restrict__ xr, Rec256* __restrict__ xr2, int* __restrict__ reset_counter)
+                                     Rec128* __restrict__ xr, Rec256* __restrict__ xr2, int* __restrict__ reset_counter,
+                                     int* __restrict__ reset_err)
 {
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
-    if (reset_counter && blockIdx.x == 0 && threadIdx.x == 0) *reset_counter = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (reset_counter) *reset_counter = 0;
+        if (reset_err) *reset_err = 0;
+        if (use_pv)
+#pragma unroll
+            for (int k = 0; k < kPoseDoubles; ++k) pose[k] = pv.v[k];
+    }
     double R[9], t[3];
-    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
-    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
-    const double s = 1.0 / pose[kPoseSig], ks = K_EXP2 * s;
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) R[k] = use_pv ? pv.v[k] : pose[k];
+#pragma unroll
+    for (int a = 0; a < D; ++a) t[a] = use_pv ? pv.v[kPoseT + a] : pose[kPoseT + a];
+    const double s = 1.0 / (use_pv ? pv.v[kPoseSig] : pose[kPoseSig]), ks = K_EXP2 * s;
     const int stride = gridDim.x * blockDim.x;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < M_pad + N_pad; u += stride) {
         if (u >= M_pad) {
@@ -654,11 +669,15 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(const MomSide s0, 
 
 // out[mi] = sum over the na + nb block partials of moment mi; one warp per moment, lanes
 // strided over the blocks, fixed-order warp sum.  out[nm] = the device error word, so that one
-// copy brings back both.
+// copy brings back both; host_out (optional, pinned host memory) receives the same nm + 1 values.
 __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, const double* __restrict__ b, int nb,
-                                      int nm, double* __restrict__ out, const int* __restrict__ err)
+                                      int nm, double* __restrict__ out, const int* __restrict__ err,
+                                      double* __restrict__ host_out)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[nm] = (double)*err;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        out[nm] = (double)*err;
+        if (host_out) host_out[nm] = (double)*err;
+    }
     const int lane = threadIdx.x & 31;
     const int mi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (mi >= nm) return;
@@ -666,7 +685,10 @@ __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, cons
     for (int k = lane; k < na; k += 32) v += a[(size_t)k * nm + mi];
     for (int k = lane; k < nb; k += 32) v += b[(size_t)k * nm + mi];
     v = warp_sum(v);
-    if (lane == 0) out[mi] = v;
+    if (lane == 0) {
+        out[mi] = v;
+        if (host_out) host_out[mi] = v;
+    }
 }
 
 
@@ -777,7 +799,8 @@ static FusedGrid fused_grid(int n_ib, int total_tiles, int resident, int N, int 
 // Every source row against every target row in one pass (coef_fused_kernel), then the moments
 // of both sides from the H2 copies (one per target chunk) and the H1 copies (one per source group).
 template <int D>
-static int coef_fused_launch(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s)
+static int coef_fused_launch(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s,
+                             double* host_moments)
 {
     using S = FusedCoefShape<D>;
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
@@ -838,25 +861,29 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     const MomSide m1{a.h1_part, n_grp, c.M, nb1, 1, c.y, c.yinv, c.mom_part + (size_t)nblk * NM};
     moments_kernel<D><<<dim3(std::max(nb0, nb1), 2), kMomThreads, 0, s>>>(m0, m1, pose_dev);
     moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(c.mom_part, nb0, c.mom_part + (size_t)nblk * NM, nb1, NM,
-                                                       moments_dev, c.err);
+                                                       moments_dev, c.err, host_moments);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
 
 template <int D>
 static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0,
-                     int j1)
+                     int j1, const CoefOpts& o)
 {
     DUGMA_RET(upload_moment_tables(c.dev));
     DUGMA_RET(c.ensure_coef_records());
     // all rows on both sides: one pass over the pairs; row ranges (sharding): one pass per side
     const bool fused = i0 == 0 && i1 == c.N && j0 == 0 && j1 == c.M && c.fused_coef;
     const int n = c.M_pad + c.N_pad;
+    PoseBlock pb{};
+    if (o.pose_value)
+        for (int k = 0; k < kPoseDoubles; ++k) pb.v[k] = o.pose_value[k];
     coef_prologue_kernel<D><<<std::min((n + 127) / 128, c.num_sms * 8), 128, 0, s>>>(
-        pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128, static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx,
-        c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256), fused ? c.counter : nullptr);
+        pb, o.pose_value ? 1 : 0, const_cast<double*>(pose_dev), c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128,
+        static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256),
+        fused ? c.counter : nullptr, o.reset_err ? c.err : nullptr);
     DUGMA_CK(cudaGetLastError());
-    if (fused) return coef_fused_launch<D>(c, pose_dev, moments_dev, s);
+    if (fused) return coef_fused_launch<D>(c, pose_dev, moments_dev, s, o.host_moments);
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
     // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
@@ -905,18 +932,19 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     }
     if (rc == DUGMA_OK) {
         moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(mom, nb_side[0], mom + (size_t)nblk * NM, nb_side[1], NM,
-                                                           moments_dev, c.err);
+                                                           moments_dev, c.err, o.host_moments);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(DUGMA_ERR_CUDA, "moment reduction launch failed");
     }
     return rc;
 }
 
-int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0, int j1)
+int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0, int j1,
+                const CoefOpts& opts)
 {
     if (i1 < 0) i1 = c.N;
     if (j1 < 0) j1 = c.M;
-    return c.D == 3 ? coef_impl<3>(c, pose_dev, moments_dev, s, i0, i1, j0, j1)
-                    : coef_impl<2>(c, pose_dev, moments_dev, s, i0, i1, j0, j1);
+    return c.D == 3 ? coef_impl<3>(c, pose_dev, moments_dev, s, i0, i1, j0, j1, opts)
+                    : coef_impl<2>(c, pose_dev, moments_dev, s, i0, i1, j0, j1, opts);
 }
 
 int coef_from_moments(int D, const double* mom, double* out640)

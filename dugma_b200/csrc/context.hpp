@@ -89,6 +89,7 @@ struct Context {
     // pinned host staging
     // [0,16) pose, [63] error word, [64,128) results, [256,512) multi-pose staging
     double* host = nullptr;                   // kHostDoubles doubles
+    double* host_dev = nullptr;               // the same memory as the device addresses it (null: not mapped)
     cudaStream_t stream = nullptr;
     int num_sms = 148;
     KernelShape shape_adj, shape_energy, shape_nn, shape_conv_adj, shape_conv_energy;
@@ -157,8 +158,15 @@ int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream
 // Surrogate coefficient moments: out_dev receives kNumMoments doubles.
 // Source rows [i0, i1) carry the source-side (B) terms, target rows [j0, j1) the target-side
 // (C') terms; -1 for i1 / j1 means all rows.  Sums over partitions of both add up to the whole.
+struct CoefOpts {
+    bool reset_err = false;              // the first kernel zeroes the device error word (no memset issued)
+    const double* pose_value = nullptr;  // a host pose block handed to the first kernel by value; that
+                                         // kernel writes it to pose_dev for the others (no copy issued)
+    double* host_moments = nullptr;      // device-visible pinned host memory that also receives the moments
+                                         // and, after them, the error word (no copy back issued)
+};
 int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0 = 0, int i1 = -1,
-                int j0 = 0, int j1 = -1);
+                int j0 = 0, int j1 = -1, const CoefOpts& opts = CoefOpts());
 int coef_from_moments(int D, const double* moments, double* coef640);
 int num_moments(int D);
 
