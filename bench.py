@@ -680,6 +680,32 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
             np.abs(A - Ao).max() / np.abs(Ao).max()), "tolerance": 2e-6, "against": "FP64 oracle, all 637"}
     finally:
         api.fr_m(h)
+    # registration size: the plugin calls and one EM iteration (update_sig then compi at its sigma,
+    # one captured graph) at 4096 x 4096, median wall time of 200 host-to-host calls each
+    P4 = synth.workload0(n=4096)
+    R4, t4 = eval_pose(P4, 0)
+    _, h = api.init(P4.X, P4.X_C, P4.Y, P4.Y_C)
+    try:
+        s4 = api.update_sig(h, R4, t4)
+        g = api.EMGraph(h)
+        try:
+            def med(fn, n=200):
+                fn()
+                fn()
+                w = []
+                for _ in range(n):
+                    a0 = time.perf_counter()
+                    fn()
+                    w.append(time.perf_counter() - a0)
+                return 1e3 * float(np.median(w))
+            res["sphere4k_calls"] = {"workload": "sphere4k: N = M = 4096, host-to-host calls, median of 200",
+                                     "compi_ms_per_call": med(lambda: api.compi(h, R4, t4, sig=s4)),
+                                     "update_sig_ms_per_call": med(lambda: api.update_sig(h, R4, t4)),
+                                     "em_iteration_ms": med(lambda: g(R4, t4))}
+        finally:
+            g.close()
+    finally:
+        api.fr_m(h)
     return res
 
 

@@ -135,13 +135,16 @@ using KernelFn = void (*)(PairArgs);
 // dEdx_dev, the per-row sums over target chunks.  h_part (nullable) receives the per-chunk
 // row buffer of h_width doubles per row, n_jc_out the chunk count.  The stationary side's
 // weights are c.wx unless w_stationary is given (the coefficient pass over targets).
+// counter_zeroed: a kernel before it on the stream zeroed c.counter (no memset issued).
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s, const float* w_stationary = nullptr);
+                        cudaStream_t s, const float* w_stationary = nullptr, bool counter_zeroed = false);
 // Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy, 2 / 3 their paired
-// forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form.
-int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol = false);
+// forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form; reset_counter
+// (optional) is zeroed for the pair kernel that follows.
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol = false,
+                    int* reset_counter = nullptr);
 // Pairwise energy (grad = false) or fused adjoint (grad = true) over source rows [i0, i1);
 // writes {E, g} to out_dev and, if dEdx_dev, dE/dx for rows [i0, i1) (relative index).
 int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1,

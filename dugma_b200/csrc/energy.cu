@@ -160,7 +160,7 @@ static int occupancy_blocks(KernelFn fn, int nt)
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s, const float* w_stationary)
+                        cudaStream_t s, const float* w_stationary, bool counter_zeroed)
 {
     const int rows = i1 - i0;
     const int BI = sh.ipt * sh.nt;
@@ -208,7 +208,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     a.err = c.err;
     if (h_part) *h_part = a.h_part;
     if (n_jc_out) *n_jc_out = n_jc;
-    DUGMA_CK(cudaMemsetAsync(c.counter, 0, sizeof(int), s));
+    if (!counter_zeroed) DUGMA_CK(cudaMemsetAsync(c.counter, 0, sizeof(int), s));
     const int grid = std::min(resident, n_items);
     cudaEvent_t ev1 = nullptr;
     if (c.timing) {
@@ -266,10 +266,11 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
     }
     // record layout: 0 scalar adjoint, 1 scalar Horner energy, 2 / 3 their packed-pair forms
     const int layout = (grad ? 0 : 1) + (v->shape.pack == 2 ? 2 : 0);
-    DUGMA_RET(launch_prologue(c, pose_dev, layout, s, xchol));
+    DUGMA_RET(launch_prologue(c, pose_dev, layout, s, xchol, c.counter));
     const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
     return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad / v->shape.pack, nv, c.Lmax_y,
-                               pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s);
+                               pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s, nullptr,
+                               true);
 }
 
 // ---------------------------------------------------------------------------

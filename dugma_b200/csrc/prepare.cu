@@ -243,15 +243,59 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
 //              of sym(Sigma_x_i^-1) (Cholesky form: (sqrt(|k| s) U_i)^T (sqrt(|k| s) U_i) = |k| B_i).
 // Rows past N / M are null records (lw = -inf, zero matrices): they contribute exactly 0.
 // ---------------------------------------------------------------------------
+// source i's record: x, the log2 weight and its matrix, either the Cholesky factor scaled by
+// sqrt(-ks) (ux given) or k B in the Horner layout
+template <int D>
+__device__ __forceinline__ void source_record(int i, const float* __restrict__ x, const float* __restrict__ xinv,
+                                              const float* __restrict__ lwx, int N, XRec* __restrict__ xrec,
+                                              const double* __restrict__ ux, double ks)
+{
+    constexpr int NS = Sym<D>::N;
+    XRec r;
+    float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
+    float lw = -INFINITY;
+    if (i < N) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) xv[a] = x[(size_t)i * D + a];
+        lw = lwx[i];
+        if (lw != -INFINITY && ux) {
+            const double r = sqrt(-ks);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) bp[k] = __double2float_rn(r * ux[(size_t)i * NS + k]);
+        } else if (lw != -INFINITY) {
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
+                                  (double)xinv[(size_t)i * D * D + rb + D * ra]);
+                double v = ks * b;
+                if (ra != rb) v = 2.0 * v;
+                bp[k] = __double2float_rn(v);
+            }
+        }
+    }
+    r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+    r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (D == 3) {
+        r.v2 = make_float4(bp[0], bp[1], bp[2], bp[3]);
+        r.v3 = make_float4(bp[4], bp[5], 0.f, 0.f);
+    } else {
+        r.v2 = make_float4(bp[0], bp[1], bp[2], 0.f);
+        r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    xrec[i] = r;
+}
+
 template <int D>
 __global__ void prologue_kernel(const double* __restrict__ pose, const float* __restrict__ y,
                                 const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
                                 int ylayout, YRec* __restrict__ yrec, float4* __restrict__ yp32,
                                 const float* __restrict__ x, const float* __restrict__ xinv,
                                 const float* __restrict__ lwx, int N, int N_pad, XRec* __restrict__ xrec,
-                                const double* __restrict__ ux)
+                                const double* __restrict__ ux, int* __restrict__ reset_counter)
 {
     constexpr int NS = Sym<D>::N;
+    if (reset_counter && blockIdx.x == 0 && threadIdx.x == 0) *reset_counter = 0;
     double R[9], t[3];
 #pragma unroll
     for (int k = 0; k < D * D; ++k) R[k] = pose[k];
@@ -260,7 +304,13 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
     const double s = 1.0 / pose[kPoseSig];
     const double ks = K_EXP2 * s;
     const int stride = gridDim.x * blockDim.x;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
+    // one thread per point: [0, M_pad) the targets, [M_pad, M_pad + N_pad) the sources
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < M_pad + N_pad; u += stride) {
+        if (u >= M_pad) {
+            source_record<D>(u - M_pad, x, xinv, lwx, N, xrec, ux, ks);
+            continue;
+        }
+        const int j = u;
         YRec r;
         float hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, cp[6] = {0, 0, 0, 0, 0, 0};
         float lv = -INFINITY;
@@ -346,57 +396,22 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
             pr[6 + h] = 0.f;
         }
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N_pad; i += stride) {
-        XRec r;
-        float xv[3] = {0, 0, 0}, bp[6] = {0, 0, 0, 0, 0, 0};
-        float lw = -INFINITY;
-        if (i < N) {
-#pragma unroll
-            for (int a = 0; a < D; ++a) xv[a] = x[(size_t)i * D + a];
-            lw = lwx[i];
-            if (lw != -INFINITY && ux) {
-                const double r = sqrt(-ks);
-#pragma unroll
-                for (int k = 0; k < NS; ++k) bp[k] = __double2float_rn(r * ux[(size_t)i * NS + k]);
-            } else if (lw != -INFINITY) {
-#pragma unroll
-                for (int k = 0; k < NS; ++k) {
-                    const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
-                    double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
-                                      (double)xinv[(size_t)i * D * D + rb + D * ra]);
-                    double v = ks * b;
-                    if (ra != rb) v = 2.0 * v;
-                    bp[k] = __double2float_rn(v);
-                }
-            }
-        }
-        r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
-        r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (D == 3) {
-            r.v2 = make_float4(bp[0], bp[1], bp[2], bp[3]);
-            r.v3 = make_float4(bp[4], bp[5], 0.f, 0.f);
-        } else {
-            r.v2 = make_float4(bp[0], bp[1], bp[2], 0.f);
-            r.v3 = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        xrec[i] = r;
-    }
 }
 
-int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol)
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol, int* reset_counter)
 {
     if (xchol && (!c.ux || c.x_indef > 0))
         return set_error(DUGMA_ERR_STATE, "Cholesky-form source records need a positive definite factor per source");
     const double* ux = xchol ? c.ux : nullptr;
-    const int n = std::max(c.M_pad, c.N_pad);
-    const int bs = 256;
-    const int g = std::min((n + bs - 1) / bs, c.num_sms * 4);
+    const int n = c.M_pad + c.N_pad;
+    const int bs = 128;
+    const int g = std::min((n + bs - 1) / bs, c.num_sms * 8);
     if (c.D == 3)
         prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
     else
         prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
