@@ -767,8 +767,10 @@ static int fused_coef_setup(int dev, int* per_sm)
 //   more items: items / resident x an item, plus a quarter of an item's tiles for the tail;
 //   plus the H2 / H1 copies the moments kernels read, 128 B a row, at 54 MB per tile unit (HBM
 //   bytes in one block's tile time).
-// Up to 64 copies of either side and at most 4 GB of them.  Against the grid it replaced (at most
-// 24 x 24 copies): 64K x 64K 9.5 -> 7.9 ms, 16K 0.58 -> 0.53 ms, 4096 x 4096 0.060 -> 0.054 ms.
+// Up to 64 copies of either side and at most 16 GB of them (a full round of items at 3M points
+// needs ~42 copies, 16 GB; the model's copy term keeps smaller problems far below).  Against the
+// grid it replaced (at most 24 x 24 copies): 64K x 64K 9.5 -> 7.9 ms, 16K 0.58 -> 0.53 ms,
+// 4096 x 4096 0.060 -> 0.054 ms.
 struct FusedGrid {
     int SB, n_grp, jc_tiles, n_jc;
 };
@@ -784,7 +786,7 @@ static FusedGrid fused_grid(int n_ib, int total_tiles, int resident, int N, int 
             const int jt = (total_tiles + jc - 1) / jc;
             if ((total_tiles + jt - 1) / jt != jc) continue;
             const double copies = ((double)jc * N + (double)g * M) * 128.0;
-            if (copies > 4e9 && (g > 1 || jc > 1)) continue;
+            if (copies > 16e9 && (g > 1 || jc > 1)) continue;
             const double items = (double)g * jc, tiles = (double)SB * jt, item = tiles + 2.0 * SB;
             const double cost = (items <= resident ? 1.1 * item : items / resident * item + 0.25 * tiles) + copies / 54e6;
             if (cost < best_cost) {
