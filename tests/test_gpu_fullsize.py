@@ -12,7 +12,11 @@ views), where the FP64 oracle cannot evaluate every pair in a test's time.  Chec
     a problem of their own against all targets: energy 1e-6, gradient 1e-5, no floor;
   * size-independent properties of the full evaluation: the sum of row-range partials over a
     partition equals the whole (FP64 rounding of the final additions, 1e-12), and two
-    evaluations give identical bits (fixed-order reductions).
+    evaluations give identical bits (fixed-order reductions);
+  * compi (the surrogate coefficients) over all rows, one pass over the pairs, against the sum
+    of row-range partials computed by the other kernels (one coefficient pass per side) over an
+    uneven partition of both clouds: 1e-6 of the largest coefficient (the two add the FP32
+    per-pair terms in different orders), and two calls give identical bits.
 """
 import numpy as np
 import pytest
@@ -72,6 +76,15 @@ def _check_full(P, R, t, rows, k_nn=1):
         assert abs(Eo) >= 1e-3 * abs(E)        # they do carry the energy
         assert abs(Es - Eo) <= 1e-6 * abs(Eo)
         assert _rel(gs, go) <= 1e-5
+        # compi: one pass over all pairs against the per-side passes over a partition
+        A = api.compi(h, R, t, sig=sig)
+        assert np.array_equal(A, api.compi(h, R, t, sig=sig))
+        m = P.M
+        ci, cj = [0, n // 3, n], [0, m // 5, m]
+        S = sum(api.compi_range(h, R, t, sig, ci[k], ci[k + 1], cj[k], cj[k + 1]) for k in range(2))
+        err = np.abs(S - A).max() / np.abs(A).max()
+        print(f"compi: one pass against the per-side passes, max |dA| / max |A| = {err:.2e}")
+        assert err <= 1e-6
     finally:
         api.fr_m(h)
 
