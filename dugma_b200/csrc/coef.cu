@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(NT, MINB) coef_pass_kernel(PairArgs a)
 //   phase 2: warp w sums its quarter of the sources against the tile's targets,
 //            T_j = sum_i fw_i p_ij with fw_i = (w_i / 2^Lmax_x) f(x_i), and the warps' partial
 //            sums are added in fixed order into the group's H1 rows in FP64.
-// H2 is written per (chunk, source), H1 per (group, target), and the moments kernels sum those
+// H2 is written per (chunk, source), H1 per (group, target), and the moments kernel sums those
 // copies in fixed order: the same moments as the two passes, each pair's exponentials computed
 // once, and no atomics.
 // ---------------------------------------------------------------------------
@@ -765,7 +765,7 @@ static int fused_coef_setup(int dev, int* per_sm)
 //   the ring, writing the H2 rows);
 //   items <= resident: one round, 1.1 x an item (no balancing: the slowest block decides);
 //   more items: items / resident x an item, plus a quarter of an item's tiles for the tail;
-//   plus the H2 / H1 copies the moments kernels read, 128 B a row, at 54 MB per tile unit (HBM
+//   plus the H2 / H1 copies the moments kernel reads, 128 B a row, at 54 MB per tile unit (HBM
 //   bytes in one block's tile time).
 // Up to 64 copies of either side and at most 16 GB of them (a full round of items at 3M points
 // needs ~42 copies, 16 GB; the model's copy term keeps smaller problems far below).  Against the
