@@ -869,7 +869,7 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
 }
 
 template <int D>
-static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0,
+static int coef_impl(Context& c, double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0,
                      int j1, const CoefOpts& o)
 {
     DUGMA_RET(upload_moment_tables(c.dev));
@@ -881,7 +881,7 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     if (o.pose_value)
         for (int k = 0; k < kPoseDoubles; ++k) pb.v[k] = o.pose_value[k];
     coef_prologue_kernel<D><<<std::min((n + 127) / 128, c.num_sms * 8), 128, 0, s>>>(
-        pb, o.pose_value ? 1 : 0, const_cast<double*>(pose_dev), c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128,
+        pb, o.pose_value ? 1 : 0, pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128,
         static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256),
         fused ? c.counter : nullptr, o.reset_err ? c.err : nullptr);
     DUGMA_CK(cudaGetLastError());
@@ -940,7 +940,7 @@ static int coef_impl(Context& c, const double* pose_dev, double* moments_dev, cu
     return rc;
 }
 
-int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0, int j1,
+int launch_coef(Context& c, double* pose_dev, double* moments_dev, cudaStream_t s, int i0, int i1, int j0, int j1,
                 const CoefOpts& opts)
 {
     if (i1 < 0) i1 = c.N;

@@ -168,7 +168,7 @@ struct CoefOpts {
     double* host_moments = nullptr;      // device-visible pinned host memory that also receives the moments
                                          // and, after them, the error word (no copy back issued)
 };
-int launch_coef(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s, int i0 = 0, int i1 = -1,
+int launch_coef(Context& c, double* pose_dev, double* moments_dev, cudaStream_t s, int i0 = 0, int i1 = -1,
                 int j0 = 0, int j1 = -1, const CoefOpts& opts = CoefOpts());
 int coef_from_moments(int D, const double* moments, double* coef640);
 int num_moments(int D);
