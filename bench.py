@@ -698,10 +698,15 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
                     fn()
                     w.append(time.perf_counter() - a0)
                 return 1e3 * float(np.median(w))
-            res["sphere4k_calls"] = {"workload": "sphere4k: N = M = 4096, host-to-host calls, median of 200",
-                                     "compi_ms_per_call": med(lambda: api.compi(h, R4, t4, sig=s4)),
-                                     "update_sig_ms_per_call": med(lambda: api.update_sig(h, R4, t4)),
-                                     "em_iteration_ms": med(lambda: g(R4, t4))}
+            with Clocks(os.path.join(clock_dir, "dugma_clocks_sphere4k.csv"), torch.cuda.current_device()) as clk:
+                ent = {"workload": "sphere4k: N = M = 4096, host-to-host calls, median of 200",
+                       "compi_ms_per_call": med(lambda: api.compi(h, R4, t4, sig=s4)),
+                       "update_sig_ms_per_call": med(lambda: api.update_sig(h, R4, t4)),
+                       "em_iteration_ms": med(lambda: g(R4, t4))}
+            c = clk.summary()
+            if c:
+                ent["clocks"] = c
+            res["sphere4k_calls"] = ent
         finally:
             g.close()
     finally:
@@ -709,23 +714,30 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
     return res
 
 
-def config_kinect(modes=(0, 1)):
+def config_kinect(modes=(0, 1), clock_dir="/tmp"):
     """The reference's 30 real Kinect scenes (tests/golden/kinect_scenes.npz) registered end to end
     from the identity pose with main_kinect_real_application.m's settings: per mode, the medians of
     the error measures against the ground truth, the distance to the authors' recorded poses, and
-    the seconds per scene (host clouds in, pose out) against the authors' recorded seconds."""
+    the seconds per scene (host clouds in, pose out) against the authors' recorded seconds, with
+    the SM clocks sampled over the mode's 30 registrations."""
+    import torch
     from dugma_b200 import evaluate
     path = os.path.join(ROOT, "tests", "golden", "kinect_scenes.npz")
     out = {"workload": "kinect30: the reference's 30 two-Kinect scenes (N, M 463..5334), identity start, 300 "
                        "iterations, tolerances 1e-4 / 1e-8 / 1e-9"}
+    scenes = list(evaluate.scenes_from_npz(path))
     for mode in modes:
-        rows = [evaluate.register(P, mode, 300, rec) for P, rec in evaluate.scenes_from_npz(path)]
+        with Clocks(os.path.join(clock_dir, f"dugma_clocks_kinect{mode}.csv"), torch.cuda.current_device()) as clk:
+            rows = [evaluate.register(P, mode, 300, rec) for P, rec in scenes]
         s = evaluate.summarise(rows, mode)
         out[f"mode{mode}"] = {k: s[k]["median"] for k in ("error_R", "error_t", "deg", "iterations", "seconds",
                                                           "vs_recorded_deg", "vs_recorded_t", "recorded_error_R",
                                                           "recorded_error_t", "recorded_seconds")}
         out[f"mode{mode}"]["max_vs_recorded_deg"] = s["vs_recorded_deg"]["max"]
         out[f"mode{mode}"]["statistic"] = "median over the 30 scenes (max where named)"
+        c = clk.summary()
+        if c:
+            out[f"mode{mode}"]["clocks"] = c
     return out
 
 
@@ -751,7 +763,7 @@ def run_configs(L, peak, clock_dir):
     run("curve2d_64k", lambda: config_single(L, "cfg5", synth.workload5(), 0, peak, clock_dir=clock_dir))
     run("conv_harmonic64k", lambda: config_single(L, "conv", synth.workload2(), 1, peak, clock_dir=clock_dir))
     run("plugins_harmonic64k", lambda: config_plugins(L, synth.workload2(), peak, clock_dir=clock_dir))
-    run("kinect30_registration", config_kinect)
+    run("kinect30_registration", lambda: config_kinect(clock_dir=clock_dir))
     out["seconds"] = timings
     return out
 
