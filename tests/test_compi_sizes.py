@@ -53,3 +53,33 @@ def _check(D, n, m, seed):
         assert err <= (5e-6 if n * m == 1 else 2e-6), (n, m, err)
     finally:
         api.fr_m(h)
+
+
+@pytest.mark.parametrize("side", ["sources", "targets"])
+def test_every_covariance_of_one_cloud_neglected(side):
+    """Every covariance of one cloud with det <= 0: all its weights are zero (init.cu:48-57), so
+    every pair term vanishes -- compi's coefficients, the energy and its gradient are exactly
+    zero, as in the oracle -- and the weight normaliser of that cloud (log2 of the largest
+    weight, -inf here) must not turn into a NaN anywhere."""
+    X, XC, Y, YC = _problem_small(3, 300, 280, seed=4)
+    bad = np.diag([-1.0, 1.0, 1.0])
+    if side == "sources":
+        XC = np.repeat(bad[None], len(X), axis=0)
+    else:
+        YC = np.repeat(bad[None], len(Y), axis=0)
+    R, t = _pose(3, seed=2, scale=0.1)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, h = api.init(X, XC, Y, YC)
+    try:
+        sig = api.update_sig(h, R, t)
+        assert np.isfinite(sig) and sig > 0
+        A = api.compi(h, R, t, sig=sig)
+        Ao = orc.State(X, XC, Y, YC).coef(R, t, sig)[: A.size]
+        assert np.all(Ao == 0.0)
+        assert np.all(A == 0.0)
+        E, g, _ = api.energy_grad(h, R, t, sig)
+        assert E == 0.0 and np.all(g == 0.0)
+    finally:
+        api.fr_m(h)
