@@ -1,14 +1,17 @@
 """Registration accuracy and time over two-view scenes.
 
     python -m dugma_b200.evaluate [--mode 0|1] [--max-iteration 300]
-                                  [--scenes 30 | --mat-dir DIR [--results-dir DIR] | --npz FILE]
+                                  [--scenes 30 | --mat-dir DIR [--results-dir DIR] | --npz FILE |
+                                   --sim2d FILE [--models S|F] [--trials 100]]
 
 Scenes come from the seeded synthetic stand-ins (synth.kinect_like, default), from a
 directory of .mat files in the reference dataset's layout ({k}.mat holding X, Y, X_C, Y_C,
 R_G, t_G; dataset_all "Read Me"), optionally with a directory of recorded results
 (Ours_{k}_result.mat holding R, t) to compare against, or from an .npz holding the same
 scenes (X{k}, Y{k} point rows, cx{k}, cy{k} isotropic covariance scales, RG{k}, tG{k} and the
-recorded Ra{k}, ta{k}, sa{k}).  Each scene is registered from the identity pose with the
+recorded Ra{k}, ta{k}, sa{k}), or drawn by the reference's 2D simulation protocol from the 2D
+model contours of tests/golden/shapes2d.npz (--sim2d; main_simulation.m:17-28, whose settings
+differ only in allowing 700 iterations, line 47).  Each scene is registered from the identity pose with the
 settings of main_kinect_real_application.m:14-17 (300 iterations, rotation / translation /
 sigma tolerances 1e-4 / 1e-8 / 1e-9) and scored with its error measures (lines 33-35 there):
 ||I - R pinv(R_G)||_F and ||t - t_G||, plus the geodesic rotation angle, and, where a
@@ -21,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import time
@@ -32,21 +36,30 @@ from .pose import rotation_error_deg
 from .synth import Problem
 
 
+def _angle_deg(R, R_G) -> float:
+    """The rotation angle between R and R_G in degrees (2D or 3D)."""
+    if np.asarray(R).shape[0] == 2:
+        Q = np.asarray(R) @ np.asarray(R_G).T
+        return abs(math.degrees(math.atan2(Q[1, 0], Q[0, 0])))
+    return rotation_error_deg(R, R_G)
+
+
 def register(P: Problem, mode: int = 0, max_iteration: int = 300, recorded=None) -> dict:
     """Register one scene from the identity pose; recorded = (R, t[, seconds]) or None."""
+    D = P.X.shape[1]
     t0 = time.perf_counter()
-    R, t, stats = api.DUGMA(P.X, P.Y, P.X_C, P.Y_C, np.eye(3), np.zeros(3), Max_Iteration=max_iteration,
+    R, t, stats = api.DUGMA(P.X, P.Y, P.X_C, P.Y_C, np.eye(D), np.zeros(D), Max_Iteration=max_iteration,
                             accuracy_rotation=1e-4, accuracy_translation=1e-8, accuracy_sig=1e-9, mode=mode)
     wall = time.perf_counter() - t0
     row = {"scene": P.name, "N": P.N, "M": P.M,
-           "error_R": float(np.linalg.norm(np.eye(3) - R @ np.linalg.pinv(P.R_G))),
+           "error_R": float(np.linalg.norm(np.eye(D) - R @ np.linalg.pinv(P.R_G))),
            "error_t": float(np.linalg.norm(t - P.t_G)),
-           "deg": rotation_error_deg(R, P.R_G), "iterations": int(stats[0]), "seconds": wall}
+           "deg": _angle_deg(R, P.R_G), "iterations": int(stats[0]), "seconds": wall}
     if recorded is not None:
         Ra, ta = recorded[0], recorded[1]
         row["recorded_error_R"] = float(np.linalg.norm(np.eye(3) - Ra @ np.linalg.pinv(P.R_G)))
         row["recorded_error_t"] = float(np.linalg.norm(ta - P.t_G))
-        row["vs_recorded_deg"] = rotation_error_deg(R, Ra)
+        row["vs_recorded_deg"] = _angle_deg(R, Ra)
         row["vs_recorded_t"] = float(np.linalg.norm(t - ta))
         if len(recorded) > 2:
             row["recorded_seconds"] = float(recorded[2])
@@ -99,6 +112,17 @@ def scenes_from_npz(path: str):
         yield P, rec
 
 
+def scenes_simulation2d(path: str, models: str = "S", trials: int = 100):
+    """The reference's 2D simulation (main_simulation.m:17-28, produce_point_cloud.m) on the
+    model contours of an .npz written by tests/golden/make_shapes2d.py: trial k draws a problem
+    from model (k mod 100) + 1 with the generator restated in synth.simulation2d.  models: "S"
+    (2D_SHAPE_MODEL) or "F" (2D_Fish_MODEL, 200 points)."""
+    f = np.load(path)
+    for k in range(trials):
+        m = k % 100 + 1
+        yield synth.simulation2d(f[f"{models}{m}"], k, name=f"{models}{m}_trial{k}"), None
+
+
 def summarise(rows, mode) -> dict:
     summ = {"scenes": len(rows), "mode": mode}
     for key in ("error_R", "error_t", "deg", "iterations", "seconds", "vs_recorded_deg", "vs_recorded_t",
@@ -115,18 +139,26 @@ def main(argv=None):
     ap.add_argument("--mat-dir", default="", help="directory of {k}.mat scenes in the reference layout")
     ap.add_argument("--results-dir", default="", help="directory of Ours_{k}_result.mat recorded results")
     ap.add_argument("--npz", default="", help=".npz of scenes (see the module docstring)")
+    ap.add_argument("--sim2d", default="", help=".npz of 2D model contours (tests/golden/shapes2d.npz): the "
+                                               "reference's 2D simulation protocol")
+    ap.add_argument("--models", default="S", help="with --sim2d: S (shapes) or F (fish)")
+    ap.add_argument("--trials", type=int, default=100, help="with --sim2d: problems drawn")
     ap.add_argument("--mode", type=int, default=0)
-    ap.add_argument("--max-iteration", type=int, default=300)
+    ap.add_argument("--max-iteration", type=int, default=0, help="default 300, or 700 with --sim2d "
+                                                                  "(main_simulation.m:47)")
     a = ap.parse_args(argv)
-    if a.npz:
+    if a.sim2d:
+        src = scenes_simulation2d(a.sim2d, a.models, a.trials)
+    elif a.npz:
         src = scenes_from_npz(a.npz)
     elif a.mat_dir:
         src = scenes_from_mat(a.mat_dir, a.results_dir or None)
     else:
         src = scenes_synthetic(a.scenes)
+    max_it = a.max_iteration or (700 if a.sim2d else 300)
     rows = []
     for P, rec in src:
-        r = register(P, a.mode, a.max_iteration, rec)
+        r = register(P, a.mode, max_it, rec)
         rows.append(r)
         print(json.dumps(r), flush=True)
     print(json.dumps({"summary": summarise(rows, a.mode)}), flush=True)
