@@ -741,20 +741,21 @@ def config_kinect(modes=(0, 1), clock_dir="/tmp"):
     return out
 
 
-def config_sim2d(clock_dir="/tmp", trials=100):
-    """The reference's 2D simulation protocol (main_simulation.m:17-56: random rotation within
-    30 deg, translation, noise, outliers and occlusion drawn per problem) on its own 2D model
-    contours (tests/golden/shapes2d.npz), registered with the reference's loop from the identity
-    with main_simulation.m's settings; per model set the medians of the error measures, the share
-    of problems within 2 deg of the ground truth and the seconds per registration."""
+def config_simulation(clock_dir="/tmp", trials=100):
+    """The reference's simulation protocol (main_simulation.m:17-56: random rotation within 30 deg,
+    translation, noise, outliers and occlusion drawn per problem) on its own models
+    (tests/golden/sim_models.npz: 2D shape and fish contours, the 3D surface), registered with
+    the reference's loop from the identity with main_simulation.m's settings; per model set the
+    medians of the error measures, the share of problems within 2 deg of the ground truth and the
+    seconds per registration."""
     import torch
     from dugma_b200 import evaluate
-    path = os.path.join(ROOT, "tests", "golden", "shapes2d.npz")
-    out = {"workload": f"sim2d: {trials} problems per model set (2D_SHAPE_MODEL 'S', 2D_Fish_MODEL/dataset2D_200 "
-                       "'F'), seeded, mode 0, 700 iterations, tolerances 1e-4 / 1e-8 / 1e-9"}
-    for models in ("S", "F"):
-        with Clocks(os.path.join(clock_dir, f"dugma_clocks_sim2d{models}.csv"), torch.cuda.current_device()) as clk:
-            rows = [evaluate.register(P, 0, 700) for P, _ in evaluate.scenes_simulation2d(path, models, trials)]
+    path = os.path.join(ROOT, "tests", "golden", "sim_models.npz")
+    out = {"workload": f"simulation: {trials} problems per model set (2D_SHAPE_MODEL 'S', 2D_Fish_MODEL/dataset2D_200 "
+                       "'F', 3D_SHAPE 'T'), seeded, mode 0, 700 iterations, tolerances 1e-4 / 1e-8 / 1e-9"}
+    for models in ("S", "F", "T"):
+        with Clocks(os.path.join(clock_dir, f"dugma_clocks_sim{models}.csv"), torch.cuda.current_device()) as clk:
+            rows = [evaluate.register(P, 0, 700) for P, _ in evaluate.scenes_simulation(path, models, trials)]
         deg = np.array([r["deg"] for r in rows])
         ent = {k: float(np.median([r[k] for r in rows])) for k in ("error_R", "error_t", "deg", "iterations", "seconds")}
         ent["within_2deg"] = float(np.mean(deg < 2.0))
@@ -789,7 +790,7 @@ def run_configs(L, peak, clock_dir):
     run("conv_harmonic64k", lambda: config_single(L, "conv", synth.workload2(), 1, peak, clock_dir=clock_dir))
     run("plugins_harmonic64k", lambda: config_plugins(L, synth.workload2(), peak, clock_dir=clock_dir))
     run("kinect30_registration", lambda: config_kinect(clock_dir=clock_dir))
-    run("sim2d_registration", lambda: config_sim2d(clock_dir=clock_dir))
+    run("simulation_registration", lambda: config_simulation(clock_dir=clock_dir))
     out["seconds"] = timings
     return out
 

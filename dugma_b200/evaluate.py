@@ -2,16 +2,16 @@
 
     python -m dugma_b200.evaluate [--mode 0|1] [--max-iteration 300]
                                   [--scenes 30 | --mat-dir DIR [--results-dir DIR] | --npz FILE |
-                                   --sim2d FILE [--models S|F] [--trials 100]]
+                                   --sim FILE [--models S|F|T] [--trials 100]]
 
 Scenes come from the seeded synthetic stand-ins (synth.kinect_like, default), from a
 directory of .mat files in the reference dataset's layout ({k}.mat holding X, Y, X_C, Y_C,
 R_G, t_G; dataset_all "Read Me"), optionally with a directory of recorded results
 (Ours_{k}_result.mat holding R, t) to compare against, or from an .npz holding the same
 scenes (X{k}, Y{k} point rows, cx{k}, cy{k} isotropic covariance scales, RG{k}, tG{k} and the
-recorded Ra{k}, ta{k}, sa{k}), or drawn by the reference's 2D simulation protocol from the 2D
-model contours of tests/golden/shapes2d.npz (--sim2d; main_simulation.m:17-28, whose settings
-differ only in allowing 700 iterations, line 47).  Each scene is registered from the identity pose with the
+recorded Ra{k}, ta{k}, sa{k}), or drawn by the reference's simulation protocol from its 2D model
+contours and 3D model surface in tests/golden/sim_models.npz (--sim; main_simulation.m:17-35,
+whose settings differ only in allowing 700 iterations, line 47).  Each scene is registered from the identity pose with the
 settings of main_kinect_real_application.m:14-17 (300 iterations, rotation / translation /
 sigma tolerances 1e-4 / 1e-8 / 1e-9) and scored with its error measures (lines 33-35 there):
 ||I - R pinv(R_G)||_F and ||t - t_G||, plus the geodesic rotation angle, and, where a
@@ -112,15 +112,16 @@ def scenes_from_npz(path: str):
         yield P, rec
 
 
-def scenes_simulation2d(path: str, models: str = "S", trials: int = 100):
-    """The reference's 2D simulation (main_simulation.m:17-28, produce_point_cloud.m) on the
-    model contours of an .npz written by tests/golden/make_shapes2d.py: trial k draws a problem
-    from model (k mod 100) + 1 with the generator restated in synth.simulation2d.  models: "S"
-    (2D_SHAPE_MODEL) or "F" (2D_Fish_MODEL, 200 points)."""
+def scenes_simulation(path: str, models: str = "S", trials: int = 100):
+    """The reference's simulation (main_simulation.m:17-56, produce_point_cloud.m) on the models
+    of an .npz written by tests/golden/make_sim_models.py: trial k draws a problem from model
+    (k mod 100) + 1 of the set with the generator restated in synth.simulation.  models: "S"
+    (2D_SHAPE_MODEL), "F" (2D_Fish_MODEL, 200 points) or "T" (the 3D_SHAPE surface, the one
+    3D model released)."""
     f = np.load(path)
     for k in range(trials):
-        m = k % 100 + 1
-        yield synth.simulation2d(f[f"{models}{m}"], k, name=f"{models}{m}_trial{k}"), None
+        key = "T1" if models == "T" else f"{models}{k % 100 + 1}"
+        yield synth.simulation(f[key], k, name=f"{key}_trial{k}"), None
 
 
 def summarise(rows, mode) -> dict:
@@ -139,23 +140,23 @@ def main(argv=None):
     ap.add_argument("--mat-dir", default="", help="directory of {k}.mat scenes in the reference layout")
     ap.add_argument("--results-dir", default="", help="directory of Ours_{k}_result.mat recorded results")
     ap.add_argument("--npz", default="", help=".npz of scenes (see the module docstring)")
-    ap.add_argument("--sim2d", default="", help=".npz of 2D model contours (tests/golden/shapes2d.npz): the "
-                                               "reference's 2D simulation protocol")
-    ap.add_argument("--models", default="S", help="with --sim2d: S (shapes) or F (fish)")
-    ap.add_argument("--trials", type=int, default=100, help="with --sim2d: problems drawn")
+    ap.add_argument("--sim", default="", help=".npz of simulation models (tests/golden/sim_models.npz): the "
+                                             "reference's simulation protocol")
+    ap.add_argument("--models", default="S", help="with --sim: S (2D shapes), F (2D fish) or T (3D)")
+    ap.add_argument("--trials", type=int, default=100, help="with --sim: problems drawn")
     ap.add_argument("--mode", type=int, default=0)
-    ap.add_argument("--max-iteration", type=int, default=0, help="default 300, or 700 with --sim2d "
+    ap.add_argument("--max-iteration", type=int, default=0, help="default 300, or 700 with --sim "
                                                                   "(main_simulation.m:47)")
     a = ap.parse_args(argv)
-    if a.sim2d:
-        src = scenes_simulation2d(a.sim2d, a.models, a.trials)
+    if a.sim:
+        src = scenes_simulation(a.sim, a.models, a.trials)
     elif a.npz:
         src = scenes_from_npz(a.npz)
     elif a.mat_dir:
         src = scenes_from_mat(a.mat_dir, a.results_dir or None)
     else:
         src = scenes_synthetic(a.scenes)
-    max_it = a.max_iteration or (700 if a.sim2d else 300)
+    max_it = a.max_iteration or (700 if a.sim else 300)
     rows = []
     for P, rec in src:
         r = register(P, a.mode, max_it, rec)

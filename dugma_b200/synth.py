@@ -373,8 +373,8 @@ WORKLOADS = {0: workload0, 1: workload1, 2: workload2, 4: workload4, 5: workload
 
 
 # ---------------------------------------------------------------------------
-# 2D simulation protocol of main_simulation.m:17-28 on a model contour (the reference's
-# 2D_SHAPE_MODEL / 2D_Fish_MODEL points, tests/golden/shapes2d.npz), seeded
+# The simulation protocol of main_simulation.m:17-35 on a model (the reference's 2D_SHAPE_MODEL /
+# 2D_Fish_MODEL contours and its 3D_SHAPE surface, tests/golden/sim_models.npz), seeded
 # ---------------------------------------------------------------------------
 def _radius(P: np.ndarray):
     """get_radius.m:4-21: the centroid and sqrt(mean squared distance to it) of (n, D) points."""
@@ -382,54 +382,72 @@ def _radius(P: np.ndarray):
     return mean, math.sqrt(float(((P - mean) ** 2).sum()) / len(P))
 
 
-def _noise_and_sampling2d(rng, model: np.ndarray, R_G: np.ndarray, t_G: np.ndarray, noi: float, miss: float,
-                          for_y: bool):
-    """noise_and_sampling2D.m:1-95 for one of its two outputs: per model point an axis-aligned
-    covariance diag(exp(fa r_x), exp(fa r_y)) with r = |noi * randn| (fa = 3.4657), the point
-    moved by r * randn * radius per axis, a contiguous occluded patch (the round(miss * M)
-    points nearest a random model point) left out, and the rest kept with probability 0.9 (X) or
-    0.85 (Y); Y's points and covariances are then mapped by (R_G, t_G)."""
+def _noise_and_sampling(rng, model: np.ndarray, R_G: np.ndarray, t_G: np.ndarray, noi: float, miss: float,
+                        for_y: bool):
+    """noise_and_sampling2D.m:1-95 / noise_and_sampling3D.m:1-120 for one of their two outputs:
+    per model point an axis-aligned covariance diag(exp(fa r_a)) with r_a = |noi * randn| per
+    axis (fa = 3.4657), the point moved by r_a * randn * radius along each axis, a contiguous
+    occluded patch (the round(miss * M) points nearest a random model point) left out, and the
+    rest kept with probability 0.9 (X) or 0.85 (Y); Y's points and covariances are then mapped by
+    (R_G, t_G)."""
     fa = 3.4657
-    M = len(model)
+    M, D = model.shape
     occ = rng.integers(0, M)
     d2 = ((model - model[occ]) ** 2).sum(axis=1)
     occluded = np.zeros(M, bool)
     occluded[np.argsort(d2, kind="stable")[:int(round(miss * M))]] = True
     _, radius = _radius(model)
-    rx, ry = np.abs(noi * rng.standard_normal(M)), np.abs(noi * rng.standard_normal(M))
-    vx, vy = np.exp(rx * fa), np.exp(ry * fa)
-    moved = model + np.stack([rx * rng.standard_normal(M), ry * rng.standard_normal(M)], axis=1) * radius
+    r = np.abs(noi * rng.standard_normal((M, D)))
+    moved = model + r * rng.standard_normal((M, D)) * radius
     keep = (rng.random(M) <= (0.85 if for_y else 0.9)) & ~occluded
     P = moved[keep]
-    C = np.zeros((int(keep.sum()), 2, 2))
-    C[:, 0, 0], C[:, 1, 1] = vx[keep], vy[keep]
+    C = np.zeros((int(keep.sum()), D, D))
+    for a in range(D):
+        C[:, a, a] = np.exp(r[keep, a] * fa)
     if for_y:
         P = P @ R_G.T + t_G
         C = R_G @ C @ R_G.T
     return P, C
 
 
-def simulation2d(model: np.ndarray, trial: int = 0, rand_degree: float = 30.0, rand_noise: float = 0.1,
-                 rand_outliers: int = 50, rand_miss_rate: float = 0.1, name: str = "") -> Problem:
-    """One registration problem of the reference's 2D simulation (produce_point_cloud.m:1-55 with
-    main_simulation.m:19-22's ranges): a rotation by U[-30, 30] deg and a translation in
-    [-0.5, 0.5]^2, a noise level in [0, 0.1], up to 50 outliers (add_outliers.m: Gaussian around
-    the model's centroid with its radius as deviation, drawn separately for X and Y) and an
-    occlusion rate in [0, 0.1]; X and Y are sampled from the model independently
-    (noise_and_sampling2D.m).  Returned with the ground truth of produce_point_cloud.m, the
-    pose that maps Y back onto X (lines 49-50): R_G @ y + t_G ~ x.  model: (n, 2) contour points."""
-    rng = rng_for(60, trial)
-    deg = rand_degree * (2 * rng.random() - 1)
+def _eul2rotm_zyx(z: float, y: float, x: float) -> np.ndarray:
+    """Rotation from ZYX Euler angles in radians: Rz(z) Ry(y) Rx(x)."""
+    cz, sz, cy, sy, cx, sx = math.cos(z), math.sin(z), math.cos(y), math.sin(y), math.cos(x), math.sin(x)
+    Rz = np.array([[cz, -sz, 0.0], [sz, cz, 0.0], [0.0, 0.0, 1.0]])
+    Ry = np.array([[cy, 0.0, sy], [0.0, 1.0, 0.0], [-sy, 0.0, cy]])
+    Rx = np.array([[1.0, 0.0, 0.0], [0.0, cx, -sx], [0.0, sx, cx]])
+    return Rz @ Ry @ Rx
+
+
+def simulation(model: np.ndarray, trial: int = 0, rand_degree: float = 30.0, rand_noise: float = 0.1,
+               rand_outliers: int | None = None, rand_miss_rate: float = 0.1, name: str = "") -> Problem:
+    """One registration problem of the reference's simulation (produce_point_cloud.m:1-52 with
+    main_simulation.m:19-22 / 31-34's ranges): a rotation by U[-30, 30] deg (2D), or by ZYX Euler
+    angles each in U[-30, 30] deg (3D, eul2rotm), a translation in [-0.5, 0.5]^D, a noise level in
+    [0, 0.1], up to 50 (2D) or 100 (3D) outliers (add_outliers.m: Gaussian around the model's
+    centroid with its radius as deviation, drawn separately for X and Y) and an occlusion rate in
+    [0, 0.1]; X and Y are sampled from the model independently (noise_and_sampling2D.m /
+    noise_and_sampling3D.m).  Returned with the ground truth of produce_point_cloud.m:49-50, the
+    pose that maps Y back onto X: R_G @ y + t_G ~ x.  model: (n, D) points."""
+    model = np.asarray(model, dtype=np.float64)
+    D = model.shape[1]
+    if rand_outliers is None:
+        rand_outliers = 50 if D == 2 else 100
+    rng = rng_for(60 if D == 2 else 61, trial)
+    if D == 2:
+        deg = rand_degree * (2 * rng.random() - 1)
+        c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))
+        R = np.array([[c, -s], [s, c]])
+    else:
+        dx, dy, dz = (rand_degree * (2 * rng.random() - 1) for _ in range(3))
+        R = _eul2rotm_zyx(math.radians(dz), math.radians(dy), math.radians(dx))
     noi = rand_noise * rng.random()
     n_out = int(round(rand_outliers * rng.random()))
     miss = rand_miss_rate * rng.random()
-    c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))
-    R = np.array([[c, -s], [s, c]])
-    t = (1 - 2 * rng.random(2)) * 0.5
-    model = np.asarray(model, dtype=np.float64)
+    t = (1 - 2 * rng.random(D)) * 0.5
     mean, radius = _radius(model)
-    mx = np.concatenate([model, rng.standard_normal((n_out, 2)) * radius + mean])
-    my = np.concatenate([model, rng.standard_normal((n_out, 2)) * radius + mean])
-    X, X_C = _noise_and_sampling2d(rng, mx, R, t, noi, miss, False)
-    Y, Y_C = _noise_and_sampling2d(rng, my, R, t, noi, miss, True)
-    return Problem(X, Y, X_C, Y_C, R.T.copy(), -R.T @ t, name or f"sim2d_{trial}")
+    mx = np.concatenate([model, rng.standard_normal((n_out, D)) * radius + mean])
+    my = np.concatenate([model, rng.standard_normal((n_out, D)) * radius + mean])
+    X, X_C = _noise_and_sampling(rng, mx, R, t, noi, miss, False)
+    Y, Y_C = _noise_and_sampling(rng, my, R, t, noi, miss, True)
+    return Problem(X, Y, X_C, Y_C, R.T.copy(), -R.T @ t, name or f"sim{D}d_{trial}")
