@@ -285,6 +285,28 @@ static int coef_call(Context& c, const double* R, const double* t, double sig, i
     return coef_from_moments(c.D, c.host + kHostMoments, coefficient);
 }
 
+// sigma at a pose without copies or memsets: the pose goes to the search prologue by value (it
+// also zeroes the error word), and the result with the error word behind it comes back through
+// the mapped pinned staging, or by copies when it is not mapped.  o = (exact, quantised) sigma.
+static int sigma_call(Context& c, const double* R, const double* t, double o[2])
+{
+    pack_pose(c, R, t, 1.0, c.host);
+    PoseBlock pb;
+    memcpy(pb.v, c.host, sizeof(pb.v));
+    SigmaOpts so;
+    so.pose_value = &pb;
+    so.reset_err = true;
+    so.host_out = c.host_dev ? c.host_dev + 64 : nullptr;
+    DUGMA_RET(launch_sigma(c, c.pose, c.out, c.stream, 0, -1, so));
+    if (!so.host_out) return fetch(c, c.out, 2, o);
+    DUGMA_CK(cudaStreamSynchronize(c.stream));
+    const double err = c.host[66];
+    if (err != 0.0) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", (int)err);
+    o[0] = c.host[64];
+    o[1] = c.host[65];
+    return DUGMA_OK;
+}
+
 static bool check_sizes(const Context& c, const double* N, const double* M, const double* D)
 {
     if (N && (int)*N != c.N) return false;
@@ -461,10 +483,8 @@ int dugma_update_sig(float* Ptr[6], const double* R, const double* t, const doub
     if (!R || !t || !sig) return set_error(DUGMA_ERR_ARG, "update_sig: null argument");
     GET_CTX(c, Ptr);
     if (!check_sizes(*c, N, M, D)) return set_error(DUGMA_ERR_ARG, "update_sig: N, M, D differ from init");
-    DUGMA_RET(upload_pose(*c, R, t, 1.0));
-    DUGMA_RET(launch_sigma(*c, c->pose, c->out, c->stream));
     double o[2];
-    DUGMA_RET(fetch(*c, c->out, 2, o));
+    DUGMA_RET(sigma_call(*c, R, t, o));
     sig[0] = (float)o[1];
     return DUGMA_OK;
 }
@@ -473,10 +493,8 @@ int dugma_sigma(float* Ptr[6], const double* R, const double* t, double* sig)
 {
     if (!R || !t || !sig) return set_error(DUGMA_ERR_ARG, "sigma: null argument");
     GET_CTX(c, Ptr);
-    DUGMA_RET(upload_pose(*c, R, t, 1.0));
-    DUGMA_RET(launch_sigma(*c, c->pose, c->out, c->stream));
     double o[2];
-    DUGMA_RET(fetch(*c, c->out, 2, o));
+    DUGMA_RET(sigma_call(*c, R, t, o));
     *sig = o[0];
     return DUGMA_OK;
 }
@@ -886,22 +904,31 @@ int dugma_graph_destroy(void* graph)
 
 namespace dugma {
 
-__global__ void pose_sig_from_sigma_kernel(double* pose, const double* sig_out)
-{
-    pose[kPoseSig] = sig_out[1];   // the quantised sigma, rounded to float as update_sig returns it
-}
-
+// One EM step on stream s: the pose block from the pinned staging (the search prologue reads it
+// there when the staging is mapped, else a copy brings it), sigma there (the search prologue
+// zeroes the error word; the sigma kernel puts the quantised sigma into the pose block), compi at
+// that pose and sigma.  Sigma, the moments and the error word come back through the mapped
+// staging (sigma at [64, 66), the error word behind the moments), or by copies when the staging
+// is not mapped (the error word then at [63] as an int).
 static int em_enqueue(Context& c, cudaStream_t s)
 {
-    DUGMA_CK(cudaMemcpyAsync(c.pose, c.host, sizeof(double) * kPoseDoubles, cudaMemcpyHostToDevice, s));
-    DUGMA_CK(cudaMemsetAsync(c.err, 0, sizeof(int), s));
-    DUGMA_RET(launch_sigma(c, c.pose, c.out, s));
-    pose_sig_from_sigma_kernel<<<1, 1, 0, s>>>(c.pose, c.out);
-    DUGMA_CK(cudaGetLastError());
-    DUGMA_RET(launch_coef(c, c.pose, c.mom, s));
-    DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * num_moments(c.D), cudaMemcpyDeviceToHost, s));
-    DUGMA_CK(cudaMemcpyAsync(c.host + 64, c.out, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
-    DUGMA_CK(cudaMemcpyAsync(c.host + 63, c.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (!c.host_dev)
+        DUGMA_CK(cudaMemcpyAsync(c.pose, c.host, sizeof(double) * kPoseDoubles, cudaMemcpyHostToDevice, s));
+    SigmaOpts so;
+    so.pose_src = c.host_dev;
+    so.reset_err = true;
+    so.pose_sig = c.pose;
+    so.host_out = c.host_dev ? c.host_dev + 64 : nullptr;
+    DUGMA_RET(launch_sigma(c, c.pose, c.out, s, 0, -1, so));
+    CoefOpts co;
+    co.host_moments = c.host_dev ? c.host_dev + kHostMoments : nullptr;
+    DUGMA_RET(launch_coef(c, c.pose, c.mom, s, 0, -1, 0, -1, co));
+    if (!c.host_dev) {
+        DUGMA_CK(cudaMemcpyAsync(c.host + kHostMoments, c.mom, sizeof(double) * num_moments(c.D),
+                                 cudaMemcpyDeviceToHost, s));
+        DUGMA_CK(cudaMemcpyAsync(c.host + 64, c.out, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+        DUGMA_CK(cudaMemcpyAsync(c.host + 63, c.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
     return DUGMA_OK;
 }
 
@@ -960,7 +987,10 @@ int dugma_em_step(void* graph, const double* R, const double* t, float sig[1], d
     DUGMA_CK(cudaGraphLaunch(g->exec, c->stream));
     DUGMA_CK(cudaStreamSynchronize(c->stream));
     int err = 0;
-    memcpy(&err, c->host + 63, sizeof(int));
+    if (c->host_dev)
+        err = (int)c->host[kHostMoments + num_moments(c->D)];
+    else
+        memcpy(&err, c->host + 63, sizeof(int));
     if (err) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", err);
     sig[0] = (float)c->host[65];
     return coef_from_moments(c->D, c->host + kHostMoments, coefficient);

@@ -59,10 +59,6 @@ __device__ __forceinline__ void write_pair_half(Rec256* __restrict__ out, int j,
 // Records: y side (v0 = y'hi, lv; v1 = y'lo; v2/v3 = k C'_j Horner-packed; g = monomials of y')
 //          x side (v0 = x, lw; v1 = 0;     v2/v3 = k B_i Horner-packed;  g = monomials of x)
 // ---------------------------------------------------------------------------
-struct PoseBlock {
-    double v[kPoseDoubles];
-};
-
 // One thread per point: indices [0, M_pad) are the targets, [M_pad, M_pad + N_pad) the sources.
 // The pose is pv when use_pv (block 0 then writes it to `pose` for the kernels that follow), else
 // read from `pose`.  reset_counter and reset_err (each optional) are zeroed for those kernels.

@@ -32,6 +32,11 @@ constexpr int kPadJ = 128;    // target rows padded to a multiple (largest j-til
 constexpr int kMomSlots = 512;   // doubles in Context::mom (moments; block partials during init)
 constexpr int kNumMomentsMax = 270;   // surrogate moments of the 3D coefficients (the 2D ones: 66)
 
+// A pose block handed to a kernel by value (no copy to the device before the launch).
+struct PoseBlock {
+    double v[kPoseDoubles];
+};
+
 struct KernelShape {
     int ipt = 0;      // source points per thread
     int nt = 0;       // threads per block
@@ -140,6 +145,12 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
                         cudaStream_t s, const float* w_stationary = nullptr, bool counter_zeroed = false);
+// Nearest-neighbour prologue: only the target records of the search (c.yp32), y' = R y + t as the
+// full prologue rounds it.  The pose is *pv when given, else read from pose_src (device-visible
+// memory) when given -- in both cases also written to pose_dev -- else read from pose_dev;
+// reset_counter / reset_err (optional) are zeroed for the kernels that follow.
+int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, const double* pose_src,
+                       int* reset_counter, int* reset_err);
 // Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy, 2 / 3 their paired
 // forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form; reset_counter
 // (optional) is zeroed for the pair kernel that follows.
@@ -152,12 +163,24 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
 // REF energy at the reference's FP64 per-pair precision (ref64.cu), sums to out_dev[0].
 int ref64_launch(Context& c, const double* pose_dev, int i0, int i1, double* out_dev, cudaStream_t s);
 // Nearest neighbours: writes idx/d2 (device) and optionally the per-point minimum only.
-int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
+int launch_nn(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
               const KernelShape* force = nullptr);
+// Options of a sigma evaluation, for a call that issues no copy or memset:
+struct SigmaOpts {
+    const PoseBlock* pose_value = nullptr;   // the pose by value to the first kernel (which also writes
+                                             // it to pose_dev), instead of read from pose_dev
+    const double* pose_src = nullptr;        // else the pose from device-visible memory (the mapped
+                                             // staging a captured graph reads at each launch)
+    bool reset_err = false;                  // the first kernel zeroes the device error word
+    double* host_out = nullptr;              // mapped pinned memory that also receives out_dev[0..1] and,
+                                             // at [2], the error word
+    double* pose_sig = nullptr;              // a device pose block whose sig receives out_dev[1]
+};
 // sigma: out_dev[0] = exact FP64 sigma, out_dev[1] = quantised (reference) sigma.  For a source
 // row range [i0, i1) (i1 >= 0) the partial sums instead: out_dev[0] = sum of the nearest squared
 // distances, out_dev[1] = sum of the reference's quantised terms (an integer below 2^53).
-int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s, int i0 = 0, int i1 = -1);
+int launch_sigma(Context& c, double* pose_dev, double* out_dev, cudaStream_t s, int i0 = 0, int i1 = -1,
+                 const SigmaOpts& opts = SigmaOpts());
 // Surrogate coefficient moments: out_dev receives kNumMoments doubles.
 // Source rows [i0, i1) carry the source-side (B) terms, target rows [j0, j1) the target-side
 // (C') terms; -1 for i1 / j1 means all rows.  Sums over partitions of both add up to the whole.

@@ -236,8 +236,11 @@ __global__ void sigma_partial_kernel(const float* __restrict__ dmin, int n, int 
     }
 }
 
+// host_out (optional, mapped pinned memory) receives out[0..1] and the error word at [2];
+// pose_sig (optional) a device pose block whose sig becomes out[1]
 __global__ void sigma_final_kernel(const double* __restrict__ pe, const unsigned long long* __restrict__ pq, int nb,
-                                   int n, int D, double* __restrict__ out)
+                                   int n, int D, double* __restrict__ out, double* __restrict__ host_out,
+                                   const int* __restrict__ err, double* __restrict__ pose_sig)
 {
     __shared__ double s_exact[256];
     __shared__ unsigned long long s_q[256];
@@ -258,12 +261,21 @@ __global__ void sigma_final_kernel(const double* __restrict__ pe, const unsigned
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        double o0, o1;
         if (n > 0) {
-            out[0] = s_exact[0] / ((double)D * n);
-            out[1] = (double)__double2float_rn((double)s_q[0] / 1e6 / (double)n);
+            o0 = s_exact[0] / ((double)D * n);
+            o1 = (double)__double2float_rn((double)s_q[0] / 1e6 / (double)n);
         } else {   // the partial sums of a row range: sum d2min, and the sum of the quantised terms
-            out[0] = s_exact[0];
-            out[1] = (double)s_q[0];
+            o0 = s_exact[0];
+            o1 = (double)s_q[0];
+        }
+        out[0] = o0;
+        out[1] = o1;
+        if (pose_sig) pose_sig[kPoseSig] = o1;   // the quantised sigma, rounded to float as update_sig returns it
+        if (host_out) {
+            host_out[0] = o0;
+            host_out[1] = o1;
+            host_out[2] = (double)*err;
         }
     }
 }
@@ -309,12 +321,16 @@ std::vector<KernelShape> nn_shapes()
 
 // Runs the brute-force search; dmin_dev (nullable) receives the nearest squared distance per source.
 // Source rows [i0, i1) (i1 < 0: all); idx/d2 rows are relative to i0, dmin is indexed absolutely.
-static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, float* dmin_dev,
-                  cudaStream_t s, const KernelShape* force, int i0 = 0, int i1 = -1)
+// The search: the targets' search records (the nearest-neighbour prologue, which also zeroes the
+// work counter, and the error word when reset_err; the pose by value when pv, or read from
+// pose_src), the pair kernel, the merge of its per-chunk lists.
+static int nn_run(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_dev, float* dmin_dev,
+                  cudaStream_t s, const KernelShape* force, int i0 = 0, int i1 = -1, const PoseBlock* pv = nullptr,
+                  const double* pose_src = nullptr, bool reset_err = false)
 {
     if (i1 < 0) i1 = c.N;
     const int rows = i1 - i0;
-    DUGMA_RET(launch_prologue(c, pose_dev, 0, s));
+    DUGMA_RET(launch_nn_prologue(c, pose_dev, s, pv, pose_src, c.counter, reset_err ? c.err : nullptr));
     const KernelShape want = force ? *force : c.shape_nn;
     const auto& vars = c.D == 3 ? nn_variants<3>() : nn_variants<2>();
     const NNVariant* v = &vars[0];
@@ -339,7 +355,7 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     double* hp = nullptr;
     int n_jc = 0;
     DUGMA_RET(launch_pair_variant(c, fn, sh, c.x, c.yp32, (size_t)c.M_pad / 2, 1, 0.0, pose_dev, i0, i1, nullptr,
-                                  nullptr, &hp, K, &n_jc, s));
+                                  nullptr, &hp, K, &n_jc, s, nullptr, true));
     const int g = std::min((rows + 255) / 256, c.num_sms * 8);
     const float2* part = reinterpret_cast<const float2*>(hp);
     float* dm = dmin_dev ? dmin_dev + i0 : nullptr;
@@ -353,26 +369,27 @@ static int nn_run(Context& c, const double* pose_dev, int k, int* idx_dev, float
     return DUGMA_OK;
 }
 
-int launch_nn(Context& c, const double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
+int launch_nn(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_dev, cudaStream_t s,
               const KernelShape* force)
 {
     if (k < 1 || k > 16 || k > c.M) return set_error(DUGMA_ERR_ARG, "k = %d must be in [1, min(16, M)]", k);
     return nn_run(c, pose_dev, k, idx_dev, d2_dev, nullptr, s, force);
 }
 
-int launch_sigma(Context& c, const double* pose_dev, double* out_dev, cudaStream_t s, int i0, int i1)
+int launch_sigma(Context& c, double* pose_dev, double* out_dev, cudaStream_t s, int i0, int i1, const SigmaOpts& o)
 {
     const bool whole = i1 < 0;
     if (whole) i1 = c.N;
     const int rows = i1 - i0;
-    DUGMA_RET(nn_run(c, pose_dev, 1, nullptr, nullptr, c.dmin, s, nullptr, i0, i1));
+    DUGMA_RET(nn_run(c, pose_dev, 1, nullptr, nullptr, c.dmin, s, nullptr, i0, i1, o.pose_value, o.pose_src,
+                     o.reset_err));
     // partials in the scratch region (the search's chunk lists there are merged by now, in stream order)
     const int nb = std::max(1, std::min(2 * c.num_sms, (rows + 1023) / 1024));
     DUGMA_RET(c.ensure_scratch(sizeof(double) * 2 * (size_t)nb));
     double* pe = c.scratch;
     unsigned long long* pq = reinterpret_cast<unsigned long long*>(c.scratch + nb);
     sigma_partial_kernel<<<nb, 256, 0, s>>>(c.dmin + i0, rows, c.D, pe, pq);
-    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, whole ? c.N : 0, c.D, out_dev);
+    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, whole ? c.N : 0, c.D, out_dev, o.host_out, c.err, o.pose_sig);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }

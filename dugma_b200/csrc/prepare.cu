@@ -398,6 +398,74 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
     }
 }
 
+// the search records of target j (the yp32 layout of prologue_kernel): two targets per 32 bytes,
+// coordinates negated, padding targets at +inf
+// The pose: pv (use_pv), else pose_src (device-visible memory, e.g. the mapped pinned staging a
+// captured graph reads at each launch), else pose itself; block 0 writes it to pose in the first
+// two cases.
+template <int D>
+__global__ void nn_prologue_kernel(const PoseBlock pv, int use_pv, const double* __restrict__ pose_src,
+                                   double* __restrict__ pose, const float* __restrict__ y, int M, int M_pad,
+                                   float4* __restrict__ yp32, int* __restrict__ reset_counter,
+                                   int* __restrict__ reset_err)
+{
+    __shared__ double sp[kPoseDoubles];
+    if (threadIdx.x == 0) {
+        const double* src = pose_src ? pose_src : pose;
+#pragma unroll
+        for (int k = 0; k < kPoseDoubles; ++k) sp[k] = use_pv ? pv.v[k] : src[k];
+        if (blockIdx.x == 0) {
+            if (reset_counter) *reset_counter = 0;
+            if (reset_err) *reset_err = 0;
+            if (use_pv || pose_src)
+#pragma unroll
+                for (int k = 0; k < kPoseDoubles; ++k) pose[k] = sp[k];
+        }
+    }
+    __syncthreads();
+    double R[9], t[3];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) R[k] = sp[k];
+#pragma unroll
+    for (int a = 0; a < D; ++a) t[a] = sp[kPoseT + a];
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
+        float hi[3] = {0, 0, 0};
+        if (j < M) {
+            double yj[3];
+#pragma unroll
+            for (int a = 0; a < D; ++a) yj[a] = (double)y[(size_t)j * D + a];
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                double v = R[a] * yj[0] + R[a + D] * yj[1];
+                if (D == 3) v = v + R[a + 6] * yj[2];
+                v = v + t[a];
+                hi[a] = __double2float_rn(v);
+            }
+        }
+        float* pr = reinterpret_cast<float*>(yp32 + 2 * (j / 2));
+        const int h = j & 1;
+        for (int q = 0; q < 3; ++q) pr[2 * q + h] = j < M ? (q < D ? -hi[q] : 0.f) : -INFINITY;
+        pr[6 + h] = 0.f;
+    }
+}
+
+int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, const double* pose_src,
+                       int* reset_counter, int* reset_err)
+{
+    PoseBlock pb{};
+    if (pv) pb = *pv;
+    const int g = std::min((c.M_pad + 127) / 128, c.num_sms * 8);
+    if (c.D == 3)
+        nn_prologue_kernel<3><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_src, pose_dev, c.y, c.M, c.M_pad, c.yp32,
+                                                reset_counter, reset_err);
+    else
+        nn_prologue_kernel<2><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_src, pose_dev, c.y, c.M, c.M_pad, c.yp32,
+                                                reset_counter, reset_err);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
 int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol, int* reset_counter)
 {
     if (xchol && (!c.ux || c.x_indef > 0))
@@ -407,10 +475,10 @@ int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_
     const int bs = 128;
     const int g = std::min((n + bs - 1) / bs, c.num_sms * 8);
     if (c.D == 3)
-        prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
+        prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, nullptr,
                                             c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
     else
-        prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, c.yp32,
+        prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, nullptr,
                                             c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
