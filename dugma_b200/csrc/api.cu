@@ -285,6 +285,29 @@ static int coef_call(Context& c, const double* R, const double* t, double sig, i
     return coef_from_moments(c.D, c.host + kHostMoments, coefficient);
 }
 
+// The REF model's evaluation options that need no copy or memset (EvalIO), when the pinned
+// staging is mapped: the pose by value (pv given: a single call) or loaded from host[0, 16) at
+// each launch (a captured graph), the nv results and the error word to host[64, ...).
+static bool mapped_io(const Context& c, int model, const PoseBlock* pv, EvalIO* io)
+{
+    if (!c.host_dev || model != DUGMA_MODEL_REF) return false;
+    io->pv = pv;
+    io->pose_src = pv ? nullptr : c.host_dev;
+    io->pose_out = c.pose;
+    io->host_out = c.host_dev + 64;
+    return true;
+}
+
+// after a launch with mapped_io: the nv results once the stream is done, the error word checked
+static int mapped_fetch(Context& c, int nv, double* dst)
+{
+    DUGMA_CK(cudaStreamSynchronize(c.stream));
+    const double err = c.host[64 + nv];
+    if (err != 0.0) return set_error(DUGMA_ERR_TIMEOUT, "a device wait gave up (error word 0x%x)", (int)err);
+    memcpy(dst, c.host + 64, sizeof(double) * nv);
+    return DUGMA_OK;
+}
+
 // sigma at a pose without copies or memsets: the pose goes to the search prologue by value (it
 // also zeroes the error word), and the result with the error word behind it comes back through
 // the mapped pinned staging, or by copies when it is not mapped.  o = (exact, quantised) sigma.
@@ -541,6 +564,13 @@ int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, in
     if (!R || !t || !E) return set_error(DUGMA_ERR_ARG, "energy: null argument");
     if (!(sig > 0)) return set_error(DUGMA_ERR_ARG, "energy: sig must be positive");
     GET_CTX(c, Ptr);
+    EvalIO io;
+    PoseBlock pb;
+    if (mapped_io(*c, model, &pb, &io)) {
+        pack_pose(*c, R, t, sig, pb.v);
+        DUGMA_RET(launch_pairs(*c, c->pose, model, false, 0, c->N, c->out, nullptr, c->stream, nullptr, &io));
+        return mapped_fetch(*c, 1, E);
+    }
     DUGMA_RET(upload_pose(*c, R, t, sig));
     DUGMA_RET(launch_pairs(*c, c->pose, model, false, 0, c->N, c->out, nullptr, c->stream));
     return fetch(*c, c->out, 1, E);
@@ -549,15 +579,23 @@ int dugma_energy(float* Ptr[6], const double* R, const double* t, double sig, in
 static int energy_grad_impl(Context* c, const double* R, const double* t, double sig, int model, int i0, int i1,
                             double* E, double* g, double* dEdx)
 {
-    DUGMA_RET(upload_pose(*c, R, t, sig));
-    if (dEdx && !c->dedx) DUGMA_CK(cudaMalloc(&c->dedx, sizeof(double) * (size_t)c->N * c->D));
-    DUGMA_RET(launch_pairs(*c, c->pose, model, true, i0, i1, c->out, dEdx ? c->dedx : nullptr, c->stream));
-    if (dEdx)
-        DUGMA_CK(cudaMemcpyAsync(dEdx, c->dedx, sizeof(double) * (size_t)(i1 - i0) * c->D, cudaMemcpyDeviceToHost,
-                                 c->stream));
     const int ng = ng_of(c->D);
     double o[8];
-    DUGMA_RET(fetch(*c, c->out, 1 + ng, o));
+    EvalIO io;
+    PoseBlock pb;
+    if (!dEdx && mapped_io(*c, model, &pb, &io)) {
+        pack_pose(*c, R, t, sig, pb.v);
+        DUGMA_RET(launch_pairs(*c, c->pose, model, true, i0, i1, c->out, nullptr, c->stream, nullptr, &io));
+        DUGMA_RET(mapped_fetch(*c, 1 + ng, o));
+    } else {
+        DUGMA_RET(upload_pose(*c, R, t, sig));
+        if (dEdx && !c->dedx) DUGMA_CK(cudaMalloc(&c->dedx, sizeof(double) * (size_t)c->N * c->D));
+        DUGMA_RET(launch_pairs(*c, c->pose, model, true, i0, i1, c->out, dEdx ? c->dedx : nullptr, c->stream));
+        if (dEdx)
+            DUGMA_CK(cudaMemcpyAsync(dEdx, c->dedx, sizeof(double) * (size_t)(i1 - i0) * c->D, cudaMemcpyDeviceToHost,
+                                     c->stream));
+        DUGMA_RET(fetch(*c, c->out, 1 + ng, o));
+    }
     if (E) *E = o[0];
     if (g) memcpy(g, o + 1, sizeof(double) * ng);
     if (!std::isfinite(o[0])) return set_error(DUGMA_ERR_NUMERIC, "energy is not finite");
@@ -828,6 +866,7 @@ struct Graph {
     Context* c = nullptr;
     float* ptr[6];
     int model = 0;
+    bool mapped = false;   // the graph reads its pose from and writes its results to the mapped staging
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -849,8 +888,14 @@ int dugma_graph_create(float* Ptr[6], int model, void** out)
     g->c = c;
     for (int k = 0; k < 6; ++k) g->ptr[k] = Ptr[k];
     g->model = model;
+    // REF model with mapped staging: the captured prologue reads the pose the host packs before each
+    // launch, and the reduction writes the results back there (no copy or memset in the graph or
+    // around it)
+    EvalIO io;
+    g->mapped = mapped_io(*c, model, nullptr, &io);
     DUGMA_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_pairs(*c, c->pose, model, true, 0, c->N, c->out, nullptr, c->stream);
+    int rc = launch_pairs(*c, c->pose, model, true, 0, c->N, c->out, nullptr, c->stream, nullptr,
+                          g->mapped ? &io : nullptr);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc != DUGMA_OK || e != cudaSuccess) {
@@ -875,11 +920,17 @@ int dugma_graph_eval(void* graph, const double* R, const double* t, double sig, 
     Context* c = find_context(g->ptr);
     if (c != g->c) return set_error(DUGMA_ERR_STATE, "graph_eval: the context of this graph was freed");
     std::lock_guard<std::mutex> lk(c->mu);
-    DUGMA_RET(upload_pose(*c, R, t, sig));
-    DUGMA_CK(cudaGraphLaunch(g->exec, c->stream));
     const int ng = ng_of(c->D);
     double o[8];
-    DUGMA_RET(fetch(*c, c->out, 1 + ng, o));
+    if (g->mapped) {
+        pack_pose(*c, R, t, sig, c->host);
+        DUGMA_CK(cudaGraphLaunch(g->exec, c->stream));
+        DUGMA_RET(mapped_fetch(*c, 1 + ng, o));
+    } else {
+        DUGMA_RET(upload_pose(*c, R, t, sig));
+        DUGMA_CK(cudaGraphLaunch(g->exec, c->stream));
+        DUGMA_RET(fetch(*c, c->out, 1 + ng, o));
+    }
     *E = o[0];
     memcpy(gout, o + 1, sizeof(double) * ng);
     return DUGMA_OK;

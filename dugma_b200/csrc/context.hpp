@@ -140,26 +140,46 @@ using KernelFn = void (*)(PairArgs);
 // dEdx_dev, the per-row sums over target chunks.  h_part (nullable) receives the per-chunk
 // row buffer of h_width doubles per row, n_jc_out the chunk count.  The stationary side's
 // weights are c.wx unless w_stationary is given (the coefficient pass over targets).
-// counter_zeroed: a kernel before it on the stream zeroed c.counter (no memset issued).
+// counter_zeroed: a kernel before it on the stream zeroed c.counter (no memset issued); host_out
+// (optional, mapped pinned memory): also receives out_dev's nv values and, behind them, the
+// error word.
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s, const float* w_stationary = nullptr, bool counter_zeroed = false);
+                        cudaStream_t s, const float* w_stationary = nullptr, bool counter_zeroed = false,
+                        double* host_out = nullptr);
 // Nearest-neighbour prologue: only the target records of the search (c.yp32), y' = R y + t as the
-// full prologue rounds it.  The pose is *pv when given, else read from pose_src (device-visible
-// memory) when given -- in both cases also written to pose_dev -- else read from pose_dev;
-// reset_counter / reset_err (optional) are zeroed for the kernels that follow.
-int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, const double* pose_src,
-                       int* reset_counter, int* reset_err);
+// full prologue rounds it.  The pose is *pv when given (then also written to pose_dev), else read
+// from pose_dev; reset_counter / reset_err (optional) are zeroed for the kernels that follow.
+int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, int* reset_counter,
+                       int* reset_err);
+// One small kernel: the pose block from src (device-visible memory, e.g. the mapped pinned staging
+// a captured graph reads at each launch) into pose_dev, and the error word zeroed if reset_err.
+int launch_pose_in(Context& c, const double* src, double* pose_dev, cudaStream_t s, bool reset_err);
 // Per-evaluation prologue: y records (layout 0 = adjoint, 1 = Horner energy, 2 / 3 their paired
-// forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form; reset_counter
-// (optional) is zeroed for the pair kernel that follows.
+// forms), x records in the Cholesky form (xchol, from c.ux) or the Horner form; reset_counter and
+// reset_err (optional) are zeroed for the kernels that follow; the pose is *pv when given (and then
+// also written to pose_out, if given), else read from pose_dev.
 int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol = false,
-                    int* reset_counter = nullptr);
+                    int* reset_counter = nullptr, const PoseBlock* pv = nullptr, double* pose_out = nullptr,
+                    int* reset_err = nullptr);
 // Pairwise energy (grad = false) or fused adjoint (grad = true) over source rows [i0, i1);
 // writes {E, g} to out_dev and, if dEdx_dev, dE/dx for rows [i0, i1) (relative index).
+// Options of an evaluation that issues no copy or memset (REF model).  The pose: *pv by value to the
+// prologue (a single call), or loaded from pose_src (device-visible memory: the mapped pinned
+// staging a captured graph reads at each launch) by a one-block kernel first; either way it is
+// written to pose_out (the device pose block the pair kernel reads) and the error word is zeroed.
+// The results (nv values) and, behind them, the error word are written to host_out (mapped pinned
+// memory) as well.
+struct EvalIO {
+    const PoseBlock* pv = nullptr;
+    const double* pose_src = nullptr;
+    double* pose_out = nullptr;
+    double* host_out = nullptr;
+};
 int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1,
-                 double* out_dev, double* dEdx_dev, cudaStream_t s, const KernelShape* force = nullptr);
+                 double* out_dev, double* dEdx_dev, cudaStream_t s, const KernelShape* force = nullptr,
+                 const EvalIO* io = nullptr);
 // REF energy at the reference's FP64 per-pair precision (ref64.cu), sums to out_dev[0].
 int ref64_launch(Context& c, const double* pose_dev, int i0, int i1, double* out_dev, cudaStream_t s);
 // Nearest neighbours: writes idx/d2 (device) and optionally the per-point minimum only.
@@ -169,8 +189,9 @@ int launch_nn(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_dev, 
 struct SigmaOpts {
     const PoseBlock* pose_value = nullptr;   // the pose by value to the first kernel (which also writes
                                              // it to pose_dev), instead of read from pose_dev
-    const double* pose_src = nullptr;        // else the pose from device-visible memory (the mapped
-                                             // staging a captured graph reads at each launch)
+    const double* pose_src = nullptr;        // else the pose loaded into pose_dev first from
+                                             // device-visible memory (the mapped staging a captured
+                                             // graph reads at each launch)
     bool reset_err = false;                  // the first kernel zeroes the device error word
     double* host_out = nullptr;              // mapped pinned memory that also receives out_dev[0..1] and,
                                              // at [2], the error word

@@ -41,8 +41,10 @@ __global__ void __launch_bounds__(NT, MINB) pair_kernel_occ(PairArgs a)
 
 // deterministic reduction of per-item partials: out[v] = sum_items partials[item][v];
 // block v sums value v in a fixed order (strided per thread, then a fixed tree)
+// host_out (optional, mapped pinned memory) receives out[0..nv) and the error word at [nv]
 __global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __restrict__ part, int n_items, int nv,
-                                                             double* __restrict__ out)
+                                                             double* __restrict__ out, double* __restrict__ host_out,
+                                                             const int* __restrict__ err)
 {
     __shared__ double red[1024];
     const int v = blockIdx.x;
@@ -55,7 +57,13 @@ __global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __rest
         if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[v] = red[0];
+    if (threadIdx.x == 0) {
+        out[v] = red[0];
+        if (host_out) {
+            host_out[v] = red[0];
+            if (v == 0) host_out[nv] = (double)*err;
+        }
+    }
 }
 
 __global__ void reduce_chunks_kernel(const double* __restrict__ part, int n_jc, size_t n, double* __restrict__ out)
@@ -160,7 +168,7 @@ static int occupancy_blocks(KernelFn fn, int nt)
 int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const void* xrec, const void* yrec,
                         size_t yrec_size, int nv, double Lmax, const double* pose_dev, int i0, int i1,
                         double* out_dev, double* dEdx_dev, double** h_part, int h_width, int* n_jc_out,
-                        cudaStream_t s, const float* w_stationary, bool counter_zeroed)
+                        cudaStream_t s, const float* w_stationary, bool counter_zeroed, double* host_out)
 {
     const int rows = i1 - i0;
     const int BI = sh.ipt * sh.nt;
@@ -226,7 +234,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
     DUGMA_CK(cudaGetLastError());
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
     if (out_dev) {
-        reduce_items_kernel<<<nv, 1024, 0, s>>>(a.partials, n_items, nv, out_dev);
+        reduce_items_kernel<<<nv, 1024, 0, s>>>(a.partials, n_items, nv, out_dev, host_out, c.err);
         DUGMA_CK(cudaGetLastError());
     }
     if (dEdx_dev) {
@@ -239,7 +247,7 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
 }
 
 int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i0, int i1, double* out_dev,
-                 double* dEdx_dev, cudaStream_t s, const KernelShape* force)
+                 double* dEdx_dev, cudaStream_t s, const KernelShape* force, const EvalIO* io)
 {
     if (i0 < 0 || i1 > c.N || i0 >= i1) return set_error(DUGMA_ERR_ARG, "bad source row range [%d, %d)", i0, i1);
     if (model == DUGMA_MODEL_CONV) return conv_launch(c, pose_dev, grad, i0, i1, out_dev, dEdx_dev, s, force);
@@ -266,11 +274,17 @@ int launch_pairs(Context& c, const double* pose_dev, int model, bool grad, int i
     }
     // record layout: 0 scalar adjoint, 1 scalar Horner energy, 2 / 3 their packed-pair forms
     const int layout = (grad ? 0 : 1) + (v->shape.pack == 2 ? 2 : 0);
-    DUGMA_RET(launch_prologue(c, pose_dev, layout, s, xchol, c.counter));
+    if (io && (io->pv || io->pose_src) && !io->pose_out)
+        return set_error(DUGMA_ERR_ARG, "a pose by value or from host memory needs a device pose block");
+    if (io && io->pose_src) DUGMA_RET(launch_pose_in(c, io->pose_src, io->pose_out, s, true));
+    const double* pose_read = io && io->pose_src ? io->pose_out : pose_dev;
+    DUGMA_RET(launch_prologue(c, pose_read, layout, s, xchol, c.counter, io ? io->pv : nullptr,
+                              io ? io->pose_out : nullptr, io && io->pv ? c.err : nullptr));
     const int nv = grad ? 1 + (c.D == 3 ? 6 : 3) : 1;
     return launch_pair_variant(c, v->fn, v->shape, c.xrec, c.yrec, (size_t)c.M_pad / v->shape.pack, nv, c.Lmax_y,
-                               pose_dev, i0, i1, out_dev, grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s, nullptr,
-                               true);
+                               io && io->pose_out ? io->pose_out : pose_dev, i0, i1, out_dev,
+                               grad ? dEdx_dev : nullptr, nullptr, 0, nullptr, s, nullptr, true,
+                               io ? io->host_out : nullptr);
 }
 
 // ---------------------------------------------------------------------------

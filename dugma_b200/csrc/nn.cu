@@ -330,7 +330,11 @@ static int nn_run(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_d
 {
     if (i1 < 0) i1 = c.N;
     const int rows = i1 - i0;
-    DUGMA_RET(launch_nn_prologue(c, pose_dev, s, pv, pose_src, c.counter, reset_err ? c.err : nullptr));
+    if (pose_src) {
+        DUGMA_RET(launch_pose_in(c, pose_src, pose_dev, s, reset_err));
+        reset_err = false;
+    }
+    DUGMA_RET(launch_nn_prologue(c, pose_dev, s, pv, c.counter, reset_err ? c.err : nullptr));
     const KernelShape want = force ? *force : c.shape_nn;
     const auto& vars = c.D == 3 ? nn_variants<3>() : nn_variants<2>();
     const NNVariant* v = &vars[0];

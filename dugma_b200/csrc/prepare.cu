@@ -292,16 +292,25 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
                                 int ylayout, YRec* __restrict__ yrec, float4* __restrict__ yp32,
                                 const float* __restrict__ x, const float* __restrict__ xinv,
                                 const float* __restrict__ lwx, int N, int N_pad, XRec* __restrict__ xrec,
-                                const double* __restrict__ ux, int* __restrict__ reset_counter)
+                                const double* __restrict__ ux, int* __restrict__ reset_counter, const PoseBlock pv,
+                                int use_pv, double* __restrict__ pose_out, int* __restrict__ reset_err)
 {
     constexpr int NS = Sym<D>::N;
-    if (reset_counter && blockIdx.x == 0 && threadIdx.x == 0) *reset_counter = 0;
+    // the pose pv by value (use_pv; block 0 also writes it to pose_out, if given, for the kernels
+    // that follow) or from pose
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (reset_counter) *reset_counter = 0;
+        if (reset_err) *reset_err = 0;
+        if (use_pv && pose_out)
+#pragma unroll
+            for (int k = 0; k < kPoseDoubles; ++k) pose_out[k] = pv.v[k];
+    }
     double R[9], t[3];
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) R[k] = pose[k];
+    for (int k = 0; k < D * D; ++k) R[k] = use_pv ? pv.v[k] : pose[k];
 #pragma unroll
-    for (int a = 0; a < D; ++a) t[a] = pose[kPoseT + a];
-    const double s = 1.0 / pose[kPoseSig];
+    for (int a = 0; a < D; ++a) t[a] = use_pv ? pv.v[kPoseT + a] : pose[kPoseT + a];
+    const double s = 1.0 / (use_pv ? pv.v[kPoseSig] : pose[kPoseSig]);
     const double ks = K_EXP2 * s;
     const int stride = gridDim.x * blockDim.x;
     // one thread per point: [0, M_pad) the targets, [M_pad, M_pad + N_pad) the sources
@@ -400,34 +409,24 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
 
 // the search records of target j (the yp32 layout of prologue_kernel): two targets per 32 bytes,
 // coordinates negated, padding targets at +inf
-// The pose: pv (use_pv), else pose_src (device-visible memory, e.g. the mapped pinned staging a
-// captured graph reads at each launch), else pose itself; block 0 writes it to pose in the first
-// two cases.
+// The pose: pv by value (use_pv; block 0 also writes it to pose), else read from pose.
 template <int D>
-__global__ void nn_prologue_kernel(const PoseBlock pv, int use_pv, const double* __restrict__ pose_src,
-                                   double* __restrict__ pose, const float* __restrict__ y, int M, int M_pad,
-                                   float4* __restrict__ yp32, int* __restrict__ reset_counter,
-                                   int* __restrict__ reset_err)
+__global__ void nn_prologue_kernel(const PoseBlock pv, int use_pv, double* __restrict__ pose,
+                                   const float* __restrict__ y, int M, int M_pad, float4* __restrict__ yp32,
+                                   int* __restrict__ reset_counter, int* __restrict__ reset_err)
 {
-    __shared__ double sp[kPoseDoubles];
-    if (threadIdx.x == 0) {
-        const double* src = pose_src ? pose_src : pose;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (reset_counter) *reset_counter = 0;
+        if (reset_err) *reset_err = 0;
+        if (use_pv)
 #pragma unroll
-        for (int k = 0; k < kPoseDoubles; ++k) sp[k] = use_pv ? pv.v[k] : src[k];
-        if (blockIdx.x == 0) {
-            if (reset_counter) *reset_counter = 0;
-            if (reset_err) *reset_err = 0;
-            if (use_pv || pose_src)
-#pragma unroll
-                for (int k = 0; k < kPoseDoubles; ++k) pose[k] = sp[k];
-        }
+            for (int k = 0; k < kPoseDoubles; ++k) pose[k] = pv.v[k];
     }
-    __syncthreads();
     double R[9], t[3];
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) R[k] = sp[k];
+    for (int k = 0; k < D * D; ++k) R[k] = use_pv ? pv.v[k] : pose[k];
 #pragma unroll
-    for (int a = 0; a < D; ++a) t[a] = sp[kPoseT + a];
+    for (int a = 0; a < D; ++a) t[a] = use_pv ? pv.v[kPoseT + a] : pose[kPoseT + a];
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M_pad; j += stride) {
         float hi[3] = {0, 0, 0};
@@ -450,24 +449,43 @@ __global__ void nn_prologue_kernel(const PoseBlock pv, int use_pv, const double*
     }
 }
 
-int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, const double* pose_src,
-                       int* reset_counter, int* reset_err)
+// One block: the pose block from src (device-visible memory: the mapped pinned staging a captured
+// graph reads at each launch) into pose, the error word zeroed.  The kernels that follow read the
+// pose from device memory (every block reading the staging over the host link costs more).
+__global__ void pose_in_kernel(const double* __restrict__ src, double* __restrict__ pose, int* __restrict__ err)
+{
+    if (threadIdx.x < kPoseDoubles) pose[threadIdx.x] = src[threadIdx.x];
+    if (threadIdx.x == 0 && err) *err = 0;
+}
+
+int launch_pose_in(Context& c, const double* src, double* pose_dev, cudaStream_t s, bool reset_err)
+{
+    pose_in_kernel<<<1, 32, 0, s>>>(src, pose_dev, reset_err ? c.err : nullptr);
+    DUGMA_CK(cudaGetLastError());
+    return DUGMA_OK;
+}
+
+int launch_nn_prologue(Context& c, double* pose_dev, cudaStream_t s, const PoseBlock* pv, int* reset_counter,
+                       int* reset_err)
 {
     PoseBlock pb{};
     if (pv) pb = *pv;
     const int g = std::min((c.M_pad + 127) / 128, c.num_sms * 8);
     if (c.D == 3)
-        nn_prologue_kernel<3><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_src, pose_dev, c.y, c.M, c.M_pad, c.yp32,
-                                                reset_counter, reset_err);
+        nn_prologue_kernel<3><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_dev, c.y, c.M, c.M_pad, c.yp32, reset_counter,
+                                                reset_err);
     else
-        nn_prologue_kernel<2><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_src, pose_dev, c.y, c.M, c.M_pad, c.yp32,
-                                                reset_counter, reset_err);
+        nn_prologue_kernel<2><<<g, 128, 0, s>>>(pb, pv ? 1 : 0, pose_dev, c.y, c.M, c.M_pad, c.yp32, reset_counter,
+                                                reset_err);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
 
-int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol, int* reset_counter)
+int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_t s, bool xchol, int* reset_counter,
+                    const PoseBlock* pv, double* pose_out, int* reset_err)
 {
+    PoseBlock pb{};
+    if (pv) pb = *pv;
     if (xchol && (!c.ux || c.x_indef > 0))
         return set_error(DUGMA_ERR_STATE, "Cholesky-form source records need a positive definite factor per source");
     const double* ux = xchol ? c.ux : nullptr;
@@ -476,10 +494,12 @@ int launch_prologue(Context& c, const double* pose_dev, int ylayout, cudaStream_
     const int g = std::min((n + bs - 1) / bs, c.num_sms * 8);
     if (c.D == 3)
         prologue_kernel<3><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, nullptr,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter, pb,
+                                            pv ? 1 : 0, pose_out, reset_err);
     else
         prologue_kernel<2><<<g, bs, 0, s>>>(pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, ylayout, c.yrec, nullptr,
-                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter);
+                                            c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec, ux, reset_counter, pb,
+                                            pv ? 1 : 0, pose_out, reset_err);
     DUGMA_CK(cudaGetLastError());
     return DUGMA_OK;
 }
