@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -467,8 +468,12 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     c->scratch_bytes = c->arena_scratch_bytes = scratch_bytes;
     c->host = pinned_acquire();
     if (!c->host) return fail(set_error(DUGMA_ERR_NOMEM, "init: pinned staging allocation failed"));
-    if (cudaHostGetDevicePointer((void**)&c->host_dev, c->host, 0) != cudaSuccess) {
-        c->host_dev = nullptr;   // not mapped: results come back by copies
+    // the staging as the device addresses it; without it (not mapped, or DUGMA_NO_MAPPED_STAGING set
+    // in the environment) poses and results travel by copies
+    const char* no_map = getenv("DUGMA_NO_MAPPED_STAGING");
+    if ((no_map && *no_map && *no_map != '0') ||
+        cudaHostGetDevicePointer((void**)&c->host_dev, c->host, 0) != cudaSuccess) {
+        c->host_dev = nullptr;
         cudaGetLastError();
     }
     if (cudaMemsetAsync(c->err, 0, sizeof(int) * 4, c->stream) != cudaSuccess)
