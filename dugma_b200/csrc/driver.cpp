@@ -109,8 +109,7 @@ const std::vector<Mono>& mono_table(int D)
     return D == 3 ? t3 : t2;
 }
 
-// Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq and its gradient in v (product rule over the
-// factor list: a factor repeated e times contributes e v^(e-1) times the rest).
+// Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq, its gradient and Hessian in v.
 struct Surrogate {
     int D, K, nv;
     const double* A;
@@ -126,44 +125,67 @@ struct Surrogate {
         }
         return s;
     }
-    void grad(const double* v, double* g) const
+    // Gradient and Hessian in v (nv x nv, row-major) in one pass: for a monomial A x_0 .. x_{n-1}
+    // (its factor list; a variable of exponent e appears e times) the gradient gets the product
+    // of the other factors at each factor's variable, and every unordered pair of factor
+    // positions gets the product of the remaining factors at both off-diagonal entries (a
+    // repeated variable so collects e (e - 1) v^(e - 2) on the diagonal).  Written out per
+    // factor count (1..4) so that each product is formed once.
+    void grad_hess(const double* v, double* g, double* H) const
     {
         const std::vector<Mono>& T = mono_table(D);
         for (int q = 0; q < nv; ++q) g[q] = 0;
-        for (int k = 0; k < K; ++k) {
-            const signed char* f = T[k].f;
-            int n = 0;
-            double x[4];
-            for (; n < 4 && f[n] >= 0; ++n) x[n] = v[f[n]];
-            for (int j = 0; j < n; ++j) {
-                double m = A[k];
-                for (int l = 0; l < n; ++l)
-                    if (l != j) m *= x[l];
-                g[f[j]] += m;
-            }
-        }
-    }
-    // Hessian in v (nv x nv, row-major): every unordered pair of factor positions of a monomial
-    // contributes the product of its other factors to both off-diagonal entries (a factor
-    // repeated e times so gets e (e - 1) v^(e - 2) on the diagonal)
-    void hess(const double* v, double* H) const
-    {
-        const std::vector<Mono>& T = mono_table(D);
         for (int q = 0; q < nv * nv; ++q) H[q] = 0;
+        // the upper triangle only (a pair on the diagonal counts twice), mirrored at the end
+        auto pair = [&](int a, int b, double m) {
+            if (a == b)
+                H[a * nv + a] += 2.0 * m;
+            else if (a < b)
+                H[a * nv + b] += m;
+            else
+                H[b * nv + a] += m;
+        };
         for (int k = 0; k < K; ++k) {
             const signed char* f = T[k].f;
-            int n = 0;
-            double x[4];
-            for (; n < 4 && f[n] >= 0; ++n) x[n] = v[f[n]];
-            for (int j = 0; j < n; ++j)
-                for (int l = j + 1; l < n; ++l) {
-                    double m = A[k];
-                    for (int o = 0; o < n; ++o)
-                        if (o != j && o != l) m *= x[o];
-                    H[f[j] * nv + f[l]] += m;
-                    H[f[l] * nv + f[j]] += m;
-                }
+            const double c = A[k];
+            if (f[0] < 0) continue;
+            const double x0 = v[f[0]];
+            if (f[1] < 0) {
+                g[f[0]] += c;
+                continue;
+            }
+            const double x1 = v[f[1]];
+            if (f[2] < 0) {
+                g[f[0]] += c * x1;
+                g[f[1]] += c * x0;
+                pair(f[0], f[1], c);
+                continue;
+            }
+            const double x2 = v[f[2]];
+            if (f[3] < 0) {
+                g[f[0]] += c * x1 * x2;
+                g[f[1]] += c * x0 * x2;
+                g[f[2]] += c * x0 * x1;
+                pair(f[0], f[1], c * x2);
+                pair(f[0], f[2], c * x1);
+                pair(f[1], f[2], c * x0);
+                continue;
+            }
+            const double x3 = v[f[3]];
+            const double c01 = c * x0 * x1, c23 = c * x2 * x3;
+            g[f[0]] += c23 * x1;
+            g[f[1]] += c23 * x0;
+            g[f[2]] += c01 * x3;
+            g[f[3]] += c01 * x2;
+            pair(f[0], f[1], c23);
+            pair(f[2], f[3], c01);
+            pair(f[0], f[2], c * x1 * x3);
+            pair(f[0], f[3], c * x1 * x2);
+            pair(f[1], f[2], c * x0 * x3);
+            pair(f[1], f[3], c * x0 * x2);
         }
+        for (int a = 0; a < nv; ++a)
+            for (int b = a + 1; b < nv; ++b) H[b * nv + a] = H[a * nv + b];
     }
 };
 
@@ -208,8 +230,7 @@ struct SurrogatePose {
         const int nv = S.nv, n = np();
         double v[12], gv[12], Hv[144], J[12 * 6] = {};
         v_of(R, t, v);
-        S.grad(v, gv);
-        S.hess(v, Hv);
+        S.grad_hess(v, gv, Hv);
         if (D == 3) {
             for (int i = 0; i < 3; ++i) {
                 const Mat3 G = mul(skew_unit(i), R);
@@ -242,15 +263,18 @@ struct SurrogatePose {
                 H[k * n + l] = s;
             }
         if (D == 3) {
+            // sum_rc gR_rc (([e_i]x [e_j]x + [e_j]x [e_i]x) / 2 R)_rc with [a]x [b]x = b a^T - (a.b) I:
+            // (gR_j . R_i + gR_i . R_j) / 2 - delta_ij <gR, R>, R_i and gR_i the i-th rows
+            double dots[3][3], tr = 0;
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
-                    const Mat3 Ki = skew_unit(i), Kj = skew_unit(j);
-                    const Mat3 A = mul(mul(Ki, Kj), R), B = mul(mul(Kj, Ki), R);
-                    double s = 0;
-                    for (int r = 0; r < 3; ++r)
-                        for (int c = 0; c < 3; ++c) s += gv[3 + 3 * r + c] * 0.5 * (A(r, c) + B(r, c));
-                    H[i * n + j] += s;
+                    double d = 0;
+                    for (int c = 0; c < 3; ++c) d += gv[3 + 3 * i + c] * R(j, c);
+                    dots[i][j] = d;   // gR_i . R_j
                 }
+            for (int i = 0; i < 3; ++i) tr += dots[i][i];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) H[i * n + j] += 0.5 * (dots[j][i] + dots[i][j]) - (i == j ? tr : 0.0);
         } else {
             H[0] -= gv[2] * v[2] + gv[3] * v[3];   // d2 cos = -cos, d2 sin = -sin
         }
@@ -274,8 +298,8 @@ struct SurrogatePose {
     }
 };
 
-// Solve (H + lam I) x = -g for small symmetric systems (Gaussian elimination with pivoting)
-bool solve(int n, std::vector<double> H, std::vector<double> b, std::vector<double>& x)
+// Solve H x = b for a small system (n <= 6; Gaussian elimination with partial pivoting, in place)
+bool solve(int n, double* H, double* b, double* x)
 {
     for (int c = 0; c < n; ++c) {
         int piv = c;
@@ -292,7 +316,6 @@ bool solve(int n, std::vector<double> H, std::vector<double> b, std::vector<doub
             b[r] -= f * b[c];
         }
     }
-    x.assign(n, 0.0);
     for (int r = n - 1; r >= 0; --r) {
         double s = b[r];
         for (int k = r + 1; k < n; ++k) s -= H[r * n + k] * x[k];
@@ -314,10 +337,10 @@ int minimise_surrogate(const SurrogatePose& F, Mat3& R, double* t, int* evals)
     if (!std::isfinite(f)) return -1;
     double lam = 0;
     for (int it = 0; it < 100; ++it) {
-        std::vector<double> g(n), H(n * n);
-        F.derivs(R, t, g.data(), H.data());
+        double g[6], H[36];
+        F.derivs(R, t, g, H);
         double gn = 0;
-        for (double v : g) gn += v * v;
+        for (int k = 0; k < n; ++k) gn += g[k] * g[k];
         gn = std::sqrt(gn);
         for (int r = 0; r < n; ++r)
             for (int c = r + 1; c < n; ++c) H[r * n + c] = H[c * n + r] = 0.5 * (H[r * n + c] + H[c * n + r]);
@@ -326,24 +349,24 @@ int minimise_surrogate(const SurrogatePose& F, Mat3& R, double* t, int* evals)
         if (lam == 0) lam = 1e-9 * std::max(hmax, 1e-300);
         bool accepted = false;
         for (int tries = 0; tries < 40 && !accepted; ++tries) {
-            std::vector<double> A = H, x;
+            double A[36], mg[6], x[6];
+            for (int q = 0; q < n * n; ++q) A[q] = H[q];
             for (int r = 0; r < n; ++r) A[r * n + r] += lam;
-            std::vector<double> mg(n);
             for (int r = 0; r < n; ++r) mg[r] = -g[r];
             if (!solve(n, A, mg, x)) {
                 lam *= 10;
                 continue;
             }
             double step = 0;
-            for (double v : x) step += v * v;
+            for (int k = 0; k < n; ++k) step += x[k] * x[k];
             step = std::sqrt(step);
             if (step > 0.5) {   // trust region on the rotation increment / translation
-                for (double& v : x) v *= 0.5 / step;
+                for (int k = 0; k < n; ++k) x[k] *= 0.5 / step;
                 step = 0.5;
             }
             Mat3 Rn;
             double tn[3] = {0, 0, 0};
-            F.step(R, t, x.data(), Rn, tn);
+            F.step(R, t, x, Rn, tn);
             const double fn = F.value(Rn, tn);
             ++*evals;
             if (std::isfinite(fn) && fn <= f) {
