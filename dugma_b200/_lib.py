@@ -67,6 +67,7 @@ EXPORTS = {
     "dugma_get_shape": (c_int, [PtrArray, c_int, ip]),
     "dugma_calibrate": (c_int, [c_int, dp, dp]),
     "dugma_wait_selftest": (c_int, [c_int, ip]),
+    "dugma_coef_work_grid": (c_int, [c_int, c_int, c_int, ip]),
 }
 
 

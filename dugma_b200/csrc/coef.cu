@@ -794,6 +794,26 @@ static FusedGrid fused_grid(int n_ib, int total_tiles, int resident, int N, int 
     return best;
 }
 
+}  // namespace dugma
+
+extern "C" int dugma_coef_work_grid(int N, int M, int resident, int grid[4])
+{
+    using dugma::FusedCoefShape;
+    if (N < 1 || M < 1 || resident < 1 || !grid)
+        return dugma::set_error(DUGMA_ERR_ARG, "coef_work_grid: N, M, resident must be positive");
+    const int n_ib = (N + FusedCoefShape<3>::BI - 1) / FusedCoefShape<3>::BI;
+    const int M_pad = (M + dugma::kPadJ - 1) / dugma::kPadJ * dugma::kPadJ;
+    const int total_tiles = M_pad / 2 / FusedCoefShape<3>::TJ;
+    const dugma::FusedGrid g = dugma::fused_grid(n_ib, total_tiles, resident, N, M);
+    grid[0] = g.SB;
+    grid[1] = g.n_grp;
+    grid[2] = g.jc_tiles;
+    grid[3] = g.n_jc;
+    return DUGMA_OK;
+}
+
+namespace dugma {
+
 // Every source row against every target row in one pass (coef_fused_kernel), then the moments
 // of both sides from the H2 copies (one per target chunk) and the H1 copies (one per source group).
 template <int D>

@@ -164,6 +164,11 @@ int dugma_autotune(float* Ptr[6], int what, int model, char* report, size_t repo
  * record} into shapes[4 * k] and returns the count (negative status on error). */
 int dugma_shapes(int what, int* shapes, int max);
 
+/* The work grid compi's one-pass kernel uses for N sources and M targets when `resident` blocks
+ * fit the GPU at once (148 SMs x 3 on a B200): grid = {source blocks of 256 per group, groups,
+ * target tiles of 32 per chunk, chunks}; items = groups x chunks.  Host-only (no device work). */
+int dugma_coef_work_grid(int N, int M, int resident, int grid[4]);
+
 /* Pins the kernel shape used for `what` on this context (one of dugma_shapes' tuples). */
 int dugma_set_shape(float* Ptr[6], int what, int ipt, int nt, int tj, int pack);
 
