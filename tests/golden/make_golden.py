@@ -1,10 +1,11 @@
 """Record the reference plugins' outputs as golden fixtures (run on a GPU).
 
-    python tests/golden/make_golden.py [out_dir]
+    python tests/golden/make_golden.py [out_dir [case ...]]
 
 Runs the reference's own init / update_sig / compi (built from its sources by
-oracle/ref_build.py into oracle/_ref) on small seeded inputs and stores inputs and
-outputs in tests/golden/ref_<case>.npz:
+oracle/ref_build.py into oracle/_ref) on small seeded inputs -- and on 2048 points of each view
+of the reference's own Kinect scene 1 -- and stores inputs and outputs in
+tests/golden/ref_<case>.npz:
   inputs   X, X_C, Y, Y_C (float64), poses R (k, D, D), t (k, D)
   outputs  the FP32 device state after init (d_X, inverse covariances, d_Y, ..., det_X,
            det_Y), sig from update_sig at each pose, the 640 compi coefficients at each
@@ -64,11 +65,28 @@ def cases():
         "n,ab->nab", rng.uniform(0, 1e-3, n), np.array([[0, 1.0], [1.0, 0]]))
     YC = np.einsum("n,ab->nab", rng.uniform(1e-3, 4e-3, m), np.eye(2))
     yield "curve2d_320x256", X, XC, Y, YC, [np.eye(2), rot2d(-0.4)], [np.zeros(2), np.array([-0.1, 0.2])]
+    # 4: real data -- Kinect scene 1 of the reference's dataset (tests/golden/kinect_scenes.npz), 2048
+    # points of each view drawn without replacement, normalised as DUGMA.m:19-32 does before its
+    # init call (covariances unscaled), at the identity and at the authors' recorded pose
+    f = np.load(os.path.join(ROOT, "tests", "golden", "kinect_scenes.npz"))
+    X0, Y0 = f["X1"].astype(np.float64), f["Y1"].astype(np.float64)
+    cx, cy = f["cx1"].astype(np.float64), f["cy1"].astype(np.float64)
+    ix = np.sort(rng.choice(len(X0), 2048, replace=False))
+    iy = np.sort(rng.choice(len(Y0), 2048, replace=False))
+    X, Y = X0[ix], Y0[iy]
+    XC, YC = np.einsum("n,ab->nab", cx[ix], np.eye(3)), np.einsum("n,ab->nab", cy[iy], np.eye(3))
+    xd, yd = X.mean(axis=0), Y.mean(axis=0)
+    scale = max(np.sqrt(((X - xd) ** 2).sum(1).mean()), np.sqrt(((Y - yd) ** 2).sum(1).mean()))
+    X, Y = (X - xd) / scale, (Y - yd) / scale
+    Ra, ta = f["Ra1"], f["ta1"]
+    yield "kinect1_2048", X, XC, Y, YC, [np.eye(3), Ra], [np.zeros(3), (ta - xd + Ra @ yd) / scale]
 
 
-def main(out_dir):
+def main(out_dir, only=None):
     os.makedirs(out_dir, exist_ok=True)
     for name, X, XC, Y, YC, Rs, ts in cases():
+        if only and name not in only:
+            continue
         N, D = X.shape
         M = Y.shape[0]
         ptr = ref_plugins.init(X, XC, Y, YC)
@@ -86,4 +104,4 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"), sys.argv[2:] or None)
