@@ -17,6 +17,7 @@
 #include "coef_map.h"
 #include "context.hpp"
 #include "pairs.cuh"
+#include "umma.cuh"
 
 namespace dugma {
 
@@ -543,6 +544,376 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
     }
 }
 
+// ---------------------------------------------------------------------------
+// The one pass with the source-side sums on the tensor cores.  H2_i = sum_j p_ij g_j is, per
+// tile, the product P (sources x 32 targets) G (32 targets x monomials): each thread writes its
+// source's p into tensor memory (TMEM) as the A operand, the block writes the tile's monomials
+// into shared memory as the B operand, and one thread issues tcgen05.mma (kind::tf32, M = 128
+// sources, K = 8 targets) into FP32 accumulators in TMEM, folded into FP64 every FOLD tiles.
+// FP32 accuracy from TF32 operands by the three-term split P G ~ Ph Gh + Pl Gh + Ph Gl (h = the
+// value rounded to TF32, l = the remainder rounded to TF32): B = [Gh | Gl] (N = 32 columns) takes
+// Ph into D columns 0-15 and 16-31 in one MMA, and Pl x Gh (N = 16) adds into columns 0-15.
+// The FP32 pipe keeps the exponents and the target-side sums: 36 of the 45 lane operations a
+// pair costs in the FMA-only kernel (coef_fused_kernel).  Measured on the B200 at 64K x 64K it
+// is the slower of the two (10.5 ms against 7.8 ms; 11.1 ms with 2 sources per thread), so it is
+// the opt-in one: every pair still issues 46 instructions against 35.6 -- the TF32 split (4 integer
+// operations and a subtraction), the TMEM stores and MMA synchronisation, and at one source per
+// thread (four blocks' TMEM per SM) twice the pair-record loads -- more than the 5 packed FMAs per
+// pair it takes off the FP32 pipe, at the same 52 % issue rate.
+// IPT sources per thread, 128 threads: M-block ii holds the block's sources 128 ii .. 128 ii + 127,
+// thread tid their row tid (warp w reaches TMEM lanes 32 w .. 32 w + 31, its own rows).  TMEM per
+// M-block: 32 + 32 A columns (Ph, Pl of the tile) and 32 D columns; 128 (IPT 1) or 256 (IPT 2)
+// columns per block, so 4 or 2 blocks share an SM's 512.  The MMAs of k-step s (targets 8s..8s+7)
+// commit to mbarrier s: the next tile's p for those targets overwrites the A columns once they
+// completed.  Phase 2 (target-side sums) runs per warp over the warp's own sources, so only the
+// MMA issuer waits for the block (a named barrier) between the phases.
+// ---------------------------------------------------------------------------
+template <int D, int IPT_>
+struct TcCoefShape {
+    static constexpr int IPT = IPT_, NT = 128, TJ = 16, STAGES = 4;
+    static constexpr int FOLD = 4;                   // tiles accumulated in TMEM before each FP64 fold
+    static constexpr int BI = IPT * NT, NW = NT / 32, TT = 2 * TJ;
+    static constexpr int KS = TT / 8;                // MMA k-steps per tile
+    static constexpr int NG = 16;                    // the monomials, padded; B holds hi and lo: 2 NG columns
+    static constexpr int NF = Feat<D>::N, NP = NF / 2, SF = (NF + 3) / 4 * 4, SPS = TT + 2;
+    static constexpr uint32_t kCols = IPT == 1 ? 128 : 256;   // TMEM columns allocated
+    static constexpr uint32_t kColD = IPT * 2 * TT;            // first accumulator column
+    static constexpr int kPerSM = 512 / kCols;                 // blocks that fit an SM's TMEM
+    static constexpr int kGFloats = TT * 2 * NG;               // one B operand buffer
+    static constexpr size_t kOffBars = (size_t)STAGES * TJ * sizeof(Rec256);
+    static constexpr size_t kOffG = kOffBars + 128;            // [2 buffers][kGFloats]
+    static constexpr size_t kOffP = kOffG + sizeof(float) * 2 * kGFloats;
+    static constexpr size_t kOffF = kOffP + sizeof(float) * BI * SPS;
+    static constexpr size_t kOffT = kOffF + sizeof(float) * BI * SF;
+    static constexpr size_t kUsed = kOffT + sizeof(float) * NW * TT * (NF + 1) + 16;
+    // shared memory per block such that no more blocks fit an SM than its TMEM holds
+    static constexpr size_t kBytes = kUsed > (232448 / (kPerSM + 1) + 1024) ? kUsed : 232448 / (kPerSM + 1) + 1024;
+    static_assert(IPT * (2 * TT + 2 * NG) <= (int)kCols, "TMEM columns");
+    static_assert(NF <= NG && TT % 8 == 0 && NW == 4, "MMA shape");
+    static_assert(kBytes * kPerSM <= 232448, "shared memory");
+};
+
+template <int D, int IPT>
+__global__ void __launch_bounds__(128, 4 / IPT) coef_tc_kernel(FusedCoefArgs a)
+{
+    using S = TcCoefShape<D, IPT>;
+    constexpr int NT = S::NT, TJ = S::TJ, STAGES = S::STAGES, BI = S::BI, NW = S::NW, TT = S::TT;
+    constexpr int NF = S::NF, NP = S::NP, SF = S::SF, SPS = S::SPS, NS = Sym<D>::N, KS = S::KS, NG = S::NG;
+    static_assert(TT == 32, "phase 2 maps a lane of each half-warp to two targets of a tile");
+    static_assert(NF % 2 == 0, "monomials in pairs");
+    constexpr uint32_t kTileBytes = TJ * sizeof(Rec256);
+    constexpr uint32_t kIdescHL = idesc_tf32(128, 2 * NG), kIdescL = idesc_tf32(128, NG);
+    extern __shared__ __align__(128) unsigned char smem[];
+    Rec256(*ybuf)[TJ] = reinterpret_cast<Rec256(*)[TJ]>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::kOffBars);   // [0, STAGES): ring; then KS MMA bars
+    uint64_t* mbars = bars + STAGES;
+    int* s_item = reinterpret_cast<int*>(smem + S::kOffBars + 96);
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + S::kOffBars + 100);
+    float* sG = reinterpret_cast<float*>(smem + S::kOffG);
+    float(*sP)[SPS] = reinterpret_cast<float(*)[SPS]>(smem + S::kOffP);
+    float(*sF)[SF] = reinterpret_cast<float(*)[SF]>(smem + S::kOffF);
+    float(*sT)[TT][NF + 1] = reinterpret_cast<float(*)[TT][NF + 1]>(smem + S::kOffT);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (warp == 0) tmem_alloc(s_tmem, S::kCols);
+    if (tid == 32) {
+        for (int st = 0; st < STAGES + KS; ++st) mbar_init(&bars[st], 1);
+        mbar_fence_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *s_tmem;
+    const uint32_t tlane = 32u * warp;   // this warp's TMEM lanes (its rows of every M-block)
+    const double sgm = 1.0 / a.pose[kPoseSig];
+    const double Gs = pow(sgm, (double)D);
+    const double G2 = Gs * exp2(a.Lmax_y);
+    const double G1 = Gs * exp2(a.Lmax_x + a.Lmax_y);
+    const double inv_wmax = exp2(-a.Lmax_x);
+    const Rec256* yg = a.yrec;
+    const int n_items = a.n_grp * a.n_jc;
+    uint32_t tcount = 0;   // tiles this block has run (ring and MMA barrier phases)
+    int last_issued = -1;  // the last tile whose MMAs were issued
+    bool failed = false;
+    for (;;) {
+        if (tid == 0) *s_item = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int item = *s_item;
+        if (item >= n_items) break;
+        const int grp = item % a.n_grp, jc = item / a.n_grp;
+        const int tile0 = jc * a.jc_tiles;
+        const int ntiles = min(a.jc_tiles, a.total_tiles - tile0);
+        for (int sb = 0; sb < a.SB; ++sb) {
+            const int ib = grp * a.SB + sb;
+            if (ib >= a.n_ib) break;
+            if (tid == 0)
+                for (int k = 0; k < STAGES && k < ntiles; ++k) {
+                    const int st = (tcount + k) % STAGES;
+                    mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                    bulk_g2s(&ybuf[st][0], yg + (size_t)(tile0 + k) * TJ, kTileBytes, &bars[st]);
+                }
+            float2 PH[IPT][3], Mx[IPT][6];
+            double H[IPT][NF];
+            int row[IPT];
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) {
+                const int il = ii * NT + tid, i = ib * BI + il;
+                const bool ok = i < a.N;
+                row[ii] = ok ? i : -1;
+                const Rec128 r = a.xrec[ok ? i : 0];
+                const float hv[3] = {r.v0.x, r.v0.y, r.v0.z};
+                const float mv[6] = {r.v2.x, r.v2.y, r.v2.z, r.v2.w, r.v3.x, r.v3.y};
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const float v = ok && q < D ? hv[q] : 0.f;
+                    PH[ii][q] = make_float2(v, v);
+                }
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const float v = ok && q < NS ? mv[q] : 0.f;
+                    Mx[ii][q] = make_float2(v, v);
+                }
+                const double ws = ok ? (double)a.wx[i] * inv_wmax : 0.0;
+#pragma unroll
+                for (int q = 0; q < SF; ++q) sF[il][q] = q < NF ? __double2float_rn(ws * (double)r.g[q]) : 0.f;
+#pragma unroll
+                for (int q = 0; q < NF; ++q) H[ii][q] = 0.0;
+            }
+            constexpr int NE = (TT * NF + NT - 1) / NT;   // H1 entries of a tile per thread
+            for (int k = 0; k < ntiles; ++k) {
+                const uint32_t u = tcount + k;
+                const int st = u % STAGES;
+                const int jt = (tile0 + k) * TT;
+                // this thread's H1 entries of the tile as the previous source block left them
+                double prev[NE];
+#pragma unroll
+                for (int n = 0; n < NE; ++n) {
+                    const int e = tid + n * NT, l2 = e / NF, q = e - l2 * NF;
+                    prev[n] = (sb > 0 && e < TT * NF && jt + l2 < a.M)
+                                  ? a.h1_part[((size_t)grp * a.M + jt + l2) * 16 + q]
+                                  : 0.0;
+                }
+                bool ok = mbar_wait_bounded(&bars[st], (u / STAGES) & 1u, a.err);
+                const Rec256* yb = ybuf[st];
+                // B operand: the tile's target monomials zero-padded to NG, TF32 hi in columns 0..NG-1
+                // and lo in NG..2NG-1, as core matrices of 8 columns x 4 targets (k-step s starts
+                // 256 s floats in; LBO 512 B between target quads, SBO 128 B between column
+                // octets).  Buffer u & 1: the MMAs that read it two tiles ago completed before the
+                // previous tile's p went to TMEM.
+                float* gb = sG + (u & 1) * S::kGFloats;
+#pragma unroll
+                for (int e = tid; e < TT * NG; e += NT) {
+                    const int t = e / NG, n = e - t * NG;
+                    float v = 0.f;
+                    if (n < NF) {
+                        const float2 gv = fld256(yb[t >> 1], 16 + n);
+                        v = (t & 1) ? gv.y : gv.x;
+                    }
+                    const float hi = tf32_rna(v);
+                    const int base = ((t >> 2) * 4) * 32 + (t & 3);
+                    gb[base + (n >> 3) * 32 + (n & 7) * 4] = hi;
+                    gb[base + ((n + NG) >> 3) * 32 + (n & 7) * 4] = tf32_rna(v - hi);
+                }
+                // phase 1: p for every pair, into sP (phase 2) and TMEM (the MMAs), 4 records per k-step
+#pragma unroll
+                for (int s = 0; s < KS; ++s) {
+                    float2 pq[IPT][4];
+#pragma unroll
+                    for (int r4 = 0; r4 < 4; ++r4) {
+                        const int jj = 4 * s + r4;
+                        const Rec256& r = yb[jj];
+                        float2 nh[3], nl[3], ms[6];
+#pragma unroll
+                        for (int q = 0; q < D; ++q) { nh[q] = fld256(r, q); nl[q] = fld256(r, 4 + q); }
+                        const float2 lv = fld256(r, 3);
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) ms[q] = fld256(r, 8 + q);
+#pragma unroll
+                        for (int ii = 0; ii < IPT; ++ii) {
+                            float2 d[3];
+#pragma unroll
+                            for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), nl[q]);
+                            const float2 t1 = qform2<D>(Mx[ii], d, lv);
+                            const float2 t2 = qform2<D>(ms, d, lv);
+                            const float2 p =
+                                fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+                            pq[ii][r4] = p;
+                            *reinterpret_cast<float2*>(&sP[ii * NT + tid][2 * jj]) = p;
+                        }
+                    }
+                    // the previous tile's k-step s read these A columns
+                    if (u > 0) {
+                        ok = mbar_wait_bounded(&mbars[s], (u - 1) & 1u, a.err) && ok;
+                        tc_fence_after();
+                    }
+#pragma unroll
+                    for (int ii = 0; ii < IPT; ++ii) {
+                        float hv[8], lv8[8];
+#pragma unroll
+                        for (int r4 = 0; r4 < 4; ++r4) {
+                            hv[2 * r4] = tf32_rna(pq[ii][r4].x);
+                            hv[2 * r4 + 1] = tf32_rna(pq[ii][r4].y);
+                            lv8[2 * r4] = tf32_rna(pq[ii][r4].x - hv[2 * r4]);
+                            lv8[2 * r4 + 1] = tf32_rna(pq[ii][r4].y - hv[2 * r4 + 1]);
+                        }
+                        const uint32_t c0 = (uint32_t)ii * 2 * TT + 8 * s;
+                        tmem_st8(tmem_addr(tbase, tlane, c0), hv);
+                        tmem_st8(tmem_addr(tbase, tlane, c0 + TT), lv8);
+                    }
+                }
+                // fold the accumulators of the last FOLD tiles (complete: k-step KS-1 of the previous
+                // tile was waited for above) before this tile's MMAs restart them
+                if (k > 0 && k % S::FOLD == 0) {
+#pragma unroll
+                    for (int ii = 0; ii < IPT; ++ii) {
+                        float d0[16], d1[16];
+                        const uint32_t cd = S::kColD + 2u * NG * ii;
+                        tmem_ld16(tmem_addr(tbase, tlane, cd), d0);
+                        tmem_ld16(tmem_addr(tbase, tlane, cd + NG), d1);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int q = 0; q < NF; ++q) H[ii][q] += (double)d0[q] + (double)d1[q];
+                    }
+                }
+                // the block's p and B operand are in place: the MMA issuer (warp 0) waits for the
+                // other warps; they go on to phase 2
+                tmem_wait_st();
+                fence_proxy_async_smem();
+                tc_fence_before();
+                if (warp == 0) {
+                    named_bar_sync(1, NT);
+                    last_issued = (int)u;
+                    if (lane == 0) {
+                        tc_fence_after();
+#pragma unroll 1
+                        for (int s = 0; s < KS; ++s) {
+                            const uint64_t bd = smem_desc_kmajor(gb + 256 * s, 512, 128);
+#pragma unroll
+                            for (int ii = 0; ii < IPT; ++ii) {
+                                const uint32_t dcol = tbase + S::kColD + 2u * NG * ii;
+                                const uint32_t acol = tbase + (uint32_t)ii * 2 * TT + 8u * s;
+                                umma_tf32_ts(dcol, acol, bd, kIdescHL, s > 0 || k % S::FOLD != 0);
+                                umma_tf32_ts(dcol, acol + TT, bd, kIdescL, true);
+                            }
+                            umma_commit(&mbars[s]);
+                        }
+                        if (k + STAGES < ntiles) {
+                            mbar_arrive_expect_tx(&bars[st], kTileBytes);
+                            bulk_g2s(&ybuf[st][0], yg + (size_t)(tile0 + k + STAGES) * TJ, kTileBytes, &bars[st]);
+                        }
+                    }
+                    __syncwarp();
+                } else {
+                    named_bar_arrive(1, NT);
+                    last_issued = (int)u;
+                }
+                // phase 2 (the FP32 pipe): warp w sums its own sources (rows 32 w + lane of each
+                // M-block); lane (sh, tl) owns targets 2 tl and 2 tl + 1 and takes every other source
+                // (parity sh), each f32x2 operation a pair of monomials; the two halves then swap
+                // partials so that lane (sh, tl) holds all of the warp's sources for target 2 tl + sh
+                {
+                    const int sh = lane >> 4, tl = lane & 15;
+                    float2 a0[NP], a1[NP];
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) a0[q] = a1[q] = make_float2(0.f, 0.f);
+#pragma unroll 8
+                    for (int s2 = 0; s2 < 16 * IPT; ++s2) {
+                        const int kk = sh + 2 * s2;
+                        const int i = (kk >> 5) * NT + 32 * warp + (kk & 31);
+                        const float2 pv = *reinterpret_cast<const float2*>(&sP[i][2 * tl]);
+                        const float4* f4 = reinterpret_cast<const float4*>(&sF[i][0]);
+                        float f[SF];
+#pragma unroll
+                        for (int v = 0; v < SF / 4; ++v) {
+                            const float4 fv = f4[v];
+                            f[4 * v] = fv.x;
+                            f[4 * v + 1] = fv.y;
+                            f[4 * v + 2] = fv.z;
+                            f[4 * v + 3] = fv.w;
+                        }
+                        const float2 p0 = make_float2(pv.x, pv.x), p1 = make_float2(pv.y, pv.y);
+#pragma unroll
+                        for (int q = 0; q < NP; ++q) {
+                            const float2 fq = make_float2(f[2 * q], f[2 * q + 1]);
+                            a0[q] = ffma2(p0, fq, a0[q]);
+                            a1[q] = ffma2(p1, fq, a1[q]);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        const float2 give = sh ? a0[q] : a1[q];
+                        float2 keep = sh ? a1[q] : a0[q];
+                        keep.x += __shfl_xor_sync(0xffffffffu, give.x, 16);
+                        keep.y += __shfl_xor_sync(0xffffffffu, give.y, 16);
+                        sT[warp][2 * tl + sh][2 * q] = keep.x;
+                        sT[warp][2 * tl + sh][2 * q + 1] = keep.y;
+                    }
+                }
+                if (__syncthreads_or(!ok)) {
+                    // a tile or an MMA never completed: drain the copies still in flight (bounded), stop
+                    failed = true;
+                    if (tid == 0)
+                        for (int q = k; q < ntiles && q <= k + STAGES; ++q) {
+                            const uint32_t uq = tcount + q;
+                            mbar_wait_bounded(&bars[uq % STAGES], (uq / STAGES) & 1u, nullptr);
+                        }
+                    break;
+                }
+                // the warps' partials in fixed order, into the group's H1 rows (FP64)
+#pragma unroll
+                for (int n = 0; n < NE; ++n) {
+                    const int e = tid + n * NT, l2 = e / NF, q = e - l2 * NF;
+                    if (e >= TT * NF || jt + l2 >= a.M) continue;
+                    float sum = sT[0][l2][q];
+#pragma unroll
+                    for (int w2 = 1; w2 < NW; ++w2) sum += sT[w2][l2][q];
+                    a.h1_part[((size_t)grp * a.M + jt + l2) * 16 + q] = prev[n] + G1 * (double)sum;
+                }
+            }
+            if (failed) break;
+            // the last tile's MMAs, then its accumulators into H
+            const bool ok = mbar_wait_bounded(&mbars[KS - 1], (uint32_t)last_issued & 1u, a.err);
+            tc_fence_after();
+            if (ok)
+#pragma unroll
+                for (int ii = 0; ii < IPT; ++ii) {
+                    float d0[16], d1[16];
+                    const uint32_t cd = S::kColD + 2u * NG * ii;
+                    tmem_ld16(tmem_addr(tbase, tlane, cd), d0);
+                    tmem_ld16(tmem_addr(tbase, tlane, cd + NG), d1);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < NF; ++q) H[ii][q] += (double)d0[q] + (double)d1[q];
+                }
+            tcount += ntiles;
+            tc_fence_before();
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+#pragma unroll
+            for (int ii = 0; ii < IPT; ++ii) {
+                if (row[ii] < 0) continue;
+                const double w = (double)a.wx[row[ii]] * G2;
+                double* o = a.h2_part + ((size_t)jc * a.N + row[ii]) * 16;
+#pragma unroll
+                for (int q = 0; q < NF; ++q) o[q] = w * H[ii][q];
+            }
+        }
+        if (failed) break;
+    }
+    // every MMA this block issued has completed (or its wait gave up and the error word is set):
+    // give the TMEM back
+    if (failed && tid == 0 && last_issued >= 0)
+        mbar_wait_bounded(&mbars[KS - 1], (uint32_t)last_issued & 1u, nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tbase, S::kCols);
+    }
+}
+
 __constant__ signed char c_moment3[kNumMoments3D][4];
 __constant__ signed char c_moment2[kNumMoments2D][4];
 // per side, the indices of its moments in the table (kind 2: side 0, kind 1: side 1)
@@ -732,8 +1103,9 @@ static int upload_moment_tables(int dev)
     return DUGMA_OK;
 }
 
-// the fused kernel's dynamic shared memory limit, once per device; its resident blocks per SM
-template <int D>
+// the one-pass kernel's dynamic shared memory limit, once per device; its resident blocks per SM
+// (KIND 0: coef_fused_kernel; 1, 2: coef_tc_kernel with 1 or 2 sources per thread)
+template <int D, int KIND>
 static int fused_coef_setup(int dev, int* per_sm)
 {
     static std::mutex mu;
@@ -743,11 +1115,34 @@ static int fused_coef_setup(int dev, int* per_sm)
         *per_sm = blocks[dev];
         return DUGMA_OK;
     }
-    DUGMA_CK(cudaFuncSetAttribute(coef_fused_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)FusedCoefShape<D>::kBytes));
+    using T = TcCoefShape<D, KIND == 2 ? 2 : 1>;
+    const void* fn = KIND == 0 ? (const void*)coef_fused_kernel<D> : (const void*)coef_tc_kernel<D, T::IPT>;
+    const int nt = KIND == 0 ? FusedCoefShape<D>::NT : T::NT;
+    const size_t bytes = KIND == 0 ? FusedCoefShape<D>::kBytes : T::kBytes;
+    DUGMA_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     int nb = 0;
-    DUGMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, coef_fused_kernel<D>, FusedCoefShape<D>::NT,
-                                                           FusedCoefShape<D>::kBytes));
+    if (KIND == 0) {
+        DUGMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, nt, bytes));
+    } else {
+        // The occupancy query answers 1 for every kernel that allocates TMEM (measured on the B200
+        // with driver 580), while the SM runs as many such blocks as their TMEM columns, registers
+        // and shared memory allow; the shared memory per block is sized so that no more blocks fit
+        // than TMEM holds (a block beyond them would wait in tcgen05.alloc until another exits).
+        cudaFuncAttributes fa{};
+        DUGMA_CK(cudaFuncGetAttributes(&fa, fn));
+        int smem_sm = 0, regs_sm = 0;
+        DUGMA_CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        DUGMA_CK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+        const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;   // allocated per warp in units of 256
+        const int by_regs = regs_sm / (regs_warp * (nt / 32));
+        const int by_smem = smem_sm / (int)(bytes + 1024);            // 1 KB reserved per block
+        nb = std::min(T::kPerSM, std::min(by_regs, by_smem));
+        if (nb < 1 || by_smem > T::kPerSM)
+            return set_error(DUGMA_ERR_STATE,
+                             "compi: the tensor-core kernel fits %d blocks per SM by registers and %d by shared "
+                             "memory; TMEM holds %d",
+                             by_regs, by_smem, T::kPerSM);
+    }
     if (dev >= (int)blocks.size()) blocks.resize(dev + 1, 0);
     blocks[dev] = std::max(nb, 1);
     *per_sm = blocks[dev];
@@ -820,13 +1215,20 @@ template <int D>
 static int coef_fused_launch(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s,
                              double* host_moments)
 {
-    using S = FusedCoefShape<D>;
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
+    const int kind = c.coef_kernel;
     int per_sm = 1;
-    DUGMA_RET(fused_coef_setup<D>(c.dev, &per_sm));
+    if (kind == 1)
+        DUGMA_RET((fused_coef_setup<D, 1>(c.dev, &per_sm)));
+    else if (kind == 2)
+        DUGMA_RET((fused_coef_setup<D, 2>(c.dev, &per_sm)));
+    else
+        DUGMA_RET((fused_coef_setup<D, 0>(c.dev, &per_sm)));
     const int resident = c.num_sms * per_sm;
-    const int n_ib = (c.N + S::BI - 1) / S::BI;
-    const int total_tiles = c.M_pad / 2 / S::TJ;
+    const int BI = kind == 1 ? TcCoefShape<D, 1>::BI : kind == 2 ? TcCoefShape<D, 2>::BI : FusedCoefShape<D>::BI;
+    const int n_ib = (c.N + BI - 1) / BI;
+    static_assert(TcCoefShape<D, 1>::TJ == FusedCoefShape<D>::TJ, "the kernels stream tiles of the same records");
+    const int total_tiles = c.M_pad / 2 / FusedCoefShape<D>::TJ;
     if (c.coef_grid[0] == 0) {
         const FusedGrid fg = fused_grid(n_ib, total_tiles, resident, c.N, c.M);
         c.coef_grid[0] = fg.SB;
@@ -870,7 +1272,12 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
         ++c.tused;
     }
     const int grid = std::min(resident, n_grp * n_jc);
-    coef_fused_kernel<D><<<grid, S::NT, S::kBytes, s>>>(a);
+    if (kind == 1)
+        coef_tc_kernel<D, 1><<<grid, TcCoefShape<D, 1>::NT, TcCoefShape<D, 1>::kBytes, s>>>(a);
+    else if (kind == 2)
+        coef_tc_kernel<D, 2><<<grid, TcCoefShape<D, 2>::NT, TcCoefShape<D, 2>::kBytes, s>>>(a);
+    else
+        coef_fused_kernel<D><<<grid, FusedCoefShape<D>::NT, FusedCoefShape<D>::kBytes, s>>>(a);
     DUGMA_CK(cudaGetLastError());
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
     const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
