@@ -6,9 +6,11 @@ The kernel is chosen when a context is created (DUGMA_COEF_KERNEL = 1: one sourc
 four blocks per SM; 2: two sources per thread, two blocks per SM), so a child process computes the
 coefficients with it on ragged sizes in 3D and 2D -- clouds smaller than one 128-source M-block,
 one past a tile boundary, more rows than fit one round of work items -- twice each (the repeat must
-give the same bits).  The parent holds them to the oracle at the tolerance of the other compi tests
-(2e-6 of the largest coefficient; a single pair 5e-6, its exponent ~100) and to the default
-kernel's coefficients at 4e-6.
+give the same bits).  The problems are those of test_compi_sizes.py (same seeds).  The parent holds
+them to the oracle at the tolerance of the other compi tests (2e-6 of the largest coefficient; the
+single pair 5e-6, its exponent ~100) and to the default kernel's coefficients at 4e-6.  (A single
+pair whose exponent falls below FP32's range, -126 in log2, is 0 in both kernels and tiny in the
+FP64 oracle; these seeds stay inside it.)
 """
 import json
 import os
@@ -36,8 +38,8 @@ from tests.test_gpu_parity import _pose, _problem_small
 out = []
 for D, n, m in json.loads(sys.argv[2]):
     bad = (0,) if min(n, m) > 1 else ()
-    X, XC, Y, YC = _problem_small(D, n, m, seed=n * 3 + m, bad=bad)
-    R, t = _pose(D, seed=(n + m) % 7, scale=0.1)
+    X, XC, Y, YC = _problem_small(D, n, m, seed=n * 7 + m, bad=bad)
+    R, t = _pose(D, seed=(n * 7 + m) % 11, scale=0.1)
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
         _, h = api.init(X, XC, Y, YC)
@@ -64,8 +66,8 @@ def test_tensor_core_compi_matches_oracle_and_default_kernel(kind):
     import warnings
     for (D, n, m), r in zip(CASES, res):
         bad = (0,) if min(n, m) > 1 else ()
-        X, XC, Y, YC = _problem_small(D, n, m, seed=n * 3 + m, bad=bad)
-        R, t = _pose(D, seed=(n + m) % 7, scale=0.1)
+        X, XC, Y, YC = _problem_small(D, n, m, seed=n * 7 + m, bad=bad)
+        R, t = _pose(D, seed=(n * 7 + m) % 11, scale=0.1)
         with warnings.catch_warnings():
             warnings.simplefilter("ignore")
             _, h = api.init(X, XC, Y, YC)
