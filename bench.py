@@ -12,7 +12,8 @@ value       whole-job pair-terms/s with the clouds resident on the device (CUDA 
             by writing 256 MiB on that stream before each step's start event).
 e2e         the same metric through the C ABI with host buffers: dugma_init (FP64 clouds
             and covariances copied in from pinned host memory), dugma_energy_grad (E and g
-            copied out) and dugma_fr_m per step, wall clock (max over ranks).
+            copied out) and dugma_fr_m per step, wall clock (max over ranks); the host thread
+            and the pinned inputs on the CPUs NVML reports local to the GPU.
 roofline    the adjoint kernel's FP32-pipe instruction rate (algorithmic instructions per
             pair x pairs per launch / launch time from CUDA events inside the library)
             against the FP32 fused-multiply-add rate measured in this run.
@@ -138,6 +139,25 @@ def all_reduce(values, op):
         t = t.cuda()
     dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX)
     return [float(v) for v in t.cpu()]
+
+
+def gpu_local_cpus(dev):
+    """The host CPUs NVML reports as local to CUDA device `dev` (its NUMA node), within this
+    process's allowed set; empty when NVML cannot tell (read-only queries, nothing is changed)."""
+    try:
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+            n = os.cpu_count() or 64
+            masks = pynvml.nvmlDeviceGetCpuAffinity(h, (n + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * w + b for w, m in enumerate(masks) for b in range(64) if (int(m) >> b) & 1}
+        return cpus & os.sched_getaffinity(0)
+    except Exception:
+        return set()
 
 
 def workload(wl, n=0):
@@ -990,41 +1010,53 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        # the step's inputs in pinned host memory, laid out as the C ABI takes them (the
-        # covariance arrays are views whose transpose is the contiguous MATLAB block order)
-        def pinned(a):
-            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        # the host threads and the pinned inputs on the GPU's own NUMA node (NVML's CPU affinity of
+        # the device), as a host application placed for this GPU would have them; restored after
+        cpus_all = os.sched_getaffinity(0)
+        cpus_local = gpu_local_cpus(torch.cuda.current_device())
+        if cpus_local:
+            os.sched_setaffinity(0, cpus_local)
+        try:
+            # the step's inputs in pinned host memory, laid out as the C ABI takes them (the
+            # covariance arrays are views whose transpose is the contiguous MATLAB block order)
+            def pinned(a):
+                return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
 
-        Xh, Yh = pinned(P.X), pinned(P.Y)
-        X_C = pinned(np.transpose(P.X_C, (0, 2, 1))).transpose(0, 2, 1)
-        Y_C = pinned(np.transpose(P.Y_C, (0, 2, 1))).transpose(0, 2, 1)
-        # the clouds and covariances, plus the 16-double pose block dugma_energy_grad uploads
-        h2d = 8 * (Xh.size + X_C.size + Yh.size + Y_C.size) + 8 * 16
-        # warm-up of the end-to-end path
-        _, h2 = api.init(Xh, X_C, Yh, Y_C)
-        api.energy_grad(h2, R, t, sig, model=args.model)
-        api.fr_m(h2)
-        ksteps = max(3, min(args.steps, 10))
-        ph = [0.0, 0.0, 0.0]
-        t0 = time.perf_counter()
-        for _ in range(ksteps):
-            a = time.perf_counter()
+            Xh, Yh = pinned(P.X), pinned(P.Y)
+            X_C = pinned(np.transpose(P.X_C, (0, 2, 1))).transpose(0, 2, 1)
+            Y_C = pinned(np.transpose(P.Y_C, (0, 2, 1))).transpose(0, 2, 1)
+            # the clouds and covariances, plus the 16-double pose block dugma_energy_grad uploads
+            h2d = 8 * (Xh.size + X_C.size + Yh.size + Y_C.size) + 8 * 16
+            # warm-up of the end-to-end path
             _, h2 = api.init(Xh, X_C, Yh, Y_C)
-            b = time.perf_counter()
             api.energy_grad(h2, R, t, sig, model=args.model)
-            c = time.perf_counter()
             api.fr_m(h2)
-            d = time.perf_counter()
-            ph[0] += b - a
-            ph[1] += c - b
-            ph[2] += d - c
-        el = time.perf_counter() - t0
-        el = all_reduce([el], "max")[0]
-        e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "host_memory": "pinned",
-               "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": 8 * (1 + ng) + 4, "steps": ksteps,
-               "ms_per_step": {"init": 1e3 * ph[0] / ksteps, "energy_grad": 1e3 * ph[1] / ksteps,
-                               "fr_m": 1e3 * ph[2] / ksteps}}
+            ksteps = max(3, min(args.steps, 10))
+            ph = [0.0, 0.0, 0.0]
+            t0 = time.perf_counter()
+            for _ in range(ksteps):
+                a = time.perf_counter()
+                _, h2 = api.init(Xh, X_C, Yh, Y_C)
+                b = time.perf_counter()
+                api.energy_grad(h2, R, t, sig, model=args.model)
+                c = time.perf_counter()
+                api.fr_m(h2)
+                d = time.perf_counter()
+                ph[0] += b - a
+                ph[1] += c - b
+                ph[2] += d - c
+            el = time.perf_counter() - t0
+            el = all_reduce([el], "max")[0]
+            e2e = {"value": world * pairs * ksteps / el, "unit": "pair-terms/s", "host_memory": "pinned",
+                   "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": 8 * (1 + ng) + 4, "steps": ksteps,
+                   "ms_per_step": {"init": 1e3 * ph[0] / ksteps, "energy_grad": 1e3 * ph[1] / ksteps,
+                                   "fr_m": 1e3 * ph[2] / ksteps}}
+        finally:
+            if cpus_local:
+                os.sched_setaffinity(0, cpus_all)
+        e2e["host_cpus"] = (f"{len(cpus_local)} CPUs local to the GPU (NVML affinity)" if cpus_local
+                            else "all allowed CPUs (NVML gave no affinity)")
 
     cpu = None
     if not args.no_cpu and world == 1:

@@ -474,6 +474,9 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     // source-side sums on the tensor cores, 1 or 2 sources per thread)
     const char* coef_k = getenv("DUGMA_COEF_KERNEL");
     if (coef_k && *coef_k >= '0' && *coef_k <= '2' && !coef_k[1]) c->coef_kernel = *coef_k - '0';
+    // the kernels of a call each wait for the one before (DUGMA_NO_PDL set): no early launch
+    const char* no_pdl = getenv("DUGMA_NO_PDL");
+    c->pdl = !(no_pdl && *no_pdl && *no_pdl != '0');
     const char* no_map = getenv("DUGMA_NO_MAPPED_STAGING");
     if ((no_map && *no_map && *no_map != '0') ||
         cudaHostGetDevicePointer((void**)&c->host_dev, c->host, 0) != cudaSuccess) {

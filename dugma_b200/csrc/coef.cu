@@ -72,6 +72,7 @@ __global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __r
                                      Rec128* __restrict__ xr, Rec256* __restrict__ xr2, int* __restrict__ reset_counter,
                                      int* __restrict__ reset_err)
 {
+    pdl_trigger();   // the one-pass kernel may be scheduled now; it waits for this kernel's writes
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (reset_counter) *reset_counter = 0;
@@ -352,6 +353,10 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
     float(*sF)[SF] = reinterpret_cast<float(*)[SF]>(smem + S::kOffF);
     float(*sT)[TT][NF + 1] = reinterpret_cast<float(*)[TT][NF + 1]>(smem + S::kOffT);
 
+    // a dependent of the coefficient prologue (records, pose, zeroed counter), and the moments
+    // kernel a dependent of this one
+    pdl_trigger();
+    pdl_wait();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         for (int st = 0; st < STAGES; ++st) mbar_init(&bars[st], 1);
@@ -614,6 +619,8 @@ __global__ void __launch_bounds__(128, 4 / IPT) coef_tc_kernel(FusedCoefArgs a)
     float(*sF)[SF] = reinterpret_cast<float(*)[SF]>(smem + S::kOffF);
     float(*sT)[TT][NF + 1] = reinterpret_cast<float(*)[TT][NF + 1]>(smem + S::kOffT);
 
+    pdl_trigger();   // as in coef_fused_kernel
+    pdl_wait();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (warp == 0) tmem_alloc(s_tmem, S::kCols);
     if (tid == 32) {
@@ -943,6 +950,8 @@ template <int D>
 __global__ void __launch_bounds__(kMomThreads) moments_kernel(const MomSide s0, const MomSide s1,
                                                               const double* __restrict__ pose)
 {
+    pdl_trigger();   // in one pass: a dependent of the one-pass kernel, and the reduction one of this kernel
+    pdl_wait();
     const MomSide ms = blockIdx.y == 0 ? s0 : s1;
     if ((int)blockIdx.x >= ms.nblk) return;
     const double* __restrict__ hpart = ms.h;
@@ -1041,6 +1050,7 @@ __global__ void moments_reduce_kernel(const double* __restrict__ a, int na, cons
                                       int nm, double* __restrict__ out, const int* __restrict__ err,
                                       double* __restrict__ host_out)
 {
+    pdl_wait();   // in one pass: a dependent of the moments kernel
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         out[nm] = (double)*err;
         if (host_out) host_out[nm] = (double)*err;
@@ -1273,21 +1283,25 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     }
     const int grid = std::min(resident, n_grp * n_jc);
     if (kind == 1)
-        coef_tc_kernel<D, 1><<<grid, TcCoefShape<D, 1>::NT, TcCoefShape<D, 1>::kBytes, s>>>(a);
+        DUGMA_CK(launch_dependent(c.pdl, coef_tc_kernel<D, 1>, grid, TcCoefShape<D, 1>::NT, TcCoefShape<D, 1>::kBytes,
+                                  s, a));
     else if (kind == 2)
-        coef_tc_kernel<D, 2><<<grid, TcCoefShape<D, 2>::NT, TcCoefShape<D, 2>::kBytes, s>>>(a);
+        DUGMA_CK(launch_dependent(c.pdl, coef_tc_kernel<D, 2>, grid, TcCoefShape<D, 2>::NT, TcCoefShape<D, 2>::kBytes,
+                                  s, a));
     else
-        coef_fused_kernel<D><<<grid, FusedCoefShape<D>::NT, FusedCoefShape<D>::kBytes, s>>>(a);
+        DUGMA_CK(launch_dependent(c.pdl, coef_fused_kernel<D>, grid, FusedCoefShape<D>::NT,
+                                  FusedCoefShape<D>::kBytes, s, a));
     DUGMA_CK(cudaGetLastError());
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
     const int nblk = std::max(1, std::min(2 * c.num_sms, (std::max(c.N, c.M) + 31) / 32));
     const int nb0 = std::min(nblk, c.N), nb1 = std::min(nblk, c.M);
     const MomSide m0{a.h2_part, n_jc, c.N, nb0, 0, c.x, c.xinv, c.mom_part};
     const MomSide m1{a.h1_part, n_grp, c.M, nb1, 1, c.y, c.yinv, c.mom_part + (size_t)nblk * NM};
-    moments_kernel<D><<<dim3(std::max(nb0, nb1), 2), kMomThreads, 0, s>>>(m0, m1, pose_dev);
-    moments_reduce_kernel<<<(NM + 7) / 8, 256, 0, s>>>(c.mom_part, nb0, c.mom_part + (size_t)nblk * NM, nb1, NM,
-                                                       moments_dev, c.err, host_moments);
-    DUGMA_CK(cudaGetLastError());
+    DUGMA_CK(launch_dependent(c.pdl, moments_kernel<D>, dim3(std::max(nb0, nb1), 2), kMomThreads, 0, s, m0, m1,
+                              (const double*)pose_dev));
+    DUGMA_CK(launch_dependent(c.pdl, moments_reduce_kernel, (NM + 7) / 8, 256, 0, s, (const double*)c.mom_part, nb0,
+                              (const double*)(c.mom_part + (size_t)nblk * NM), nb1, NM, moments_dev,
+                              (const int*)c.err, host_moments));
     return DUGMA_OK;
 }
 

@@ -159,6 +159,34 @@ struct __align__(16) Rec128 {
 };
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch.  A kernel launched by launch_dependent() may be scheduled
+// before the kernel ahead of it in the stream has finished: it calls pdl_wait() before it touches
+// any memory that kernel writes or reads (pdl_wait returns once that kernel has completed and its
+// writes are visible), and the kernel ahead calls pdl_trigger() to let it be scheduled early (it
+// is scheduled only after every block of the kernel ahead has started, so it never takes an SM a
+// block of that kernel still needs).  In a kernel launched without the attribute both are no-ops.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(bool pdl, void (*fn)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                    cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, fn, args...);
+}
+
+// ---------------------------------------------------------------------------
 // Bulk copy (TMA engine, non-tensor form) + mbarrier with bounded waits
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p)

@@ -90,6 +90,7 @@ struct Context {
     size_t scratch_bytes = 0;
     bool no_alloc = false;                    // scratch is fixed: ensure_scratch fails rather than allocating
     bool fused_coef = true;                   // compi over all rows in one pass (false: one pass per side)
+    bool pdl = true;                          // a call's dependent kernels launched early (programmatic dependent launch)
     int coef_kernel = 0;                      // the one pass: 0 FP32 pipe only (the fastest); 1, 2 source-side
                                               // sums on the tensor cores, 1 or 2 sources per thread
     int coef_grid[4] = {0, 0, 0, 0};          // that pass's work grid (SB, groups, chunk tiles, chunks), set on first use

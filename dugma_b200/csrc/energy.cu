@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __rest
                                                              double* __restrict__ out, double* __restrict__ host_out,
                                                              const int* __restrict__ err)
 {
+    pdl_wait();   // a dependent of the pair kernel: its partials
     __shared__ double red[1024];
     const int v = blockIdx.x;
     if (v >= nv) return;
@@ -68,6 +69,7 @@ __global__ void __launch_bounds__(1024) reduce_items_kernel(const double* __rest
 
 __global__ void reduce_chunks_kernel(const double* __restrict__ part, int n_jc, size_t n, double* __restrict__ out)
 {
+    pdl_wait();   // a dependent of the pair kernel (or of reduce_items_kernel after it): its partials
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         double s = 0;
         for (int c = 0; c < n_jc; ++c) s += part[(size_t)c * n + e];
@@ -230,18 +232,16 @@ int launch_pair_variant(Context& c, KernelFn fn, const KernelShape& sh, const vo
         ev1 = c.tevents[c.tused].second;
         ++c.tused;
     }
-    fn<<<grid, sh.nt, 0, s>>>(a);
-    DUGMA_CK(cudaGetLastError());
+    DUGMA_CK(launch_dependent(c.pdl, fn, grid, sh.nt, 0, s, a));
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
-    if (out_dev) {
-        reduce_items_kernel<<<nv, 1024, 0, s>>>(a.partials, n_items, nv, out_dev, host_out, c.err);
-        DUGMA_CK(cudaGetLastError());
-    }
+    if (out_dev)
+        DUGMA_CK(launch_dependent(c.pdl, reduce_items_kernel, nv, 1024, 0, s, (const double*)a.partials, n_items, nv,
+                                  out_dev, host_out, (const int*)c.err));
     if (dEdx_dev) {
         const size_t n = (size_t)rows * c.D;
         const int g = (int)std::min<size_t>((n + 255) / 256, (size_t)c.num_sms * 8);
-        reduce_chunks_kernel<<<g, 256, 0, s>>>(a.dx_part, n_jc, n, dEdx_dev);
-        DUGMA_CK(cudaGetLastError());
+        DUGMA_CK(launch_dependent(c.pdl, reduce_chunks_kernel, g, 256, 0, s, (const double*)a.dx_part, n_jc, n,
+                                  dEdx_dev));
     }
     return DUGMA_OK;
 }

@@ -173,6 +173,8 @@ template <int K>
 __global__ void nn_merge_kernel(const float2* __restrict__ part, int n_jc, int rows, int k_out, int* __restrict__ idx,
                                 float* __restrict__ d2, float* __restrict__ dmin)
 {
+    pdl_trigger();   // a dependent of the search kernel; the sigma sums (if any) dependents of this one
+    pdl_wait();
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
         float bd[K];
         int bi[K];
@@ -208,6 +210,8 @@ __global__ void nn_merge_kernel(const float2* __restrict__ part, int n_jc, int r
 __global__ void sigma_partial_kernel(const float* __restrict__ dmin, int n, int D, double* __restrict__ pe,
                                      unsigned long long* __restrict__ pq)
 {
+    pdl_trigger();   // a dependent of the merge of the nearest distances; the final sum one of this kernel
+    pdl_wait();
     __shared__ double s_exact[256];
     __shared__ unsigned long long s_q[256];
     const int per = (n + gridDim.x - 1) / gridDim.x;
@@ -242,6 +246,7 @@ __global__ void sigma_final_kernel(const double* __restrict__ pe, const unsigned
                                    int n, int D, double* __restrict__ out, double* __restrict__ host_out,
                                    const int* __restrict__ err, double* __restrict__ pose_sig)
 {
+    pdl_wait();   // a dependent of sigma_partial_kernel
     __shared__ double s_exact[256];
     __shared__ unsigned long long s_q[256];
     double se = 0;
@@ -364,12 +369,11 @@ static int nn_run(Context& c, double* pose_dev, int k, int* idx_dev, float* d2_d
     const float2* part = reinterpret_cast<const float2*>(hp);
     float* dm = dmin_dev ? dmin_dev + i0 : nullptr;
     if (K == 1)
-        nn_merge_kernel<1><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
+        DUGMA_CK(launch_dependent(c.pdl, nn_merge_kernel<1>, g, 256, 0, s, part, n_jc, rows, k, idx_dev, d2_dev, dm));
     else if (K == 8)
-        nn_merge_kernel<8><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
+        DUGMA_CK(launch_dependent(c.pdl, nn_merge_kernel<8>, g, 256, 0, s, part, n_jc, rows, k, idx_dev, d2_dev, dm));
     else
-        nn_merge_kernel<16><<<g, 256, 0, s>>>(part, n_jc, rows, k, idx_dev, d2_dev, dm);
-    DUGMA_CK(cudaGetLastError());
+        DUGMA_CK(launch_dependent(c.pdl, nn_merge_kernel<16>, g, 256, 0, s, part, n_jc, rows, k, idx_dev, d2_dev, dm));
     return DUGMA_OK;
 }
 
@@ -392,9 +396,11 @@ int launch_sigma(Context& c, double* pose_dev, double* out_dev, cudaStream_t s, 
     DUGMA_RET(c.ensure_scratch(sizeof(double) * 2 * (size_t)nb));
     double* pe = c.scratch;
     unsigned long long* pq = reinterpret_cast<unsigned long long*>(c.scratch + nb);
-    sigma_partial_kernel<<<nb, 256, 0, s>>>(c.dmin + i0, rows, c.D, pe, pq);
-    sigma_final_kernel<<<1, 256, 0, s>>>(pe, pq, nb, whole ? c.N : 0, c.D, out_dev, o.host_out, c.err, o.pose_sig);
-    DUGMA_CK(cudaGetLastError());
+    DUGMA_CK(launch_dependent(c.pdl, sigma_partial_kernel, nb, 256, 0, s, (const float*)(c.dmin + i0), rows, c.D, pe,
+                              pq));
+    DUGMA_CK(launch_dependent(c.pdl, sigma_final_kernel, 1, 256, 0, s, (const double*)pe,
+                              (const unsigned long long*)pq, nb, whole ? c.N : 0, c.D, out_dev, o.host_out,
+                              (const int*)c.err, o.pose_sig));
     return DUGMA_OK;
 }
 

@@ -57,6 +57,10 @@ __device__ __forceinline__ void run_pairs(const PairArgs& a, Body& body)
     __shared__ double red[NT / 32][NV];
     __shared__ int s_item;
 
+    // launched as a dependent of the prologue (and the reductions as dependents of this kernel):
+    // let them be scheduled, then wait for the prologue's records, pose and zeroed counter
+    pdl_trigger();
+    pdl_wait();
     const int tid = threadIdx.x;
     if (tid == 0) {
 #pragma unroll

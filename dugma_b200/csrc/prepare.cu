@@ -295,6 +295,7 @@ __global__ void prologue_kernel(const double* __restrict__ pose, const float* __
                                 const double* __restrict__ ux, int* __restrict__ reset_counter, const PoseBlock pv,
                                 int use_pv, double* __restrict__ pose_out, int* __restrict__ reset_err)
 {
+    pdl_trigger();   // the pair kernel may be scheduled now; it waits for this kernel's writes
     constexpr int NS = Sym<D>::N;
     // the pose pv by value (use_pv; block 0 also writes it to pose_out, if given, for the kernels
     // that follow) or from pose
@@ -415,6 +416,7 @@ __global__ void nn_prologue_kernel(const PoseBlock pv, int use_pv, double* __res
                                    const float* __restrict__ y, int M, int M_pad, float4* __restrict__ yp32,
                                    int* __restrict__ reset_counter, int* __restrict__ reset_err)
 {
+    pdl_trigger();   // the search kernel may be scheduled now; it waits for this kernel's writes
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (reset_counter) *reset_counter = 0;
         if (reset_err) *reset_err = 0;
