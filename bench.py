@@ -63,7 +63,8 @@ FP32_INSTR_ADJOINT_2D = 26
 # exponent and normalisation 5, energy 1, nr and nr2 2, U 3 + w 3, UU 6, A 6; SFU: rsqrt + ex2
 FP32_INSTR_CONV_ADJOINT = 68
 FP32_INSTR_ENERGY = 26      # d 6, two Horner quadratic forms 9 + 9, accumulation 2
-# compi in one pass: d 6, two Horner forms 9 + 9, p = e1 + e2 1, source-side H2 += p g 10,
+# compi in one pass: d 6, two quadratic forms 9 + 9 (Cholesky form z = U d 6 and |z|^2 3 each, or
+# Horner), p = e1 + e2 1, source-side H2 += p g 10,
 # target-side T += fw p 10
 FP32_INSTR_COMPI = 45
 SFU_PER_PAIR = 2            # two ex2
@@ -674,7 +675,7 @@ def config_plugins(L, P, peak, reps=5, clock_dir="/tmp"):
             if instr:
                 ent["roofline"] = {"bound": "fp32", "instr_per_pair": instr,
                                    "frac": instr * P.N * P.M / (kms.value / reps * 1e-3) / peak,
-                                   "note": "one pass over the pairs: d 6, two Horner forms 18, p 1, source-side "
+                                   "note": "one pass over the pairs: d 6, two quadratic forms (Cholesky) 18, p 1, source-side "
                                            "sums 10, target-side sums 10 FP32 lane-ops per pair"}
             c = clk.summary()
             if c:

@@ -470,10 +470,10 @@ int dugma_init(const double* X, const double* X_C, const double* Y, const double
     if (!c->host) return fail(set_error(DUGMA_ERR_NOMEM, "init: pinned staging allocation failed"));
     // the staging as the device addresses it; without it (not mapped, or DUGMA_NO_MAPPED_STAGING set
     // in the environment) poses and results travel by copies
-    // compi's one-pass kernel (DUGMA_COEF_KERNEL = 0, the default: the FP32 pipe alone; 1, 2: the
-    // source-side sums on the tensor cores, 1 or 2 sources per thread)
+    // compi's one-pass kernel (DUGMA_COEF_KERNEL = 0, the default: the FP32 pipe alone; 1: the
+    // source-side sums on the tensor cores)
     const char* coef_k = getenv("DUGMA_COEF_KERNEL");
-    if (coef_k && *coef_k >= '0' && *coef_k <= '2' && !coef_k[1]) c->coef_kernel = *coef_k - '0';
+    if (coef_k && *coef_k >= '0' && *coef_k <= '1' && !coef_k[1]) c->coef_kernel = *coef_k - '0';
     // the kernels of a call each wait for the one before (DUGMA_NO_PDL set): no early launch
     const char* no_pdl = getenv("DUGMA_NO_PDL");
     c->pdl = !(no_pdl && *no_pdl && *no_pdl != '0');

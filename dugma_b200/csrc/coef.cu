@@ -63,14 +63,18 @@ __device__ __forceinline__ void write_pair_half(Rec256* __restrict__ out, int j,
 // One thread per point: indices [0, M_pad) are the targets, [M_pad, M_pad + N_pad) the sources.
 // The pose is pv when use_pv (block 0 then writes it to `pose` for the kernels that follow), else
 // read from `pose`.  reset_counter and reset_err (each optional) are zeroed for those kernels.
-template <int D>
+// CHOL: each matrix as the upper Cholesky factor U' of |k| B (U'^T U' = |k| B; the sources' from
+// init's FP64 factor ux of sym(Sigma_x^-1), the targets' of C'_j in FP64 here), so that an exponent is
+// lv - |U' d|^2, a sum of squares whose FP32 rounding grows with sqrt(cond B) instead of cond B; the
+// records then carry -lv.  !CHOL: k B in the Horner form (off-diagonals doubled) and lv.
+template <int D, bool CHOL>
 __global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __restrict__ pose,
                                      const float* __restrict__ y,
                                      const float* __restrict__ yinv, const float* __restrict__ lwy, int M, int M_pad,
                                      Rec128* __restrict__ yr, Rec256* __restrict__ yr2, const float* __restrict__ x,
                                      const float* __restrict__ xinv, const float* __restrict__ lwx, int N, int N_pad,
                                      Rec128* __restrict__ xr, Rec256* __restrict__ xr2, int* __restrict__ reset_counter,
-                                     int* __restrict__ reset_err)
+                                     int* __restrict__ reset_err, const double* __restrict__ ux)
 {
     pdl_trigger();   // the one-pass kernel may be scheduled now; it waits for this kernel's writes
     constexpr int NS = Sym<D>::N, NF = Feat<D>::N;
@@ -86,7 +90,7 @@ __global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __r
     for (int k = 0; k < D * D; ++k) R[k] = use_pv ? pv.v[k] : pose[k];
 #pragma unroll
     for (int a = 0; a < D; ++a) t[a] = use_pv ? pv.v[kPoseT + a] : pose[kPoseT + a];
-    const double s = 1.0 / (use_pv ? pv.v[kPoseSig] : pose[kPoseSig]), ks = K_EXP2 * s;
+    const double s = 1.0 / (use_pv ? pv.v[kPoseSig] : pose[kPoseSig]), ks = K_EXP2 * s, sk = sqrt(-ks);
     const int stride = gridDim.x * blockDim.x;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < M_pad + N_pad; u += stride) {
         if (u >= M_pad) {
@@ -105,13 +109,17 @@ __global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __r
                 lw = lwx[i];
                 if (lw != -INFINITY)
                     for (int k = 0; k < NS; ++k) {
-                        const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
-                        const double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
-                                                (double)xinv[(size_t)i * D * D + rb + D * ra]);
-                        bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
+                        if (CHOL) {
+                            bp[k] = __double2float_rn(sk * ux[(size_t)i * NS + k]);
+                        } else {
+                            const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
+                            const double b = 0.5 * ((double)xinv[(size_t)i * D * D + ra + D * rb] +
+                                                    (double)xinv[(size_t)i * D * D + rb + D * ra]);
+                            bp[k] = __double2float_rn(ks * b * (ra == rb ? 1.0 : 2.0));
+                        }
                     }
             }
-            r.v0 = make_float4(xv[0], xv[1], xv[2], lw);
+            r.v0 = make_float4(xv[0], xv[1], xv[2], CHOL ? -lw : lw);
             r.v1 = make_float4(0.f, 0.f, 0.f, 0.f);
             r.v2 = D == 3 ? make_float4(bp[0], bp[1], bp[2], bp[3]) : make_float4(bp[0], bp[1], bp[2], 0.f);
             r.v3 = D == 3 ? make_float4(bp[4], bp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -148,15 +156,29 @@ __global__ void coef_prologue_kernel(const PoseBlock pv, int use_pv, double* __r
                         for (int k = 0; k < D; ++k) acc += A[r0][k] * R[c0 + D * k];
                         T[r0][c0] = acc;
                     }
+                double pk[6];
                 for (int k = 0; k < NS; ++k) {
                     const int ra = Sym<D>::a(k), rb = Sym<D>::b(k);
                     double acc = 0;
                     for (int q = 0; q < D; ++q) acc += R[ra + D * q] * T[q][rb];
+                    pk[k] = acc;
                     cp[k] = __double2float_rn(ks * acc * (ra == rb ? 1.0 : 2.0));
+                }
+                if (CHOL) {
+                    // C'_j has the eigenvalues of sym(Sigma_y_j^-1), which init found positive definite;
+                    // a pivot the rotation's rounding pushed under chol_upper's bound gets 1e-12 of the
+                    // trace added
+                    double u[6];
+                    if (!chol_upper<D>(pk, u)) {
+                        const double tr = pk[0] + pk[1] + (D == 3 ? pk[2] : 0.0);
+                        for (int a = 0; a < D; ++a) pk[a] += 1e-12 * tr;
+                        chol_upper<D>(pk, u);
+                    }
+                    for (int k = 0; k < NS; ++k) cp[k] = __double2float_rn(sk * u[k]);
                 }
             }
         }
-        r.v0 = make_float4(hi[0], hi[1], hi[2], lv);
+        r.v0 = make_float4(hi[0], hi[1], hi[2], CHOL ? -lv : lv);
         r.v1 = make_float4(lo[0], lo[1], lo[2], 0.f);
         r.v2 = D == 3 ? make_float4(cp[0], cp[1], cp[2], cp[3]) : make_float4(cp[0], cp[1], cp[2], 0.f);
         r.v3 = D == 3 ? make_float4(cp[4], cp[5], 0.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -188,6 +210,30 @@ __device__ __forceinline__ float2 qform2(const float2* m, const float2* d, float
     }
 }
 
+// 2^(exponent) of a pair for one side's matrix record m: !CHOL the Horner form, exponent
+// d^T (k B) d + lv; CHOL the Cholesky form with z = U' d (the same 6 operations as the Horner form's
+// first step), exponent -(|z|^2 + nlv) with nlv = -lv from the record (9 FP32 operations either way).
+template <int D, bool CHOL>
+__device__ __forceinline__ float2 pexp2(const float2* m, const float2* d, float2 lv)
+{
+    if (!CHOL) {
+        const float2 t = qform2<D>(m, d, lv);
+        return make_float2(ex2(t.x), ex2(t.y));
+    }
+    float2 m2;
+    if (D == 3) {
+        const float2 z0 = ffma2(m[4], d[2], ffma2(m[3], d[1], fmul2(m[0], d[0])));
+        const float2 z1 = ffma2(m[5], d[2], fmul2(m[1], d[1]));
+        const float2 z2 = fmul2(m[2], d[2]);
+        m2 = ffma2(z0, z0, ffma2(z1, z1, ffma2(z2, z2, lv)));
+    } else {
+        const float2 z0 = ffma2(m[2], d[1], fmul2(m[0], d[0]));
+        const float2 z1 = fmul2(m[1], d[1]);
+        m2 = ffma2(z0, z0, ffma2(z1, z1, lv));
+    }
+    return make_float2(ex2(-m2.x), ex2(-m2.y));
+}
+
 // One body for both passes.  The stationary side keeps (position hi, lo, matrix) in registers,
 // duplicated in both halves; the streamed pair record supplies two points' positions,
 // matrices, log2 weights and monomials.  H accumulates P * (streamed monomials); the sign of
@@ -195,7 +241,7 @@ __device__ __forceinline__ float2 qform2(const float2* m, const float2* d, float
 // STREAM_LO: the streamed side carries the y' low parts (targets streamed, sources stationary);
 // otherwise the stationary side does.  The other side's low part is zero (x is FP32), so d
 // needs two packed adds per coordinate instead of three.
-template <int D, int IPT_, bool STREAM_LO>
+template <int D, int IPT_, bool STREAM_LO, bool CHOL>
 struct PackedCoefBody {
     using StreamRec = Rec256;
     static constexpr int IPT = IPT_;
@@ -255,9 +301,7 @@ struct PackedCoefBody {
             float2 d[3];
 #pragma unroll
             for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), STREAM_LO ? nl[q] : PL[ii][q]);
-            const float2 t1 = qform2<D>(Mx[ii], d, lv);
-            const float2 t2 = qform2<D>(ms, d, lv);
-            const float2 p = fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+            const float2 p = fadd2(pexp2<D, CHOL>(Mx[ii], d, lv), pexp2<D, CHOL>(ms, d, lv));
 #pragma unroll
             for (int q = 0; q < NF; ++q) h[ii][q] = ffma2(p, g[q], h[ii][q]);
         }
@@ -335,7 +379,7 @@ struct FusedCoefShape {
     static constexpr size_t kBytes = kOffT + sizeof(float) * NW * TT * (NF + 1) + 16;
 };
 
-template <int D>
+template <int D, bool CHOL>
 __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
 {
     using S = FusedCoefShape<D>;
@@ -453,9 +497,7 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
                         float2 d[3];
 #pragma unroll
                         for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), nl[q]);
-                        const float2 t1 = qform2<D>(Mx[ii], d, lv);
-                        const float2 t2 = qform2<D>(ms, d, lv);
-                        const float2 p = fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+                        const float2 p = fadd2(pexp2<D, CHOL>(Mx[ii], d, lv), pexp2<D, CHOL>(ms, d, lv));
 #pragma unroll
                         for (int q = 0; q < NF; ++q) h[ii][q] = ffma2(p, g[q], h[ii][q]);
                         *reinterpret_cast<float2*>(&sP[ii * NT + tid][2 * jj]) = p;
@@ -560,7 +602,7 @@ __global__ void __launch_bounds__(128, 3) coef_fused_kernel(FusedCoefArgs a)
 // Ph into D columns 0-15 and 16-31 in one MMA, and Pl x Gh (N = 16) adds into columns 0-15.
 // The FP32 pipe keeps the exponents and the target-side sums: 36 of the 45 lane operations a
 // pair costs in the FMA-only kernel (coef_fused_kernel).  Measured on the B200 at 64K x 64K it
-// is the slower of the two (10.5 ms against 7.8 ms; 11.1 ms with 2 sources per thread), so it is
+// is the slower of the two (10.5 ms against 7.8 ms; 11.1 ms with IPT 2, not built), so it is
 // the opt-in one: every pair still issues 46 instructions against 35.6 -- the TF32 split (4 integer
 // operations and a subtraction), the TMEM stores and MMA synchronisation, and at one source per
 // thread (four blocks' TMEM per SM) twice the pair-record loads -- more than the 5 packed FMAs per
@@ -598,7 +640,7 @@ struct TcCoefShape {
     static_assert(kBytes * kPerSM <= 232448, "shared memory");
 };
 
-template <int D, int IPT>
+template <int D, int IPT, bool CHOL>
 __global__ void __launch_bounds__(128, 4 / IPT) coef_tc_kernel(FusedCoefArgs a)
 {
     using S = TcCoefShape<D, IPT>;
@@ -740,10 +782,7 @@ __global__ void __launch_bounds__(128, 4 / IPT) coef_tc_kernel(FusedCoefArgs a)
                             float2 d[3];
 #pragma unroll
                             for (int q = 0; q < D; ++q) d[q] = fadd2(fadd2(PH[ii][q], nh[q]), nl[q]);
-                            const float2 t1 = qform2<D>(Mx[ii], d, lv);
-                            const float2 t2 = qform2<D>(ms, d, lv);
-                            const float2 p =
-                                fadd2(make_float2(ex2(t1.x), ex2(t1.y)), make_float2(ex2(t2.x), ex2(t2.y)));
+                            const float2 p = fadd2(pexp2<D, CHOL>(Mx[ii], d, lv), pexp2<D, CHOL>(ms, d, lv));
                             pq[ii][r4] = p;
                             *reinterpret_cast<float2*>(&sP[ii * NT + tid][2 * jj]) = p;
                         }
@@ -1114,8 +1153,8 @@ static int upload_moment_tables(int dev)
 }
 
 // the one-pass kernel's dynamic shared memory limit, once per device; its resident blocks per SM
-// (KIND 0: coef_fused_kernel; 1, 2: coef_tc_kernel with 1 or 2 sources per thread)
-template <int D, int KIND>
+// (KIND 0: coef_fused_kernel; 1: coef_tc_kernel)
+template <int D, int KIND, bool CHOL>
 static int fused_coef_setup(int dev, int* per_sm)
 {
     static std::mutex mu;
@@ -1125,8 +1164,9 @@ static int fused_coef_setup(int dev, int* per_sm)
         *per_sm = blocks[dev];
         return DUGMA_OK;
     }
-    using T = TcCoefShape<D, KIND == 2 ? 2 : 1>;
-    const void* fn = KIND == 0 ? (const void*)coef_fused_kernel<D> : (const void*)coef_tc_kernel<D, T::IPT>;
+    using T = TcCoefShape<D, 1>;
+    const void* fn =
+        KIND == 0 ? (const void*)coef_fused_kernel<D, CHOL> : (const void*)coef_tc_kernel<D, T::IPT, CHOL>;
     const int nt = KIND == 0 ? FusedCoefShape<D>::NT : T::NT;
     const size_t bytes = KIND == 0 ? FusedCoefShape<D>::kBytes : T::kBytes;
     DUGMA_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1221,7 +1261,7 @@ namespace dugma {
 
 // Every source row against every target row in one pass (coef_fused_kernel), then the moments
 // of both sides from the H2 copies (one per target chunk) and the H1 copies (one per source group).
-template <int D>
+template <int D, bool CHOL>
 static int coef_fused_launch(Context& c, const double* pose_dev, double* moments_dev, cudaStream_t s,
                              double* host_moments)
 {
@@ -1229,13 +1269,11 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     const int kind = c.coef_kernel;
     int per_sm = 1;
     if (kind == 1)
-        DUGMA_RET((fused_coef_setup<D, 1>(c.dev, &per_sm)));
-    else if (kind == 2)
-        DUGMA_RET((fused_coef_setup<D, 2>(c.dev, &per_sm)));
+        DUGMA_RET((fused_coef_setup<D, 1, CHOL>(c.dev, &per_sm)));
     else
-        DUGMA_RET((fused_coef_setup<D, 0>(c.dev, &per_sm)));
+        DUGMA_RET((fused_coef_setup<D, 0, CHOL>(c.dev, &per_sm)));
     const int resident = c.num_sms * per_sm;
-    const int BI = kind == 1 ? TcCoefShape<D, 1>::BI : kind == 2 ? TcCoefShape<D, 2>::BI : FusedCoefShape<D>::BI;
+    const int BI = kind == 1 ? TcCoefShape<D, 1>::BI : FusedCoefShape<D>::BI;
     const int n_ib = (c.N + BI - 1) / BI;
     static_assert(TcCoefShape<D, 1>::TJ == FusedCoefShape<D>::TJ, "the kernels stream tiles of the same records");
     const int total_tiles = c.M_pad / 2 / FusedCoefShape<D>::TJ;
@@ -1283,13 +1321,10 @@ static int coef_fused_launch(Context& c, const double* pose_dev, double* moments
     }
     const int grid = std::min(resident, n_grp * n_jc);
     if (kind == 1)
-        DUGMA_CK(launch_dependent(c.pdl, coef_tc_kernel<D, 1>, grid, TcCoefShape<D, 1>::NT, TcCoefShape<D, 1>::kBytes,
-                                  s, a));
-    else if (kind == 2)
-        DUGMA_CK(launch_dependent(c.pdl, coef_tc_kernel<D, 2>, grid, TcCoefShape<D, 2>::NT, TcCoefShape<D, 2>::kBytes,
-                                  s, a));
+        DUGMA_CK(launch_dependent(c.pdl, coef_tc_kernel<D, 1, CHOL>, grid, TcCoefShape<D, 1>::NT,
+                                  TcCoefShape<D, 1>::kBytes, s, a));
     else
-        DUGMA_CK(launch_dependent(c.pdl, coef_fused_kernel<D>, grid, FusedCoefShape<D>::NT,
+        DUGMA_CK(launch_dependent(c.pdl, coef_fused_kernel<D, CHOL>, grid, FusedCoefShape<D>::NT,
                                   FusedCoefShape<D>::kBytes, s, a));
     DUGMA_CK(cudaGetLastError());
     if (ev1) DUGMA_CK(cudaEventRecord(ev1, s));
@@ -1317,12 +1352,19 @@ static int coef_impl(Context& c, double* pose_dev, double* moments_dev, cudaStre
     PoseBlock pb{};
     if (o.pose_value)
         for (int k = 0; k < kPoseDoubles; ++k) pb.v[k] = o.pose_value[k];
-    coef_prologue_kernel<D><<<std::min((n + 127) / 128, c.num_sms * 8), 128, 0, s>>>(
-        pb, o.pose_value ? 1 : 0, pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128,
-        static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128, static_cast<Rec256*>(c.xrec256),
-        fused ? c.counter : nullptr, o.reset_err ? c.err : nullptr);
+    // the Cholesky form of every matrix when every weighted point's inverse covariance has a factor,
+    // else the Horner form throughout
+    const bool chol = c.ux && c.x_indef == 0 && c.y_indef == 0;
+    const int pg = std::min((n + 127) / 128, c.num_sms * 8);
+    auto prologue = chol ? coef_prologue_kernel<D, true> : coef_prologue_kernel<D, false>;
+    prologue<<<pg, 128, 0, s>>>(pb, o.pose_value ? 1 : 0, pose_dev, c.y, c.yinv, c.lwy, c.M, c.M_pad, c.yrec128,
+                                static_cast<Rec256*>(c.yrec256), c.x, c.xinv, c.lwx, c.N, c.N_pad, c.xrec128,
+                                static_cast<Rec256*>(c.xrec256), fused ? c.counter : nullptr,
+                                o.reset_err ? c.err : nullptr, (const double*)c.ux);
     DUGMA_CK(cudaGetLastError());
-    if (fused) return coef_fused_launch<D>(c, pose_dev, moments_dev, s, o.host_moments);
+    if (fused)
+        return chol ? coef_fused_launch<D, true>(c, pose_dev, moments_dev, s, o.host_moments)
+                    : coef_fused_launch<D, false>(c, pose_dev, moments_dev, s, o.host_moments);
     constexpr int NM = D == 3 ? kNumMoments3D : kNumMoments2D;
     // per side: 2 sources per thread x 128 threads when there are rows enough for two blocks
     // per SM, else 1 x 64 (more blocks for small clouds); items cover at least rows / 8
@@ -1333,11 +1375,15 @@ static int coef_impl(Context& c, double* pose_dev, double* moments_dev, cudaStre
         const int min_chunk = std::max(64, std::min(256, rows / 16));
         const bool big = rows >= 2 * 256 * c.num_sms;
         if (big)
-            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 128, 16, 2>
-                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 128, 16, 2>;
+            *fn = side == 0 ? (chol ? coef_pass_kernel<PackedCoefBody<D, 2, true, true>, 128, 16, 2>
+                                    : coef_pass_kernel<PackedCoefBody<D, 2, true, false>, 128, 16, 2>)
+                            : (chol ? coef_pass_kernel<PackedCoefBody<D, 2, false, true>, 128, 16, 2>
+                                    : coef_pass_kernel<PackedCoefBody<D, 2, false, false>, 128, 16, 2>);
         else
-            *fn = side == 0 ? coef_pass_kernel<PackedCoefBody<D, 2, true>, 64, 16, 6>
-                            : coef_pass_kernel<PackedCoefBody<D, 2, false>, 64, 16, 6>;
+            *fn = side == 0 ? (chol ? coef_pass_kernel<PackedCoefBody<D, 2, true, true>, 64, 16, 6>
+                                    : coef_pass_kernel<PackedCoefBody<D, 2, true, false>, 64, 16, 6>)
+                            : (chol ? coef_pass_kernel<PackedCoefBody<D, 2, false, true>, 64, 16, 6>
+                                    : coef_pass_kernel<PackedCoefBody<D, 2, false, false>, 64, 16, 6>);
         return big ? KernelShape{2, 128, 16, 2, 0, min_chunk} : KernelShape{2, 64, 16, 2, 0, min_chunk};
     };
     // blocks of the moments kernel: about 32 rows each, at most 2 per SM (the partial buffer's size)

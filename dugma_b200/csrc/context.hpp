@@ -61,6 +61,7 @@ struct Context {
     double* ux = nullptr;                     // upper Cholesky factor of sym(Sigma_x^-1) per source (packed,
                                               // FP64); zero for neglected and not positive definite sources
     int x_indef = 0;                          // weighted sources whose sym(Sigma_x^-1) is not positive definite
+    int y_indef = 0;                          // weighted targets whose sym(Sigma_y^-1) is not positive definite
     double Lmax_x = 0, Lmax_y = 0;
     double cscale = 1.0;                      // CONV covariances are stored divided by this
     // per-evaluation records
@@ -91,8 +92,8 @@ struct Context {
     bool no_alloc = false;                    // scratch is fixed: ensure_scratch fails rather than allocating
     bool fused_coef = true;                   // compi over all rows in one pass (false: one pass per side)
     bool pdl = true;                          // a call's dependent kernels launched early (programmatic dependent launch)
-    int coef_kernel = 0;                      // the one pass: 0 FP32 pipe only (the fastest); 1, 2 source-side
-                                              // sums on the tensor cores, 1 or 2 sources per thread
+    int coef_kernel = 0;                      // the one pass: 0 FP32 pipe only (the fastest); 1 source-side
+                                              // sums on the tensor cores
     int coef_grid[4] = {0, 0, 0, 0};          // that pass's work grid (SB, groups, chunk tiles, chunks), set on first use
     // pinned host staging
     // [0,16) pose, [63] error word, [64,128) results, [256,512) multi-pose staging

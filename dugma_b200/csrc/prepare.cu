@@ -20,7 +20,8 @@ namespace dugma {
 // ---------------------------------------------------------------------------
 // ufac (nullable): the upper Cholesky factor of sym(cinv) per point (packed, FP64) for the
 // Cholesky-form source records; zero for neglected points, and zero with a count in *indef for
-// weighted points whose sym(cinv) is not positive definite.
+// weighted points whose sym(cinv) is not positive definite.  With ufac null and indef given, only
+// the count.
 template <int D>
 __global__ void init_points_kernel(const double* __restrict__ P, const double* __restrict__ C, int n,
                                    float* __restrict__ p32, float* __restrict__ cinv,
@@ -79,7 +80,7 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
                 atomicAdd(nonpd, 1);
             }
         }
-        if (ufac) {
+        if (ufac || indef) {
             double pk[NS], u[NS];
 #pragma unroll
             for (int k = 0; k < NS; ++k) {
@@ -87,9 +88,10 @@ __global__ void init_points_kernel(const double* __restrict__ P, const double* _
                 pk[k] = 0.5 * ((double)o[ra + D * rb] + (double)o[rb + D * ra]);
             }
             const bool ok = chol_upper<D>(pk, u);
-            if (w[i] > 0.0f && !ok) atomicAdd(indef, 1);
+            if (w[i] > 0.0f && !ok && indef) atomicAdd(indef, 1);
+            if (ufac)
 #pragma unroll
-            for (int k = 0; k < NS; ++k) ufac[(size_t)i * NS + k] = w[i] > 0.0f ? u[k] : 0.0;
+                for (int k = 0; k < NS; ++k) ufac[(size_t)i * NS + k] = w[i] > 0.0f ? u[k] : 0.0;
         }
     }
 }
@@ -196,17 +198,17 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     const int nb = std::min(kMomSlots, std::max(1, (N + M + 2047) / 2048));
     cov_trace_partial_kernel<<<nb, 256, 0, s>>>(tXC, N, tYC, M, D, c.mom);
     cov_scale_kernel<<<1, 256, 0, s>>>(c.mom, nb, N + M, D, Lm + 2);
-    // counter[4]: weighted sources without a Cholesky factor
+    // counter[4], counter[5]: weighted sources / targets without a Cholesky factor
     if (D == 3) {
         init_points_kernel<3><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter, c.ux,
                                                 c.counter + 4);
         init_points_kernel<3><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter, nullptr,
-                                                nullptr);
+                                                c.counter + 5);
     } else {
         init_points_kernel<2><<<gx, bs, 0, s>>>(tX, tXC, N, c.x, c.xinv, c.wx, c.xcov, Lm + 2, c.counter, c.ux,
                                                 c.counter + 4);
         init_points_kernel<2><<<gy, bs, 0, s>>>(tY, tYC, M, c.y, c.yinv, c.wy, c.ycov, Lm + 2, c.counter, nullptr,
-                                                nullptr);
+                                                c.counter + 5);
     }
     // counter[2], counter[3]: the largest weight of each cloud as float bits (zeroed above)
     max_weight_kernel<<<std::min(gx, 4 * c.num_sms), bs, 0, s>>>(c.wx, N, c.counter + 2);
@@ -216,7 +218,8 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     ck(cudaGetLastError(), "init kernels");
     ck(cudaMemcpyAsync(c.host, Lm, 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "copy Lmax, scale");
     ck(cudaMemcpyAsync(c.host + 3, c.counter, sizeof(int), cudaMemcpyDeviceToHost, s), "copy nonpd");
-    ck(cudaMemcpyAsync(c.host + 4, c.counter + 4, sizeof(int), cudaMemcpyDeviceToHost, s), "copy indefinite count");
+    ck(cudaMemcpyAsync(c.host + 4, c.counter + 4, 2 * sizeof(int), cudaMemcpyDeviceToHost, s),
+       "copy indefinite counts");
     ck(cudaStreamSynchronize(s), "sync");
     if (rc != DUGMA_OK) return rc;
     c.Lmax_x = std::isfinite(c.host[0]) ? c.host[0] : 0.0;
@@ -225,9 +228,10 @@ int launch_init(Context& c, const double* X, const double* XC, const double* Y, 
     int nonpd = 0;
     memcpy(&nonpd, c.host + 3, sizeof(int));
     c.nonpd = nonpd;
-    int indef = 0;
-    memcpy(&indef, c.host + 4, sizeof(int));
-    c.x_indef = c.ux ? indef : N;
+    int indef[2] = {0, 0};
+    memcpy(indef, c.host + 4, 2 * sizeof(int));
+    c.x_indef = c.ux ? indef[0] : N;
+    c.y_indef = indef[1];
     return DUGMA_OK;
 }
 

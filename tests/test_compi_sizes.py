@@ -6,9 +6,10 @@ smaller than one 256-source block or one 32-target tile, sizes one past a block 
 boundary, and clouds of very different sizes on the two sides.  Each result is checked against
 the FP64 oracle (compi.cu:646-791 restated) at 2e-6 of the largest coefficient, repeated calls
 must give the same bits, and a non-positive-definite covariance on each side (weight zero,
-init.cu:48-57) must drop out.  A single pair is held to 5e-6: with one point per cloud, sigma
-is that pair's own squared distance, so the exponents reach ~100 and the FP32 exponent's
-rounding (~6e-8 of it) is the pair's error, with nothing to average it over (2D: 2.4e-6).
+init.cu:48-57) must drop out.  A single pair is held to 2e-5: with one point per cloud, sigma
+is that pair's own squared distance, so its exponent reaches ~100 (a weight of 2^-100) and the
+FP32 rounding of the exponent -- the Cholesky form's z = U d and |z|^2, ~1e-7 of it -- is the
+pair's error, with nothing to average it over (measured 1.06e-5 in 3D).
 """
 import numpy as np
 import pytest
@@ -50,7 +51,7 @@ def _check(D, n, m, seed):
         scale = np.abs(Ao).max()
         assert scale > 0
         err = np.abs(A - Ao).max() / scale
-        assert err <= (5e-6 if n * m == 1 else 2e-6), (n, m, err)
+        assert err <= (2e-5 if n * m == 1 else 2e-6), (n, m, err)
     finally:
         api.fr_m(h)
 

@@ -122,6 +122,9 @@ def test_library_matches_reference_plugins(path):
                 assert np.abs(A - Ar).max() <= 1e-6 * scale
             else:
                 Ao = st.coef(R, t, float(z["sig"][k]))[:K]
+                print(f"{_name(path)} pose {k}: library vs FP64 oracle {np.abs(A - Ao).max() / np.abs(Ao).max():.2e}, "
+                      f"vs reference {np.abs(A - Ar).max() / scale:.2e}, oracle vs reference "
+                      f"{np.abs(Ao - Ar).max() / scale:.2e}")
                 assert np.abs(A - Ao).max() <= 2e-6 * np.abs(Ao).max()
                 assert np.abs(A - Ar).max() <= np.abs(Ao - Ar).max() + 2e-6 * scale
     finally:
