@@ -389,15 +389,18 @@ def test_fd_grad_workload1(w1):
     assert _rel(g, go_lim) <= 1e-5
 
 
+@pytest.mark.parametrize("side", ["sources", "targets"])
 @pytest.mark.parametrize("D", [3, 2])
-def test_indefinite_source_inverse_uses_horner_form(D):
-    """A few source covariances with det > 0 that are not positive definite (the reference
-    accepts them: only det <= 0 is neglected, init.cu:48-57): no Cholesky factor exists, so the
-    packed kernels run on the Horner form; the results still match the oracle."""
+def test_indefinite_inverse_uses_horner_form(D, side):
+    """A few covariances with det > 0 that are not positive definite (the reference accepts them:
+    only det <= 0 is neglected, init.cu:48-57), on the source or on the target side: no Cholesky
+    factor exists, so the packed adjoint (sources) and compi (either side) run on the Horner form;
+    the energy, its gradient and the coefficients still match the oracle."""
     X, XC, Y, YC = _problem_small(D, 300, 260, seed=9)
     # det > 0 with two negative eigenvalues; their quadratic forms stay small (|exponent| < 1)
-    XC[3] = np.diag([-100.0, -100.0, 0.01]) if D == 3 else np.diag([-100.0, -100.0])
-    XC[77] = XC[3]
+    C = XC if side == "sources" else YC
+    C[3] = np.diag([-100.0, -100.0, 0.01]) if D == 3 else np.diag([-100.0, -100.0])
+    C[77] = C[3]
     st = orc.State(X, XC, Y, YC)
     _, h = api.init(X, XC, Y, YC)
     try:
@@ -409,6 +412,9 @@ def test_indefinite_source_inverse_uses_horner_form(D):
             assert abs(E - Eo) <= 1e-6 * abs(Eo), (E, Eo)
             assert _rel(g, go) <= 1e-5
             assert abs(api.energy(h, R, t, sig) - Eo) <= 1e-6 * abs(Eo)
+            A = api.compi(h, R, t, sig=sig)
+            Ao = st.coef(R, t, sig)[: A.size]
+            assert np.abs(A - Ao).max() <= 2e-6 * np.abs(Ao).max()
     finally:
         api.fr_m(h)
 
