@@ -1,4 +1,5 @@
-"""Calls with and without the mapped pinned staging give the same bits.
+"""Calls with and without the mapped pinned staging, and with and without programmatic dependent
+launch between a call's kernels, give the same bits.
 
 The plugin calls, the REF energy calls and the captured graphs hand the pose to their first
 kernel (by value, or from the mapped staging for a graph) and read their results from the mapped
@@ -65,12 +66,16 @@ print(json.dumps(out))
 """
 
 
-def _run(no_map: bool):
+def _run(no_map: bool, no_pdl: bool = False):
     env = dict(os.environ)
     if no_map:
         env["DUGMA_NO_MAPPED_STAGING"] = "1"
     else:
         env.pop("DUGMA_NO_MAPPED_STAGING", None)
+    if no_pdl:
+        env["DUGMA_NO_PDL"] = "1"
+    else:
+        env.pop("DUGMA_NO_PDL", None)
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     return json.loads(r.stdout.strip().splitlines()[-1])
@@ -84,3 +89,12 @@ def test_mapped_and_copied_staging_give_the_same_bits():
         # the graph and the single call agree as well
         assert a[D]["Ev"] == a[D]["E"] and np.array_equal(a[D]["gv"], a[D]["g"])
         assert a[D]["s_em"] == a[D]["sig"] and np.array_equal(a[D]["A_em"], a[D]["A"])
+
+
+def test_dependent_launch_gives_the_same_bits():
+    """The kernels of a call chained by programmatic dependent launch (the default) and launched one
+    after the other (DUGMA_NO_PDL=1): every entry point, the captured graphs included, the same bits."""
+    a, b = _run(False), _run(False, no_pdl=True)
+    for D in ("3", "2"):
+        for k in a[D]:
+            assert np.array_equal(np.asarray(a[D][k]), np.asarray(b[D][k])), (D, k)
