@@ -109,24 +109,6 @@ const std::vector<Mono>& mono_table(int D)
     return D == 3 ? t3 : t2;
 }
 
-// The same factor lists with every absent factor pointing at index nv, where the evaluation keeps
-// the constant 1.0: a monomial is then always four multiplications in the same order, and a
-// multiplication by 1.0 is exact, so the value is bit for bit that of the variable-length product
-// (3x faster: no data-dependent loop exit per monomial).
-const std::vector<Mono>& mono_table_padded(int D)
-{
-    auto pad = [](const std::vector<Mono>& t, int nv) {
-        std::vector<Mono> p = t;
-        for (Mono& m : p)
-            for (int q = 0; q < 4; ++q)
-                if (m.f[q] < 0) m.f[q] = (signed char)nv;
-        return p;
-    };
-    static const std::vector<Mono> t3 = pad(mono_table(3), 12);
-    static const std::vector<Mono> t2 = pad(mono_table(2), 4);
-    return D == 3 ? t3 : t2;
-}
-
 // Surrogate Q(v) = sum_k A_k prod_q v_q^e_kq, its gradient and Hessian in v.
 struct Surrogate {
     int D, K, nv;
@@ -134,12 +116,13 @@ struct Surrogate {
     const unsigned char* E;
     double value(const double* v) const
     {
-        const Mono* T = mono_table_padded(D).data();
-        double w[13];
-        for (int q = 0; q < nv; ++q) w[q] = v[q];
-        w[nv] = 1.0;
+        const std::vector<Mono>& T = mono_table(D);
         double s = 0;
-        for (int k = 0; k < K; ++k) s += A[k] * w[T[k].f[0]] * w[T[k].f[1]] * w[T[k].f[2]] * w[T[k].f[3]];
+        for (int k = 0; k < K; ++k) {
+            double m = A[k];
+            for (int j = 0; j < 4 && T[k].f[j] >= 0; ++j) m *= v[T[k].f[j]];
+            s += m;
+        }
         return s;
     }
     // Gradient and Hessian in v (nv x nv, row-major) in one pass: for a monomial A x_0 .. x_{n-1}
