@@ -61,6 +61,16 @@ def test_reference_arm_two_ranks_print_one_line():
     _check_reference_line(lines[0], 2)
 
 
+def test_gpu_local_cpus_without_a_device():
+    """The e2e placement helper reads NVML only; without a device (or NVML) it returns no CPUs, so
+    the measurement keeps the process's own affinity instead of failing."""
+    sys.path.insert(0, ROOT)
+    import bench
+    cpus = bench.gpu_local_cpus(0)
+    assert isinstance(cpus, set)
+    assert cpus <= os.sched_getaffinity(0)
+
+
 @pytest.mark.gpu
 def test_bench_line_on_gpu():
     lines = _json_lines([sys.executable, "bench.py", "--steps", "3", "--warmup", "3", "--workload", "0"])
