@@ -9,8 +9,6 @@ import os
 import re
 import subprocess
 
-import pytest
-
 from dugma_b200 import _lib, build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

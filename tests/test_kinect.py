@@ -11,7 +11,6 @@ quasi-Newton on the fused adjoint, not the reference's method) is reported and h
 """
 import os
 
-import numpy as np
 import pytest
 
 from dugma_b200 import evaluate

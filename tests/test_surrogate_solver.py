@@ -6,7 +6,6 @@ library and by scipy (BFGS on the rotation vector); both must reach the same min
 import ctypes
 
 import numpy as np
-import pytest
 from scipy.optimize import minimize
 
 from oracle import oracle as orc
